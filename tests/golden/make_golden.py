@@ -1,0 +1,231 @@
+"""Generate the golden fixtures that pin the oracle to BetterRobot itself.
+
+Run where the reference source tree is available (it is read, never copied):
+
+    python tests/golden/make_golden.py /path/to/BetterRobot/src
+
+For each synthetic robot (``betterrobot_b200.synthetic``) the script builds the
+reference ``Model`` with the reference's own ``ModelBuilder`` + ``build_model``
+in float64, runs the reference's torch code on seeded inputs and stores inputs
+and outputs in ``tests/golden/*.npz``:
+
+* ``lie.npz``       — ``se3_exp/log``, ``so3_exp/log`` (incl. theta -> 0 and qw < 0),
+                      ``right_jacobian_inv_se3`` (the truncated-series inverse).
+* ``kin_<robot>.npz`` — ``forward_kinematics`` (oMi, liMi), ``frame_pose_world``,
+                      ``get_frame_jacobian`` in all three reference frames,
+                      ``compute_joint_jacobians``, plus the reference model's topology
+                      arrays so tests can check the local ``Model`` builds the same tree.
+* ``ik_<case>.npz`` — float64 LM / GN solves built exactly as ``solve_ik`` builds them
+                      (``tasks/ik.py:191-226``) but with the configs' damping.
+* ``adjoint.npz``   — pose loss ``sum_f w_f |log(T_f^-1 oMf(q))|^2`` and its autograd
+                      gradient w.r.t. raw ``q`` (free-flyer quaternion included).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from betterrobot_b200 import synthetic as syn  # noqa: E402
+
+D = torch.float64
+
+
+def reference_model(spec):
+    from better_robot.io.build_model import build_model
+    from better_robot.io.parsers.programmatic import ModelBuilder
+
+    b = ModelBuilder(spec["name"])
+    joints = spec["joints"]
+    bodies = {0: "universe"}
+    for i, rec in enumerate(joints):
+        bodies[i + 1] = rec["body"]
+        b.add_body(rec["body"])
+    for i, rec in enumerate(joints):
+        origin = torch.tensor(rec.get("origin", [0, 0, 0, 0, 0, 0, 1.0]), dtype=D)
+        if i == 0:
+            if rec["kind"] == "free_flyer":
+                b.add_free_flyer_root(rec["name"], child=rec["body"], origin=origin)
+            continue  # fixed root: build_model inserts "root_joint" itself
+        parent_body = bodies[rec["parent"]]
+        if rec["kind"] == "revolute_rz":
+            b.add_revolute_z(rec["name"], parent=parent_body, child=rec["body"], origin=origin,
+                             lower=rec["lower"], upper=rec["upper"])
+        else:
+            raise NotImplementedError(rec["kind"])
+    for fr in spec["frames"]:
+        b.add_frame(fr["name"], parent_body=bodies[fr["parent"]],
+                    placement=torch.tensor(fr["placement"], dtype=D))
+    return build_model(b.finalize(), dtype=D)
+
+
+def topology_arrays(m):
+    return {
+        "parents": np.array(m.parents), "nqs": np.array(m.nqs), "nvs": np.array(m.nvs),
+        "idx_qs": np.array(m.idx_qs), "idx_vs": np.array(m.idx_vs),
+        "kinds": np.array([jm.kind for jm in m.joint_models]),
+        "joint_placements": m.joint_placements.numpy(),
+        "lower": m.lower_pos_limit.numpy(), "upper": m.upper_pos_limit.numpy(),
+        "frame_parent": np.array([f.parent_joint for f in m.frames]),
+        "frame_placement": torch.stack([f.joint_placement for f in m.frames]).numpy(),
+        "frame_names": np.array(m.frame_names), "q_neutral": m.q_neutral.numpy(),
+    }
+
+
+def make_lie(out):
+    from better_robot.lie import _torch_native_backend as tn
+    from better_robot.lie.tangents import right_jacobian_inv_se3
+
+    g = torch.Generator().manual_seed(11)
+    xi = torch.randn(64, 6, generator=g, dtype=D)
+    xi[:, 3:] *= torch.linspace(0.0, 3.0, 64, dtype=D)[:, None] / xi[:, 3:].norm(dim=-1, keepdim=True)
+    xi[0, 3:] = 0.0
+    xi[1, 3:] = 1e-5
+    xi[2, 3:] = torch.tensor([3e-5, -2e-5, 1e-5], dtype=D)
+    T = tn.se3_exp(xi)
+    Tq = T.clone()
+    Tq[::3, 3:] = -Tq[::3, 3:]  # double cover: qw < 0 rows
+    np.savez_compressed(out, xi=xi.numpy(), se3_exp=T.numpy(), T_in=Tq.numpy(), se3_log=tn.se3_log(Tq).numpy(),
+                        so3_exp=tn.so3_exp(xi[:, 3:]).numpy(), so3_log=tn.so3_log(Tq[:, 3:]).numpy(),
+                        jr_inv=right_jacobian_inv_se3(xi).numpy())
+
+
+def make_kin(name, spec, batch, seed, base_t, out):
+    from better_robot.kinematics.forward import forward_kinematics
+    from better_robot.kinematics.jacobian import compute_joint_jacobians, get_frame_jacobian
+
+    m = reference_model(spec)
+    mine = syn.model_from_spec(spec, dtype=D)
+    q = syn.random_q(mine, batch, seed, rev_range=2.5, base_translation=base_t)
+    data = forward_kinematics(m, q, compute_frames=True)
+    ops = [i for i, f in enumerate(m.frames) if f.frame_type != "body"]
+    sel = ops + [m.njoints - 1]
+    Js = {}
+    for ref in ("world", "local_world_aligned", "local"):
+        Js[ref] = torch.stack([get_frame_jacobian(m, data, f, reference=ref) for f in sel], -3).numpy()
+    data2 = forward_kinematics(m, q)
+    compute_joint_jacobians(m, data2)
+    np.savez_compressed(out, q=q.numpy(), oMi=data.joint_pose_world.numpy(), liMi=data.joint_pose_local.numpy(),
+                        oMf=data.frame_pose_world.numpy(), frame_ids=np.array(sel),
+                        J_world=Js["world"], J_lwa=Js["local_world_aligned"], J_local=Js["local"],
+                        joint_jacobians=data2.joint_jacobians.numpy(), **topology_arrays(m))
+
+
+def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, factor=10.0, pos_w=1.0, ori_w=1.0,
+                 limit_w=0.1, rest_w=0.01, optimizer="lm"):
+    """One float64 solve through the reference's own stack (``tasks/ik.py:191-258``)."""
+    from better_robot.costs.stack import CostStack
+    from better_robot.kinematics.forward import forward_kinematics
+    from better_robot.optim.optimizers.gauss_newton import GaussNewton
+    from better_robot.optim.optimizers.levenberg_marquardt import LevenbergMarquardt
+    from better_robot.optim.problem import LeastSquaresProblem
+    from better_robot.optim.solvers.cholesky import Cholesky
+    from better_robot.optim.strategies.adaptive import Adaptive
+    from better_robot.residuals.base import ResidualState
+    from better_robot.residuals.limits import JointPositionLimit
+    from better_robot.residuals.pose import PoseResidual
+    from better_robot.residuals.regularization import RestResidual
+
+    stack = CostStack()
+    for name, T in zip(frame_names, targets):
+        stack.add(f"pose_{name}", PoseResidual(frame_id=m.frame_id(name), target=T, pos_weight=pos_w,
+                                               ori_weight=ori_w), weight=1.0)
+    if limit_w > 0:
+        stack.add("limits", JointPositionLimit(m), weight=limit_w)
+    if rest_w > 0:
+        stack.add("rest", RestResidual(m, m.q_neutral), weight=rest_w)
+
+    def sf(x):
+        return ResidualState(model=m, data=forward_kinematics(m, x, compute_frames=True), variables=x)
+
+    prob = LeastSquaresProblem(cost_stack=stack, state_factory=sf, x0=q0.clone(), lower=m.lower_pos_limit,
+                               upper=m.upper_pos_limit, nv=m.nv, retract=lambda q, dv: m.integrate(q, dv))
+    if optimizer == "lm":
+        st = LevenbergMarquardt(lam0=lam0, factor=factor, tol=tol).minimize(
+            prob, max_iter=max_iter, linear_solver=Cholesky(), strategy=Adaptive(lam0=lam0, factor=factor))
+    else:
+        st = GaussNewton(tol=tol).minimize(prob, max_iter=max_iter, linear_solver=Cholesky())
+    return st
+
+
+def make_ik(case, spec, frame_names, P, seed, start, out, **kw):
+    m = reference_model(spec)
+    mine = syn.model_from_spec(spec, dtype=D)
+    from better_robot.kinematics.forward import forward_kinematics
+    q_star = syn.random_q(mine, P, seed, rev_range=2.5, base_translation=0.5)
+    if start == "random":
+        q0 = syn.random_q(mine, P, seed + 100, rev_range=2.8)
+    else:
+        q0 = syn.noisy_start(mine, q_star, 0.3, seed + 200)
+    data = forward_kinematics(m, q_star, compute_frames=True)
+    fids = [m.frame_id(n) for n in frame_names]
+    targets = data.frame_pose_world[:, fids, :].clone()
+    res = {"q": [], "iters": [], "converged": [], "residual": [], "cost": []}
+    for p in range(P):
+        st = reference_lm(m, frame_names, targets[p], q0[p], **kw)
+        res["q"].append(st.x.numpy())
+        res["iters"].append(st.iters)
+        res["converged"].append(st.status == "converged")
+        res["residual"].append(st.residual.numpy())
+        res["cost"].append(float(st.residual_norm))
+    np.savez_compressed(out, q_star=q_star.numpy(), q0=q0.numpy(), targets=targets.numpy(),
+                        frame_ids=np.array(fids), q_final=np.stack(res["q"]), iters=np.array(res["iters"]),
+                        converged=np.array(res["converged"]), residual=np.stack(res["residual"]),
+                        cost=np.array(res["cost"]),
+                        settings=np.array([kw.get("lam0", 0), kw.get("factor", 0), kw["tol"], kw["max_iter"],
+                                           kw.get("limit_w", 0.1), kw.get("rest_w", 0.01)]),
+                        optimizer=np.array(kw.get("optimizer", "lm")))
+
+
+def make_adjoint(spec, B, seed, out):
+    from better_robot.kinematics.forward import forward_kinematics
+    from better_robot.lie import se3
+
+    m = reference_model(spec)
+    mine = syn.model_from_spec(spec, dtype=D)
+    q = syn.random_q(mine, B, seed, rev_range=2.5, base_translation=1.0)
+    ops = [i for i, f in enumerate(m.frames) if f.frame_type != "body"]
+    targets = syn.random_targets(B, len(ops), seed + 1)
+    rng = np.random.default_rng(seed + 2)
+    w = torch.from_numpy(rng.uniform(0.5, 2.0, size=len(ops)))
+    qv = q.clone().requires_grad_(True)
+    data = forward_kinematics(m, qv, compute_frames=True)
+    oMf = data.frame_pose_world[:, ops, :]
+    xi = se3.log(se3.compose(se3.inverse(targets), oMf))
+    loss = ((xi * xi).sum(-1) * w).sum(-1)
+    (g,) = torch.autograd.grad(loss.sum(), qv)
+    np.savez_compressed(out, q=q.numpy(), targets=targets.numpy(), weights=w.numpy(), frame_ids=np.array(ops),
+                        loss=loss.detach().numpy(), grad=g.numpy())
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else None
+    if src:
+        sys.path.insert(0, src)
+    torch.set_default_dtype(D)
+    make_lie(os.path.join(HERE, "lie.npz"))
+    chain, hum, dual = syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()
+    make_kin("chain7", chain, 16, 5, 0.0, os.path.join(HERE, "kin_chain7.npz"))
+    make_kin("humanoid", hum, 8, 6, 1.0, os.path.join(HERE, "kin_humanoid.npz"))
+    make_kin("dual_arm", dual, 8, 7, 0.0, os.path.join(HERE, "kin_dual_arm.npz"))
+    lm = dict(lam0=1e-3, factor=10.0, tol=1e-6)
+    make_ik("chain7_random", chain, ["ee"], 8, 21, "random", os.path.join(HERE, "ik_chain7_random.npz"),
+            max_iter=50, **lm)
+    make_ik("chain7_noisy_gn", chain, ["ee"], 6, 22, "noisy", os.path.join(HERE, "ik_chain7_gn.npz"),
+            max_iter=30, tol=1e-6, optimizer="gn")
+    make_ik("dual_arm", dual, ["ee_l", "ee_r"], 4, 23, "noisy", os.path.join(HERE, "ik_dual_arm.npz"),
+            max_iter=100, rest_w=1e-3, **lm)
+    make_ik("humanoid", hum, ["track0", "track2", "track4"], 4, 24, "noisy",
+            os.path.join(HERE, "ik_humanoid.npz"), max_iter=100, rest_w=1e-3, **lm)
+    make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,97 @@
+"""The float64 oracle reproduces BetterRobot's own outputs (golden fixtures made by the reference)."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from betterrobot_b200 import synthetic as syn
+from oracle import ik, kinematics as K, lie
+
+from conftest import GOLDEN
+
+SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec()}
+
+
+def _load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+@pytest.mark.parametrize("robot", list(SPECS))
+def test_local_model_matches_reference_tree(robot):
+    g = _load(f"kin_{robot}.npz")
+    m = syn.model_from_spec(SPECS[robot], dtype=torch.float64)
+    assert tuple(g["parents"]) == m.parents
+    assert list(g["kinds"]) == [jm.kind for jm in m.joint_models]
+    np.testing.assert_array_equal(g["idx_qs"], m.idx_qs)
+    np.testing.assert_array_equal(g["idx_vs"], m.idx_vs)
+    np.testing.assert_array_equal(g["joint_placements"], m.joint_placements.numpy())
+    np.testing.assert_array_equal(g["lower"], m.lower_pos_limit.numpy())
+    np.testing.assert_array_equal(g["upper"], m.upper_pos_limit.numpy())
+    assert list(g["frame_names"]) == list(m.frame_names)
+    np.testing.assert_array_equal(g["frame_parent"], [f.parent_joint for f in m.frames])
+    np.testing.assert_allclose(g["frame_placement"], torch.stack([f.joint_placement for f in m.frames]).numpy(),
+                               atol=0, rtol=0)
+    np.testing.assert_array_equal(g["q_neutral"], m.q_neutral.numpy())
+
+
+@pytest.mark.parametrize("robot", list(SPECS))
+def test_fk_frames_jacobians_match_reference(robot):
+    g = _load(f"kin_{robot}.npz")
+    m = syn.model_from_spec(SPECS[robot], dtype=torch.float64)
+    oMi, liMi = K.forward_kinematics(m, g["q"])
+    np.testing.assert_allclose(oMi, g["oMi"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(liMi, g["liMi"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(K.frame_placements(m, oMi), g["oMf"], atol=1e-12, rtol=0)
+    for ref, key in (("world", "J_world"), ("local_world_aligned", "J_lwa"), ("local", "J_local")):
+        J = np.stack([K.frame_jacobian(m, oMi, g["q"], int(f), ref) for f in g["frame_ids"]], -3)
+        np.testing.assert_allclose(J, g[key], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(K.compute_joint_jacobians(m, oMi, g["q"]), g["joint_jacobians"], atol=1e-12, rtol=0)
+
+
+def test_lie_matches_reference():
+    g = _load("lie.npz")
+    np.testing.assert_allclose(lie.se3_exp(g["xi"]), g["se3_exp"], atol=1e-13, rtol=0)
+    np.testing.assert_allclose(lie.se3_log(g["T_in"]), g["se3_log"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(lie.so3_exp(g["xi"][:, 3:]), g["so3_exp"], atol=1e-13, rtol=0)
+    np.testing.assert_allclose(lie.so3_log(g["T_in"][:, 3:]), g["so3_log"], atol=1e-13, rtol=0)
+    np.testing.assert_allclose(lie.right_jacobian_inv_se3(g["xi"]), g["jr_inv"], atol=1e-12, rtol=0)
+
+
+@pytest.mark.parametrize("case,robot", [("chain7_random", "chain7"), ("chain7_gn", "chain7"),
+                                        ("dual_arm", "dual_arm"), ("humanoid", "humanoid")])
+def test_lm_gn_match_reference_solver(case, robot):
+    g = _load(f"ik_{case}.npz")
+    m = syn.model_from_spec(SPECS[robot], dtype=torch.float64)
+    st = g["settings"]
+    s = ik.IKSettings(lam0=st[0], factor=st[1], tol=st[2], max_iter=int(st[3]), limit_weight=st[4],
+                      rest_weight=st[5], optimizer=str(g["optimizer"]))
+    out = ik.solve(m, [int(f) for f in g["frame_ids"]], g["targets"], g["q0"], s)
+    np.testing.assert_array_equal(out.iters, g["iters"])
+    np.testing.assert_array_equal(out.converged, g["converged"])
+    np.testing.assert_allclose(out.q, g["q_final"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(out.cost, g["cost"], atol=1e-12, rtol=1e-9)
+
+
+def test_pose_loss_matches_reference():
+    g = _load("adjoint.npz")
+    m = syn.model_from_spec(SPECS["humanoid"], dtype=torch.float64)
+    oMi, _ = K.forward_kinematics(m, g["q"])
+    oMf = K.frame_placements(m, oMi, [int(f) for f in g["frame_ids"]])
+    xi = lie.se3_log(lie.se3_compose(lie.se3_inverse(g["targets"]), oMf))
+    loss = ((xi * xi).sum(-1) * g["weights"]).sum(-1)
+    np.testing.assert_allclose(loss, g["loss"], atol=1e-12, rtol=1e-12)
+
+
+def test_known_answers_one_joint_arm():
+    """Reference known answers on a 1-joint arm (``tests/kinematics/test_fk.py:85-103``)."""
+    import math
+    m = syn.build_model("arm", [
+        {"name": "root_joint", "kind": "fixed", "parent": 0, "body": "base"},
+        {"name": "j1", "kind": "revolute_rz", "parent": 1, "body": "link1",
+         "origin": [0, 0, 0.1, 0, 0, 0, 1], "lower": -math.pi, "upper": math.pi}], dtype=torch.float64)
+    oMi, _ = K.forward_kinematics(m, np.zeros(1))
+    assert abs(oMi[2, 2] - 0.1) < 1e-12
+    oMi, _ = K.forward_kinematics(m, np.array([math.pi / 2]))
+    assert abs(oMi[2, 5] - math.sin(math.pi / 4)) < 1e-12 and abs(oMi[2, 6] - math.cos(math.pi / 4)) < 1e-12
