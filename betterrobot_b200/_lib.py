@@ -1,0 +1,88 @@
+"""ctypes binding of ``libbr_b200.so`` (declarations in ``include/br_b200.h``).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, every entry point raises ``BackendNotAvailableError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+from .exceptions import BackendNotAvailableError, KernelError
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbr_b200.so")
+
+c_int32 = ctypes.c_int32
+c_int64 = ctypes.c_int64
+c_void_p = ctypes.c_void_p
+
+STATUS = {0: "ok", -1: "invalid argument", -2: "size above the library limit", -3: "misaligned pointer"}
+
+
+class BrTree(ctypes.Structure):
+    """Mirror of ``br_tree_t``."""
+
+    _fields_ = [("njoints", c_int32), ("nq", c_int32), ("nv", c_int32), ("nframes", c_int32),
+                ("rounds", c_int32), ("reserved", c_int32 * 3),
+                ("parent", c_void_p), ("jtype", c_void_p), ("idx_q", c_void_p), ("idx_v", c_void_p),
+                ("axis", c_void_p), ("placement", c_void_p), ("support", c_void_p),
+                ("frame_parent", c_void_p), ("frame_placement", c_void_p),
+                ("col_joint", c_void_p), ("col_kind", c_void_p), ("col_axis", c_void_p),
+                ("lower", c_void_p), ("upper", c_void_p)]
+
+
+# name -> (restype, argtypes); must match include/br_b200.h
+SIGNATURES: dict[str, tuple] = {
+    "br_version": (ctypes.c_char_p, []),
+    "br_forward_kinematics": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_void_p,
+                                        c_void_p, c_int32, c_void_p, c_void_p]),
+    "br_frame_jacobians": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32, c_int32,
+                                     c_void_p, c_void_p, c_void_p]),
+    "br_frame_jacobians_from_poses": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32,
+                                                c_int32, c_void_p, c_void_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (no device is touched)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(path):
+                raise BackendNotAvailableError(
+                    f"{path} is missing; build it with `python -m betterrobot_b200.build` (nvcc, sm_100a)")
+            lib = ctypes.CDLL(path)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def call(name: str, *args) -> None:
+    """Call an entry point and raise ``KernelError`` on a non-zero status."""
+    st = getattr(load(), name)(*args)
+    if st != 0:
+        msg = STATUS.get(st, f"CUDA error {st}")
+        raise KernelError(f"{name} returned {st} ({msg})")
+
+
+def require_cuda(t) -> None:
+    import torch
+    if not torch.cuda.is_available():
+        raise BackendNotAvailableError("the sm_100a path needs a CUDA device; none is available")
+    if not t.is_cuda:
+        from .exceptions import DeviceMismatchError
+        raise DeviceMismatchError(f"expected a CUDA tensor, got device={t.device}")
+
+
+def stream_ptr(device=None) -> int:
+    import torch
+    return torch.cuda.current_stream(device).cuda_stream

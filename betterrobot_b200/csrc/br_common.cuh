@@ -1,0 +1,56 @@
+// br_common.cuh — shared helpers: TMA bulk-store wrappers, shared-memory
+// layout arithmetic and per-device launch properties.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/br_b200.h"
+
+namespace br {
+
+constexpr int kWarp = 32;
+
+__host__ __device__ __forceinline__ int round4(int n) { return (n + 3) & ~3; }
+
+// ---- Blackwell bulk async copies (cp.async.bulk, smem -> global) ---------
+// Make generic-proxy shared-memory writes visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// One contiguous shared -> global copy; both addresses 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(ssrc));
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+               :: "l"(gdst), "r"(s), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Wait until every committed bulk group has finished READING shared memory.
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// Wait until every committed bulk group has completed (writes performed).
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Warp-cooperative copy of `n` floats from shared to global (fallback when the
+// destination block is not 16-byte aligned or its size is not a multiple of 16).
+__device__ __forceinline__ void warp_copy(float* __restrict__ g, const float* __restrict__ s, int n, int lane) {
+  for (int i = lane; i < n; i += kWarp) g[i] = s[i];
+}
+
+// ---- host helpers --------------------------------------------------------
+struct DeviceInfo {
+  int device = -1;
+  int sms = 0;
+  int max_smem_optin = 0;
+  size_t l2_bytes = 0;
+};
+
+// Cached per current device.
+const DeviceInfo& device_info();
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline bool aligned4(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 3u) == 0; }
+
+int validate_tree(const br_tree_t* t);
+
+}  // namespace br

@@ -1,0 +1,260 @@
+// br_lie.cuh — SE3 / SO3 device functions (float32).
+//
+// Same conventions and formulas as BetterRobot's torch backend
+// (src/better_robot/lie/_torch_native_backend.py): poses [t, q] with scalar-last
+// quaternions, tangents [v, w] linear first.  Where a float64 formula loses
+// precision in float32 (1 - cos, theta - sin, 1/theta^2 - cot(theta/2)/(2 theta))
+// the coefficient is evaluated from its Taylor series below a cutoff instead, so
+// results agree with the float64 reference to float32 rounding.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace br {
+
+struct Pose {
+  float3 t;
+  float4 q;  // (x, y, z, w)
+};
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 add(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 scale(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+  return f3(fmaf(a.y, b.z, -a.z * b.y), fmaf(a.z, b.x, -a.x * b.z), fmaf(a.x, b.y, -a.y * b.x));
+}
+// a + s * b
+__device__ __forceinline__ float3 axpy(float s, float3 b, float3 a) {
+  return f3(fmaf(s, b.x, a.x), fmaf(s, b.y, a.y), fmaf(s, b.z, a.z));
+}
+
+// Hamilton product a (x) b   (_quat_mul, _torch_native_backend.py:44-52)
+__device__ __forceinline__ float4 qmul(float4 a, float4 b) {
+  float4 r;
+  r.x = a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y;
+  r.y = a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x;
+  r.z = a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w;
+  r.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+  return r;
+}
+
+__device__ __forceinline__ float4 qconj(float4 q) { return make_float4(-q.x, -q.y, -q.z, q.w); }
+
+// p' = p + 2 u x (u x p + w p)   (so3_act, _torch_native_backend.py:186-199)
+__device__ __forceinline__ float3 qrot(float4 q, float3 p) {
+  const float3 u = f3(q.x, q.y, q.z);
+  const float3 c1 = axpy(q.w, p, cross(u, p));
+  return axpy(2.f, cross(u, c1), p);
+}
+__device__ __forceinline__ float3 qrot_inv(float4 q, float3 p) { return qrot(qconj(q), p); }
+
+// c = a * b   (se3_compose, _torch_native_backend.py:237-246)
+__device__ __forceinline__ Pose compose(const Pose& a, const Pose& b) {
+  Pose c;
+  c.t = add(a.t, qrot(a.q, b.t));
+  c.q = qmul(a.q, b.q);
+  return c;
+}
+
+// T^-1   (se3_inverse, _torch_native_backend.py:249-255)
+__device__ __forceinline__ Pose inverse(const Pose& a) {
+  Pose r;
+  r.q = qconj(a.q);
+  r.t = scale(qrot(r.q, a.t), -1.f);
+  return r;
+}
+
+// (se3_normalize, _torch_native_backend.py:358-361): quaternion / max(|q|, 1e-8)
+__device__ __forceinline__ float4 qnormalize(float4 q) {
+  const float n = fmaxf(sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-8f);
+  const float s = 1.f / n;
+  return make_float4(q.x * s, q.y * s, q.z * s, q.w * s);
+}
+
+// theta / sin(theta/2) factor of so3_log and the log itself
+// (so3_log, _torch_native_backend.py:162-183; folds qw < 0 onto the same rotation).
+__device__ __forceinline__ float3 so3_log(float4 q) {
+  if (q.w < 0.f) q = make_float4(-q.x, -q.y, -q.z, -q.w);
+  const float s2 = q.x * q.x + q.y * q.y + q.z * q.z;
+  const float s = sqrtf(s2);
+  float factor;
+  if (s2 < 0.25e-8f) {
+    factor = 2.f + s2 * (2.f / 3.f);
+  } else {
+    const float theta = 2.f * atan2f(s, fminf(fmaxf(q.w, -1.f), 1.f));
+    factor = theta / s;
+  }
+  return f3(factor * q.x, factor * q.y, factor * q.z);
+}
+
+// c(theta) = 1/theta^2 - cot(theta/2) / (2 theta), the W^2 coefficient of V^-1
+// (se3_log, _torch_native_backend.py:298-303) and of the SO3 Jr^-1
+// (tangents.right_jacobian_inv_so3:122-145).  Series 1/12 + t2/720 + t2^2/30240
+// + t2^3/1209600 + t2^4/47900160 below theta = 1 (float32 cancels there).
+__device__ __forceinline__ float vinv_coeff(float th2) {
+  if (th2 < 1.f) {
+    return fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 47900160.f, 1.f / 1209600.f), 1.f / 30240.f),
+                          1.f / 720.f), 1.f / 12.f);
+  }
+  const float th = sqrtf(th2);
+  float sh, ch;
+  sincosf(0.5f * th, &sh, &ch);
+  return 1.f / th2 - (ch / sh) / (2.f * th);
+}
+
+// SE3 log -> (v, w)   (se3_log, _torch_native_backend.py:289-310)
+__device__ __forceinline__ void se3_log(const Pose& T, float3& v, float3& w) {
+  w = so3_log(T.q);
+  const float th2 = dot(w, w);
+  const float c = vinv_coeff(th2);
+  // V^-1 t = t - 1/2 w x t + c w x (w x t)
+  const float3 wt = cross(w, T.t);
+  v = axpy(c, cross(w, wt), axpy(-0.5f, wt, T.t));
+}
+
+// b = (1 - cos th)/th^2 and c = (th - sin th)/th^3 of se3_exp (_torch_native_backend.py:272-278)
+__device__ __forceinline__ void exp_coeffs(float th2, float& b, float& c) {
+  if (th2 < 1.f) {
+    // b = 1/2 - t2/24 + t2^2/720 - t2^3/40320 + t2^4/3628800
+    b = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 3628800.f, -1.f / 40320.f), 1.f / 720.f), -1.f / 24.f), 0.5f);
+    // c = 1/6 - t2/120 + t2^2/5040 - t2^3/362880 + t2^4/39916800
+    c = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 39916800.f, -1.f / 362880.f), 1.f / 5040.f), -1.f / 120.f),
+             1.f / 6.f);
+  } else {
+    const float th = sqrtf(th2);
+    float s, co, sh, ch;
+    sincosf(th, &s, &co);
+    sincosf(0.5f * th, &sh, &ch);
+    b = 2.f * sh * sh / th2;  // 1 - cos th = 2 sin^2(th/2)
+    c = (th - s) / (th * th2);
+  }
+}
+
+// so3_exp (_torch_native_backend.py:144-159)
+__device__ __forceinline__ float4 so3_exp(float3 w) {
+  const float th2 = dot(w, w);
+  float k, cw;
+  if (th2 < 1e-8f) {
+    k = 0.5f - th2 / 48.f;
+    cw = 1.f - th2 / 8.f;
+  } else {
+    const float th = sqrtf(th2);
+    float sh;
+    sincosf(0.5f * th, &sh, &cw);
+    k = sh / th;
+  }
+  return make_float4(k * w.x, k * w.y, k * w.z, cw);
+}
+
+// se3_exp (_torch_native_backend.py:258-286): T = (V(w) v, exp(w))
+__device__ __forceinline__ Pose se3_exp(float3 v, float3 w) {
+  float b, c;
+  exp_coeffs(dot(w, w), b, c);
+  const float3 wv = cross(w, v);
+  Pose T;
+  T.t = axpy(c, cross(w, wv), axpy(b, wv, v));
+  T.q = so3_exp(w);
+  return T;
+}
+
+// ---------------------------------------------------------------------------
+// Inverse of the SE3 right Jacobian.
+//
+// Jr(xi) = sum_{k=0}^{N} (-1)^k/(k+1)! ad(xi)^k with ad = [[W, V], [0, W]]
+// (W = hat(w), V = hat(v); tangents._ad_matrix:164-178).  The series has the
+// block form [[A, B], [0, A]] with A a polynomial in W, so
+// Jr^-1 = [[A^-1, -A^-1 B A^-1], [0, A^-1]].  A is kept as (a0, a1, a2) in the
+// basis {I, W, W^2} (W^3 = -theta^2 W) and A^-1 as (b0, b1, b2) in the same
+// basis; B is an explicit 3x3 matrix.  N = 9 reproduces the reference's
+// truncated series (tangents.right_jacobian_se3:184-201, inverted with
+// torch.linalg.inv at :204-207); a larger N gives the exact Jacobian.
+// ---------------------------------------------------------------------------
+struct JrInv {
+  float3 w;          // rotation part of xi
+  float b0, b1, b2;  // A^-1 = b0 I + b1 W + b2 W^2
+  float B[9];        // row-major
+};
+
+// y = (b0 I + b1 W + b2 W^2) x
+__device__ __forceinline__ float3 apply_poly(const float3& w, float b0, float b1, float b2, float3 x) {
+  const float3 wx = cross(w, x);
+  return axpy(b2, cross(w, wx), axpy(b1, wx, scale(x, b0)));
+}
+
+__device__ __forceinline__ float3 mat3_vec(const float* M, float3 x) {
+  return f3(fmaf(M[0], x.x, fmaf(M[1], x.y, M[2] * x.z)), fmaf(M[3], x.x, fmaf(M[4], x.y, M[5] * x.z)),
+            fmaf(M[6], x.x, fmaf(M[7], x.y, M[8] * x.z)));
+}
+__device__ __forceinline__ float3 mat3T_vec(const float* M, float3 x) {
+  return f3(fmaf(M[0], x.x, fmaf(M[3], x.y, M[6] * x.z)), fmaf(M[1], x.x, fmaf(M[4], x.y, M[7] * x.z)),
+            fmaf(M[2], x.x, fmaf(M[5], x.y, M[8] * x.z)));
+}
+
+template <int N>
+__device__ __forceinline__ JrInv jr_inv_se3(float3 v, float3 w) {
+  // c_k = (-1)^k / (k+1)!
+  float ck[N + 1];
+  {
+    float f = 1.f;
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+      f /= (float)(k + 1);
+      ck[k] = (k & 1) ? -f : f;
+    }
+  }
+  const float th2 = dot(w, w);
+  float a0 = ck[N], a1 = 0.f, a2 = 0.f;
+  float B[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = N - 1; k >= 0; --k) {
+    // B <- W B + V A, with A = a0 I + a1 W + a2 W^2 (the previous A)
+    float nB[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float3 bc = f3(B[c], B[3 + c], B[6 + c]);
+      const float3 e = f3(c == 0 ? 1.f : 0.f, c == 1 ? 1.f : 0.f, c == 2 ? 1.f : 0.f);
+      const float3 ac = apply_poly(w, a0, a1, a2, e);     // column c of A
+      const float3 r = add(cross(w, bc), cross(v, ac));   // W B_c + V A_c
+      nB[c] = r.x;
+      nB[3 + c] = r.y;
+      nB[6 + c] = r.z;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) B[i] = nB[i];
+    // A <- c_k I + W A = c_k I + (a0 - th2 a2) W + a1 W^2
+    const float na1 = fmaf(-th2, a2, a0);
+    a2 = a1;
+    a1 = na1;
+    a0 = ck[k];
+  }
+  // A^-1 in the same basis: b0 = 1/a0; [m, -th2 a1; a1, m] [b1; b2] = -b0 [a1; a2], m = a0 - th2 a2
+  JrInv J;
+  J.w = w;
+  const float b0 = 1.f / a0;
+  const float m = fmaf(-th2, a2, a0);
+  const float r0 = -a1 * b0, r1 = -a2 * b0;
+  const float det = fmaf(m, m, th2 * a1 * a1);
+  const float idet = 1.f / det;
+  J.b0 = b0;
+  J.b1 = (r0 * m + th2 * a1 * r1) * idet;
+  J.b2 = (m * r1 - a1 * r0) * idet;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) J.B[i] = B[i];
+  return J;
+}
+
+// out = Jr^-1 [x_lin; x_ang] = [A^-1 (x_lin - B A^-1 x_ang); A^-1 x_ang]
+__device__ __forceinline__ void jr_inv_apply(const JrInv& J, float3 xl, float3 xa, float3& ol, float3& oa) {
+  oa = apply_poly(J.w, J.b0, J.b1, J.b2, xa);
+  ol = apply_poly(J.w, J.b0, J.b1, J.b2, sub(xl, mat3_vec(J.B, oa)));
+}
+
+// out = Jr^-T [x_lin; x_ang] = [A^-T x_lin; A^-T (x_ang - B^T A^-T x_lin)]   (A^-T: W -> -W)
+__device__ __forceinline__ void jr_inv_T_apply(const JrInv& J, float3 xl, float3 xa, float3& ol, float3& oa) {
+  ol = apply_poly(J.w, J.b0, -J.b1, J.b2, xl);
+  oa = apply_poly(J.w, J.b0, -J.b1, J.b2, sub(xa, mat3T_vec(J.B, ol)));
+}
+
+}  // namespace br

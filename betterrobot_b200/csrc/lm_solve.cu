@@ -1,0 +1,622 @@
+// lm_solve.cu — persistent batched Levenberg-Marquardt / Gauss-Newton IK for sm_100a.
+//
+// One launch solves thousands of independent IK problems of uneven size
+// (different robots, DOF and target counts).  The reference solves one problem
+// per call with >= 3 host syncs per iteration
+// (src/better_robot/optim/optimizers/levenberg_marquardt.py:61-135); here the whole
+// loop stays on the device:
+//
+//   * a TEAM of T lanes (T = 8, 16 or 32, chosen per robot class) owns one
+//     problem; a warp takes a work item of 32/T problems of one class from an
+//     atomic queue and its teams run their LM loops independently.  A team whose
+//     problem converges leaves the loop and the warp takes the next item, so no
+//     lane keeps iterating a converged problem (work compaction by queue);
+//   * per iteration: forward kinematics of the trial point by pointer jumping in
+//     shared memory, the stacked residual (pose targets, joint limits, rest) and
+//     its cost by a team reduction, accept/reject, and — only after an accepted
+//     step, because the reference recomputes an identical J after a rejection —
+//     the Jacobian build: J^T J and J^T r accumulated directly from the analytic
+//     pose Jacobian Jr^-1(xi) blockdiag(R^T, R^T) J_lwa (pose.py:68-103) with columns
+//     outside a target's support skipped;
+//   * H = J^T J + lambda I factored by a right-looking Cholesky in shared memory
+//     (lanes over the trailing triangle), triangular solves by shuffles;
+//   * retraction q (+) dq (Model.integrate, model.py:160-174) and clamping to the
+//     joint limits (levenberg_marquardt.py:103-107).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/br_b200.h"
+#include "br_common.cuh"
+#include "br_lie.cuh"
+
+namespace br {
+
+constexpr int kMaxClasses = BR_MAX_IK_CLASSES;
+constexpr int kMaxT = BR_MAX_IK_TARGETS;
+
+struct LmParams {
+  br_ik_settings_t s;
+  br_ik_batch_t b;
+  br_ik_result_t r;
+  br_tree_t trees[kMaxClasses];
+  int32_t team[kMaxClasses];
+  int32_t warp_floats;       // per-warp shared memory (floats)
+  int32_t* queue;            // scratch: work-queue counter (zeroed before launch)
+};
+
+// ---- per-team shared-memory layout (floats) --------------------------------
+struct TeamLayout {
+  int parent, jtype, idxq, idxv, axis, place, support, cjoint, ckind, caxis, lower, upper;
+  int fparent, fplace, tgt, cmask;
+  int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc;
+  int total;
+  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K) {
+    int o = 0;
+    auto take = [&](int n) { int r = o; o += round4(n); return r; };
+    parent = take(nj); jtype = take(nj); idxq = take(nj); idxv = take(nj);
+    axis = take(4 * nj); place = take(8 * nj); support = take(2 * nj);
+    cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
+    lower = take(nq); upper = take(nq);
+    fparent = take(K); fplace = take(8 * K); tgt = take(8 * K); cmask = take(2 * K);
+    x = take(nq); xn = take(nq); qrest = take(nq);
+    poseA = take(8 * nj); poseB = take(8 * nj); ancA = take(nj); ancB = take(nj);
+    tw = take(8 * K); xi = take(8 * K); jri = take(16 * K); colw = take(8 * nv);
+    d = take(nv); g = take(nv); delta = take(nv);
+    jtj = take(nv * (nv + 1) / 2);
+    const int jp = 6 * K * nv, lsq = nv * (nv + 1);
+    work = take(jp > lsq ? jp : lsq);  // J_pose during the Jacobian build, L during the solve
+    misc = take(8);
+    total = o;
+  }
+};
+
+__device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
+
+template <int T>
+struct Team {
+  unsigned mask;
+  int tl;  // lane within team
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  __device__ __forceinline__ float sum(float v) const {
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, T);
+    return v;
+  }
+  __device__ __forceinline__ float bcast(float v, int src) const { return __shfl_sync(mask, v, src, T); }
+};
+
+__device__ __forceinline__ Pose ld8(const float* p) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  Pose P;
+  P.t = f3(a.x, a.y, a.z);
+  P.q = *reinterpret_cast<const float4*>(p + 4);
+  return P;
+}
+__device__ __forceinline__ void st8(float* p, const Pose& P) {
+  *reinterpret_cast<float4*>(p) = make_float4(P.t.x, P.t.y, P.t.z, 0.f);
+  *reinterpret_cast<float4*>(p + 4) = P.q;
+}
+
+// ---- one problem, solved by one team ---------------------------------------
+template <int T>
+__device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
+  const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
+  const int K = P.b.max_targets;
+  const TeamLayout L(nj, nq, nv, K);
+  int* parent = reinterpret_cast<int*>(sm + L.parent);
+  int* jtype = reinterpret_cast<int*>(sm + L.jtype);
+  int* idxq = reinterpret_cast<int*>(sm + L.idxq);
+  int* idxv = reinterpret_cast<int*>(sm + L.idxv);
+  float* axis = sm + L.axis;
+  float* place = sm + L.place;
+  unsigned long long* support = reinterpret_cast<unsigned long long*>(sm + L.support);
+  int* cjoint = reinterpret_cast<int*>(sm + L.cjoint);
+  int* ckind = reinterpret_cast<int*>(sm + L.ckind);
+  float* caxis = sm + L.caxis;
+  float* lower = sm + L.lower;
+  float* upper = sm + L.upper;
+  int* fparent = reinterpret_cast<int*>(sm + L.fparent);
+  float* fplace = sm + L.fplace;
+  float* tgt = sm + L.tgt;
+  unsigned long long* cmask = reinterpret_cast<unsigned long long*>(sm + L.cmask);
+  float* x = sm + L.x;
+  float* xn = sm + L.xn;
+  float* qrest = sm + L.qrest;
+  float* poseA = sm + L.poseA;
+  float* poseB = sm + L.poseB;
+  int* ancA = reinterpret_cast<int*>(sm + L.ancA);
+  int* ancB = reinterpret_cast<int*>(sm + L.ancB);
+  float* tw = sm + L.tw;
+  float* xi = sm + L.xi;
+  float* jri = sm + L.jri;
+  float* colw = sm + L.colw;
+  float* dr = sm + L.d;
+  float* g = sm + L.g;
+  float* delta = sm + L.delta;
+  float* jtj = sm + L.jtj;
+  float* work = sm + L.work;
+  const int tl = tm.tl;
+  const br_ik_settings_t& S = P.s;
+  const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
+  const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
+
+  // ---- load the tree table and the problem -------------------------------
+  for (int j = tl; j < nj; j += T) {
+    parent[j] = tree.parent[j];
+    jtype[j] = tree.jtype[j];
+    idxq[j] = tree.idx_q[j];
+    idxv[j] = tree.idx_v[j];
+    *reinterpret_cast<float4*>(axis + 4 * j) = *reinterpret_cast<const float4*>(tree.axis + 4 * j);
+    *reinterpret_cast<float4*>(place + 8 * j) = *reinterpret_cast<const float4*>(tree.placement + 8 * j);
+    *reinterpret_cast<float4*>(place + 8 * j + 4) = *reinterpret_cast<const float4*>(tree.placement + 8 * j + 4);
+    support[j] = tree.support[j];
+  }
+  for (int c = tl; c < nv; c += T) {
+    cjoint[c] = tree.col_joint[c];
+    ckind[c] = tree.col_kind[c];
+    *reinterpret_cast<float4*>(caxis + 4 * c) = *reinterpret_cast<const float4*>(tree.col_axis + 4 * c);
+  }
+  const int64_t qoff = P.b.q_offset[prob];
+  for (int i = tl; i < nq; i += T) {
+    lower[i] = tree.lower[i];
+    upper[i] = tree.upper[i];
+    x[i] = P.b.x0[qoff + i];
+    qrest[i] = P.b.q_rest[qoff + i];
+  }
+  const int nt = P.b.n_targets[prob];
+  for (int t = tl; t < K; t += T) {
+    if (t < nt) {
+      const int f = P.b.frames[(int64_t)prob * K + t];
+      fparent[t] = tree.frame_parent[f];
+      for (int k = 0; k < 8; ++k) fplace[8 * t + k] = tree.frame_placement[8 * f + k];
+      const float* tp = P.b.targets + ((int64_t)prob * K + t) * 7;
+      st8(tgt + 8 * t, Pose{f3(tp[0], tp[1], tp[2]), make_float4(tp[3], tp[4], tp[5], tp[6])});
+    }
+  }
+  tm.sync();
+  // column support mask of each target frame
+  for (int t = 0; t < nt; ++t) {
+    const unsigned long long sup = support[fparent[t]];
+    unsigned long long m = 0ull;
+    for (int c0 = 0; c0 < nv; c0 += T) {
+      const int c = c0 + tl;
+      const bool in = c < nv && ((sup >> cjoint[c]) & 1ull);
+      const unsigned bal = __ballot_sync(tm.mask, in) >> ((threadIdx.x & 31) - tl);
+      m |= (unsigned long long)(bal & (T == 32 ? 0xffffffffu : ((1u << T) - 1u))) << c0;
+    }
+    if (tl == 0) cmask[t] = m;
+  }
+  tm.sync();
+
+  // ---- helpers ------------------------------------------------------------
+  // FK of configuration q (shared) -> world poses (returned buffer), pointer jumping.
+  auto fk = [&](const float* q) -> float* {
+    for (int j = tl; j < nj; j += T) {
+      const Pose Pj = ld8(place + 8 * j);
+      Pose Lj = Pj;
+      const int jt = jtype[j];
+      const float* qv = q + idxq[j];
+      if (jt == BR_JOINT_REVOLUTE) {
+        float s, c;
+        sincosf(0.5f * qv[0], &s, &c);
+        Lj.q = qmul(Pj.q, make_float4(s * axis[4 * j], s * axis[4 * j + 1], s * axis[4 * j + 2], c));
+      } else if (jt == BR_JOINT_PRISMATIC) {
+        Lj.t = add(Pj.t, qrot(Pj.q, f3(qv[0] * axis[4 * j], qv[0] * axis[4 * j + 1], qv[0] * axis[4 * j + 2])));
+      } else if (jt == BR_JOINT_FREE_FLYER) {
+        Lj = compose(Pj, Pose{f3(qv[0], qv[1], qv[2]), qnormalize(make_float4(qv[3], qv[4], qv[5], qv[6]))});
+      }
+      st8(poseA + 8 * j, Lj);
+      ancA[j] = parent[j];
+    }
+    tm.sync();
+    float* A = poseA;
+    float* B = poseB;
+    int* aA = ancA;
+    int* aB = ancB;
+    for (int r = 0; r < tree.rounds; ++r) {
+      for (int j = tl; j < nj; j += T) {
+        const int a = aA[j];
+        if (a >= 0) {
+          st8(B + 8 * j, compose(ld8(A + 8 * a), ld8(A + 8 * j)));
+          aB[j] = aA[a];
+        } else {
+          st8(B + 8 * j, ld8(A + 8 * j));
+          aB[j] = -1;
+        }
+      }
+      tm.sync();
+      float* tp = A; A = B; B = tp;
+      int* ta = aA; aA = aB; aB = ta;
+    }
+    return A;
+  };
+
+  // Residual of the stack at q with world poses `pose`: fills tw, xi, dr; returns 0.5 |r|^2.
+  auto residual = [&](const float* q, const float* pose) -> float {
+    float acc = 0.f;
+    for (int t = tl; t < nt; t += T) {
+      const Pose Tee = compose(ld8(pose + 8 * fparent[t]), ld8(fplace + 8 * t));
+      st8(tw + 8 * t, Tee);
+      float3 v, w;
+      se3_log(compose(inverse(ld8(tgt + 8 * t)), Tee), v, w);       // pose.py:63-64
+      *reinterpret_cast<float4*>(xi + 8 * t) = make_float4(v.x, v.y, v.z, w.x);
+      *reinterpret_cast<float4*>(xi + 8 * t + 4) = make_float4(w.y, w.z, 0.f, 0.f);
+      acc += wp * wp * dot(v, v) + wo * wo * dot(w, w);
+    }
+    if (use_limits) {                                                // limits.py:56-62
+      for (int i = tl; i < nq; i += T) {
+        const float lo = fmaxf(lower[i] - q[i], 0.f), hi = fmaxf(q[i] - upper[i], 0.f);
+        acc += wl * wl * (lo * lo + hi * hi);
+      }
+    }
+    if (use_rest) {                                                  // regularization.py:48-54
+      for (int j = tl; j < nj; j += T) {
+        const int jt = jtype[j];
+        const int iq = idxq[j], iv = idxv[j];
+        if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
+          const float dd = q[iq] - qrest[iq];
+          dr[iv] = dd;
+          acc += wr * wr * dd * dd;
+        } else if (jt == BR_JOINT_FREE_FLYER) {                      // free_flyer.py:53-57
+          const Pose a{f3(qrest[iq], qrest[iq + 1], qrest[iq + 2]),
+                       make_float4(qrest[iq + 3], qrest[iq + 4], qrest[iq + 5], qrest[iq + 6])};
+          const Pose b{f3(q[iq], q[iq + 1], q[iq + 2]), make_float4(q[iq + 3], q[iq + 4], q[iq + 5], q[iq + 6])};
+          float3 v, w;
+          se3_log(compose(inverse(a), b), v, w);
+          dr[iv] = v.x; dr[iv + 1] = v.y; dr[iv + 2] = v.z;
+          dr[iv + 3] = w.x; dr[iv + 4] = w.y; dr[iv + 5] = w.z;
+          acc += wr * wr * (dot(v, v) + dot(w, w));
+        }
+      }
+    }
+    const float tot = tm.sum(acc);
+    tm.sync();
+    return 0.5f * tot;
+  };
+
+  // J^T J (packed lower) and g = J^T r at q with world poses `pose`; returns |g|.
+  auto build_normal = [&](const float* q, const float* pose) -> float {
+    for (int c = tl; c < nv; c += T) {
+      const Pose Tj = ld8(pose + 8 * cjoint[c]);
+      const float3 a = qrot(Tj.q, f3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
+      *reinterpret_cast<float4*>(colw + 8 * c) = make_float4(a.x, a.y, a.z, 0.f);
+      *reinterpret_cast<float4*>(colw + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
+    }
+    for (int t = tl; t < nt; t += T) {                                 // Jr^-1(xi), tangents.py:204-207
+      const float4 a = *reinterpret_cast<const float4*>(xi + 8 * t);
+      const float4 b = *reinterpret_cast<const float4*>(xi + 8 * t + 4);
+      const JrInv J = jr_inv_se3<9>(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y));
+      float* o = jri + 16 * t;
+      o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
+      for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
+    }
+    tm.sync();
+    // pose Jacobians J_t = diag(w) Jr^-1 blockdiag(R^T, R^T) J_lwa, stored work[t][row][c]
+    float* Jp = work;
+    for (int idx = tl; idx < nt * nv; idx += T) {
+      const int t = idx / nv, c = idx - t * nv;
+      float3 ol = f3(0.f, 0.f, 0.f), oa = f3(0.f, 0.f, 0.f);
+      if ((cmask[t] >> c) & 1ull) {
+        const float4 a4 = *reinterpret_cast<const float4*>(colw + 8 * c);
+        const float3 a = f3(a4.x, a4.y, a4.z);
+        const Pose Tee = ld8(tw + 8 * t);
+        float3 lin, ang;
+        if (ckind[c] == 0) {
+          const float4 o4 = *reinterpret_cast<const float4*>(colw + 8 * c + 4);
+          lin = cross(a, sub(Tee.t, f3(o4.x, o4.y, o4.z)));           // jacobian.py:213-215
+          ang = a;
+        } else {
+          lin = a;
+          ang = f3(0.f, 0.f, 0.f);
+        }
+        lin = qrot_inv(Tee.q, lin);                                    // pose.py:91-95
+        ang = qrot_inv(Tee.q, ang);
+        const float* o = jri + 16 * t;
+        JrInv J;
+        J.w = f3(o[0], o[1], o[2]);
+        J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
+        for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
+        jr_inv_apply(J, lin, ang, ol, oa);
+        ol = scale(ol, wp);
+        oa = scale(oa, wo);
+      }
+      float* dst = Jp + t * 6 * nv + c;
+      dst[0] = ol.x; dst[nv] = ol.y; dst[2 * nv] = ol.z;
+      dst[3 * nv] = oa.x; dst[4 * nv] = oa.y; dst[5 * nv] = oa.z;
+    }
+    tm.sync();
+    // J^T J, lanes over the packed lower triangle
+    const int ntri = tri(nv);
+    int a = 0, b = tl;
+    while (a < nv && b > a) { b -= a + 1; ++a; }
+    for (int k = tl; k < ntri; k += T) {
+      float acc = 0.f;
+      for (int t = 0; t < nt; ++t) {
+        const unsigned long long m = cmask[t];
+        if (((m >> a) & 1ull) && ((m >> b) & 1ull)) {
+          const float* Jt = Jp + t * 6 * nv;
+#pragma unroll
+          for (int r = 0; r < 6; ++r) acc = fmaf(Jt[r * nv + a], Jt[r * nv + b], acc);
+        }
+      }
+      if (a == b) {
+        if (use_rest) acc += wr * wr;                                  // regularization.py:56-64
+        if (use_limits) {                                              // limits.py:64-86
+          const int j = cjoint[a];
+          if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
+            const int iq = idxq[j];
+            if (q[iq] < lower[iq]) acc += wl * wl;
+            if (q[iq] > upper[iq]) acc += wl * wl;
+          }
+        }
+      }
+      jtj[k] = acc;
+      b += T;
+      while (a < nv && b > a) { b -= a + 1; ++a; }
+    }
+    // g = J^T r
+    float gg = 0.f;
+    for (int c = tl; c < nv; c += T) {
+      float acc = 0.f;
+      for (int t = 0; t < nt; ++t) {
+        if ((cmask[t] >> c) & 1ull) {
+          const float* Jt = Jp + t * 6 * nv + c;
+          const float* e = xi + 8 * t;  // xi = (v.x v.y v.z w.x | w.y w.z)
+          acc = fmaf(Jt[0], wp * e[0], acc);
+          acc = fmaf(Jt[nv], wp * e[1], acc);
+          acc = fmaf(Jt[2 * nv], wp * e[2], acc);
+          acc = fmaf(Jt[3 * nv], wo * e[3], acc);
+          acc = fmaf(Jt[4 * nv], wo * e[4], acc);
+          acc = fmaf(Jt[5 * nv], wo * e[5], acc);
+        }
+      }
+      if (use_rest) acc += wr * wr * dr[c];
+      if (use_limits) {
+        const int j = cjoint[c];
+        if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
+          const int iq = idxq[j];
+          if (q[iq] < lower[iq]) acc -= wl * wl * (lower[iq] - q[iq]);
+          if (q[iq] > upper[iq]) acc += wl * wl * (q[iq] - upper[iq]);
+        }
+      }
+      g[c] = acc;
+      gg += acc * acc;
+    }
+    gg = tm.sum(gg);
+    tm.sync();
+    return sqrtf(gg);
+  };
+
+  // Solve (J^T J + damp I) delta = -g.  Returns false if the factorization failed.
+  auto solve = [&](float damp) -> bool {
+    const int ld = nv + 1;
+    float* Lm = work;
+    for (int k = tl; k < tri(nv); k += T) {
+      int i = (int)((sqrtf(8.f * k + 1.f) - 1.f) * 0.5f);
+      while (tri(i + 1) <= k) ++i;
+      while (tri(i) > k) --i;
+      const int j = k - tri(i);
+      Lm[i * ld + j] = jtj[k] + (i == j ? damp : 0.f);
+    }
+    tm.sync();
+    bool ok = true;
+    for (int j = 0; j < nv; ++j) {
+      const float djj = Lm[j * ld + j];
+      if (!(djj > 0.f) || !isfinite(djj)) { ok = false; break; }
+      const float dj = sqrtf(djj);
+      const float inv = 1.f / dj;
+      tm.sync();
+      if (tl == 0) Lm[j * ld + j] = dj;
+      for (int i = j + 1 + tl; i < nv; i += T) Lm[i * ld + j] *= inv;
+      tm.sync();
+      const int m = nv - j - 1;
+      const int ne = tri(m);
+      for (int e = tl; e < ne; e += T) {
+        int r = (int)((sqrtf(8.f * e + 1.f) - 1.f) * 0.5f);
+        while (tri(r + 1) <= e) ++r;
+        while (tri(r) > e) --r;
+        const int c = e - tri(r);
+        const int i = j + 1 + r, k = j + 1 + c;
+        Lm[i * ld + k] = fmaf(-Lm[i * ld + j], Lm[k * ld + j], Lm[i * ld + k]);
+      }
+      tm.sync();
+    }
+    tm.sync();
+    if (!ok) return false;
+    // forward: L y = -g  (y kept in delta[]), then back: L^T dx = y
+    for (int i = tl; i < nv; i += T) delta[i] = -g[i];
+    tm.sync();
+    for (int j = 0; j < nv; ++j) {
+      const float yj = delta[j] / Lm[j * ld + j];
+      tm.sync();
+      if (tl == 0) delta[j] = yj;
+      for (int i = j + 1 + tl; i < nv; i += T) delta[i] = fmaf(-Lm[i * ld + j], yj, delta[i]);
+      tm.sync();
+    }
+    for (int j = nv - 1; j >= 0; --j) {
+      const float xj = delta[j] / Lm[j * ld + j];
+      tm.sync();
+      if (tl == 0) delta[j] = xj;
+      for (int i = tl; i < j; i += T) delta[i] = fmaf(-Lm[j * ld + i], xj, delta[i]);
+      tm.sync();
+    }
+    return true;
+  };
+
+  // x_new = clamp(integrate(x, delta))
+  auto retract = [&]() {
+    for (int j = tl; j < nj; j += T) {
+      const int jt = jtype[j];
+      const int iq = idxq[j], iv = idxv[j];
+      if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
+        xn[iq] = fminf(fmaxf(x[iq] + delta[iv], lower[iq]), upper[iq]);
+      } else if (jt == BR_JOINT_FREE_FLYER) {
+        const Pose a{f3(x[iq], x[iq + 1], x[iq + 2]), make_float4(x[iq + 3], x[iq + 4], x[iq + 5], x[iq + 6])};
+        Pose n = compose(a, se3_exp(f3(delta[iv], delta[iv + 1], delta[iv + 2]),
+                                    f3(delta[iv + 3], delta[iv + 4], delta[iv + 5])));
+        n.q = qnormalize(n.q);
+        const float v7[7] = {n.t.x, n.t.y, n.t.z, n.q.x, n.q.y, n.q.z, n.q.w};
+        for (int k = 0; k < 7; ++k) xn[iq + k] = fminf(fmaxf(v7[k], lower[iq + k]), upper[iq + k]);
+      }
+    }
+    tm.sync();
+  };
+
+  // ---- the LM / GN loop (levenberg_marquardt.py:83-135, gauss_newton.py:27-76) ----
+  const bool gn = S.optimizer == BR_OPT_GN;
+  float* pose = fk(x);
+  float cost = residual(x, pose);
+  float lam = gn ? 0.f : S.lam0;
+  float gnorm = 0.f;
+  bool need_jac = true;
+  int flags = isfinite(cost) ? 0 : BR_IK_FLAG_NONFINITE;
+  int status = BR_IK_MAXITER;
+  int it = 0;
+  for (; it < S.max_iter; ++it) {
+    if (need_jac) {
+      gnorm = build_normal(x, pose);
+      need_jac = false;
+    }
+    const float damp = gn ? S.gn_eps : lam;
+    bool ok = solve(damp);
+    if (!ok) {
+      // float32 factorization failed: add diagonal regularisation (x10 per retry)
+      flags |= BR_IK_FLAG_REGULARIZED;
+      float extra = 1e-6f;
+      for (int k = 0; k < 6 && !ok; ++k, extra *= 10.f) ok = solve(damp + extra);
+      if (!ok) {
+        for (int i = tl; i < nv; i += T) delta[i] = 0.f;
+        tm.sync();
+      }
+    }
+    retract();
+    pose = fk(xn);
+    const float cn = residual(xn, pose);
+    if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
+    if (gn) {
+      for (int i = tl; i < nq; i += T) x[i] = xn[i];
+      tm.sync();
+      cost = cn;
+      need_jac = true;
+      if (gnorm < S.tol) { status = BR_IK_CONVERGED; ++it; break; }
+    } else if (cn < cost) {
+      for (int i = tl; i < nq; i += T) x[i] = xn[i];
+      tm.sync();
+      cost = cn;
+      lam = fmaxf(lam / S.factor, S.lam_min);
+      need_jac = true;
+      if (gnorm < S.tol) { status = BR_IK_CONVERGED; ++it; break; }
+    } else {
+      lam = fminf(lam * S.factor, S.lam_max);
+    }
+  }
+  // ---- results ------------------------------------------------------------
+  for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = x[i];
+  if (tl == 0) {
+    P.r.iters[prob] = it;
+    P.r.status[prob] = status | (flags << 8);
+    P.r.cost[prob] = cost;
+  }
+  tm.sync();
+}
+
+template <int T>
+__device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, int count, float* wsm, int lane) {
+  const int team = lane / T;
+  Team<T> tm;
+  tm.tl = lane % T;
+  tm.mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (team * T));
+  const br_tree_t& tree = P.trees[cls];
+  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets);
+  if (team < count) {
+    const int prob = P.b.order[first + team];
+    solve_problem<T>(P, tree, prob, wsm + team * L.total, tm);
+  }
+}
+
+__global__ void lm_solve_kernel(const LmParams P) {
+  extern __shared__ __align__(16) float smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  float* wsm = smem + (size_t)warp * P.warp_floats;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(P.queue, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= P.b.n_items) break;
+    const int first = P.b.items[3 * item], count = P.b.items[3 * item + 1], cls = P.b.items[3 * item + 2];
+    switch (P.team[cls]) {
+      case 8: run_item<8>(P, cls, first, count, wsm, lane); break;
+      case 16: run_item<16>(P, cls, first, count, wsm, lane); break;
+      default: run_item<32>(P, cls, first, count, wsm, lane); break;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace br
+
+using namespace br;
+
+extern "C" int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets) {
+  if (!tree || max_targets < 0) return BR_EINVAL;
+  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets).total;
+}
+
+extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
+                           int32_t warps_per_cta, void* scratch, int64_t scratch_bytes, void* stream) {
+  if (!batch || !settings || !result) return BR_EINVAL;
+  const br_ik_batch_t& b = *batch;
+  if (b.n_problems < 0 || b.n_items < 0 || b.n_classes < 1) return BR_EINVAL;
+  if (b.n_classes > BR_MAX_IK_CLASSES || b.max_targets > BR_MAX_IK_TARGETS) return BR_ETOOBIG;
+  if (b.max_targets < 1 || !b.trees || !b.team_size) return BR_EINVAL;
+  if (!scratch || scratch_bytes < BR_LM_SCRATCH_BYTES) return BR_EINVAL;
+  if (b.n_problems == 0 || b.n_items == 0) return BR_OK;
+  if (!b.items || !b.order || !b.n_targets || !b.frames || !b.targets || !b.q_offset || !b.x0 || !b.q_rest)
+    return BR_EINVAL;
+  if (!result->x || !result->iters || !result->status || !result->cost) return BR_EINVAL;
+  if (settings->max_iter < 0) return BR_EINVAL;
+  if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
+  LmParams p = {};
+  p.s = *settings;
+  p.b = b;
+  p.r = *result;
+  int warp_floats = 0;
+  for (int c = 0; c < b.n_classes; ++c) {
+    const int st = validate_tree(&b.trees[c]);
+    if (st) return st;
+    const int T = b.team_size[c];
+    if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
+    p.trees[c] = b.trees[c];
+    p.team[c] = T;
+    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets).total;
+    if (f > warp_floats) warp_floats = f;
+  }
+  p.warp_floats = warp_floats;
+  p.queue = reinterpret_cast<int32_t*>(scratch);
+  const DeviceInfo& dev = device_info();
+  int wpc = warps_per_cta;
+  size_t bytes = (size_t)wpc * warp_floats * sizeof(float);
+  while ((int64_t)bytes > dev.max_smem_optin && wpc > 1) {
+    wpc >>= 1;
+    bytes = (size_t)wpc * warp_floats * sizeof(float);
+  }
+  if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
+  static int configured[16] = {0};
+  if ((int)bytes > configured[dev.device & 15]) {
+    cudaError_t e = cudaFuncSetAttribute(lm_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return (int)e;
+    configured[dev.device & 15] = (int)bytes;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lm_solve_kernel, wpc * kWarp, bytes);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t need = (b.n_items + wpc - 1) / wpc;
+  const int64_t cap = (int64_t)per_sm * dev.sms;
+  const int grid = (int)(need < cap ? need : cap);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int32_t), s);
+  if (e != cudaSuccess) return (int)e;
+  lm_solve_kernel<<<grid, wpc * kWarp, bytes, s>>>(p);
+  return (int)cudaGetLastError();
+}

@@ -1,0 +1,185 @@
+/*
+ * br_b200.h — C ABI of the B200 (sm_100a) kinematics / LM-IK library (libbr_b200.so).
+ *
+ * Plain pointers and sizes only.  Every array argument is DEVICE memory unless
+ * its comment says "host".  All float data is float32; poses are stored as
+ * [tx, ty, tz, qx, qy, qz, qw] (scalar-last quaternion) and tangents as
+ * [vx, vy, vz, wx, wy, wz], exactly as in BetterRobot
+ * (src/better_robot/lie/_torch_native_backend.py:7-9).
+ *
+ * Every entry point enqueues work on `stream` (a cudaStream_t, NULL = legacy
+ * default stream), does not synchronise, allocates no memory and returns a
+ * status: BR_OK, a negative BR_E* argument error, or a positive cudaError_t.
+ *
+ * Which reference interface each entry point replaces is given beside it
+ * (paths relative to BetterRobot's repository).
+ */
+#ifndef BR_B200_H
+#define BR_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BR_API __attribute__((visibility("default")))
+#else
+#define BR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define BR_OK 0
+#define BR_EINVAL (-1)      /* null pointer, negative size, bad enum            */
+#define BR_ETOOBIG (-2)     /* njoints > 64, nv > 64, more than 64 targets ...   */
+#define BR_EALIGN (-3)      /* a pointer is not 4-byte (float) aligned           */
+
+/* ---- limits ---------------------------------------------------------- */
+#define BR_MAX_JOINTS 64    /* support sets are 64-bit masks                     */
+#define BR_MAX_NV 64
+#define BR_MAX_NQ 128
+#define BR_MAX_TARGETS 64   /* frames (or joints) per Jacobian launch            */
+
+/* ---- joint kinds in the tree table ----------------------------------- */
+#define BR_JOINT_FIXED 0        /* universe, fixed                                */
+#define BR_JOINT_REVOLUTE 1     /* revolute_rx/ry/rz/unaligned: rotation about axis */
+#define BR_JOINT_PRISMATIC 2    /* prismatic_px/py/pz/unaligned: translation along axis */
+#define BR_JOINT_FREE_FLYER 3   /* nq = 7 [t, quat], nv = 6, transform = normalize(q) */
+
+/* ---- Jacobian reference frames (kinematics/__init__.py:24-37) --------- */
+#define BR_REF_WORLD 0
+#define BR_REF_LOCAL_WORLD_ALIGNED 1
+#define BR_REF_LOCAL 2
+
+/*
+ * Device-resident description of one kinematic tree ("tree table"), packed
+ * once per Model by the host (betterrobot_b200/tree.py).  Joint j's parent
+ * precedes it; joint 0 is the universe.  Replaces the per-joint Python
+ * dispatch over model.joint_models / model.topo_order
+ * (src/better_robot/kinematics/forward.py:110-129).
+ */
+typedef struct br_tree {
+    int32_t njoints, nq, nv, nframes;
+    int32_t rounds;           /* ceil(log2(max joint depth)): pointer-jumping rounds */
+    int32_t reserved[3];
+    const int32_t* parent;          /* [njoints]   -1 for the universe            */
+    const int32_t* jtype;           /* [njoints]   BR_JOINT_*                      */
+    const int32_t* idx_q;           /* [njoints]                                   */
+    const int32_t* idx_v;           /* [njoints]                                   */
+    const float* axis;              /* [njoints*4] local axis (x, y, z, 0)         */
+    const float* placement;         /* [njoints*8] parent->joint SE3 + pad         */
+    const uint64_t* support;        /* [njoints]   bit k: joint k is ancestor-or-self */
+    const int32_t* frame_parent;    /* [nframes]                                   */
+    const float* frame_placement;   /* [nframes*8]                                 */
+    const int32_t* col_joint;       /* [nv]        joint owning tangent column c   */
+    const int32_t* col_kind;        /* [nv]        0 rotation about, 1 translation along col_axis */
+    const float* col_axis;          /* [nv*4]      column axis in its joint's frame */
+    const float* lower;             /* [nq]        position limits (+-inf allowed) */
+    const float* upper;             /* [nq]                                        */
+} br_tree_t;
+
+/*
+ * Forward kinematics for `batch` configurations q[batch, nq].
+ * Outputs (each may be NULL): joint_pose_world[batch, njoints, 7] (oMi),
+ * joint_pose_local[batch, njoints, 7] (liMi), frame_pose_world[batch, n_frames, 7]
+ * for the frame ids in `frame_ids` (HOST array of n_frames <= 64 ids).
+ * Replaces KinematicsOps.forward_kinematics (src/better_robot/backends/protocol.py:58-62,
+ * implemented by src/better_robot/kinematics/forward.py:73-135) and
+ * update_frame_placements (forward.py:194-219).
+ */
+BR_API int br_forward_kinematics(const br_tree_t* tree, const float* q, int64_t batch,
+                          float* joint_pose_world, float* joint_pose_local,
+                          const int32_t* frame_ids, int32_t n_frames, float* frame_pose_world,
+                          void* stream);
+
+/*
+ * Fused FK + frame Jacobians straight from q[batch, nq]: for each id in the HOST
+ * array `targets` (n_targets <= 64; id >= 0 is a frame id, id < 0 means joint
+ * (-id - 1) with identity placement) writes jacobians[batch, n_targets, 6, nv] in
+ * reference frame `reference` (BR_REF_*), and if non-NULL target_pose_world
+ * [batch, n_targets, 7].  Replaces forward_kinematics(..., compute_frames=True)
+ * followed by get_frame_jacobian per frame (src/better_robot/kinematics/jacobian.py:129-227).
+ */
+BR_API int br_frame_jacobians(const br_tree_t* tree, const float* q, int64_t batch,
+                       const int32_t* targets, int32_t n_targets, int32_t reference,
+                       float* target_pose_world, float* jacobians, void* stream);
+
+/*
+ * Frame (or joint) Jacobians from already computed world joint placements
+ * joint_pose_world[batch, njoints, 7] (Data.joint_pose_world), same target
+ * encoding and output layout as br_frame_jacobians.  Replaces get_frame_jacobian
+ * on a populated Data (jacobian.py:129-227) and, with targets = all joints and
+ * BR_REF_WORLD, compute_joint_jacobians (jacobian.py:30-97, protocol.py:64-68).
+ */
+BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joint_pose_world, int64_t batch,
+                                  const int32_t* targets, int32_t n_targets, int32_t reference,
+                                  float* jacobians, void* stream);
+
+/* ==== batched Levenberg-Marquardt / Gauss-Newton IK ===================== */
+#define BR_MAX_IK_CLASSES 8     /* distinct robots in one launch                   */
+#define BR_MAX_IK_TARGETS 8     /* pose targets per problem                        */
+#define BR_LM_SCRATCH_BYTES 16  /* device scratch br_lm_solve needs (work queue)   */
+#define BR_OPT_LM 0
+#define BR_OPT_GN 1
+#define BR_IK_CONVERGED 0       /* status & 0xff                                   */
+#define BR_IK_MAXITER 1
+#define BR_IK_FLAG_NONFINITE 1  /* (status >> 8) bits: a non-finite cost was seen   */
+#define BR_IK_FLAG_REGULARIZED 2 /* float32 Cholesky needed extra diagonal damping */
+
+/* Solver settings: LevenbergMarquardt(lam0, factor, tol) with Adaptive damping
+ * bounds [lam_min, lam_max] (optim/strategies/adaptive.py:19-25), GaussNewton eps,
+ * and the solve_ik cost weights (tasks/ik.py:38-48; limit/rest are the CostStack
+ * item weights). */
+typedef struct br_ik_settings {
+    float lam0, factor, tol, lam_min, lam_max, gn_eps;
+    float pos_weight, ori_weight, limit_weight, rest_weight;
+    int32_t max_iter;
+    int32_t optimizer;          /* BR_OPT_LM or BR_OPT_GN                          */
+} br_ik_settings_t;
+
+/* A packed batch of independent IK problems over up to 8 robot classes. */
+typedef struct br_ik_batch {
+    int32_t n_problems, max_targets, n_classes, n_items;
+    const br_tree_t* trees;     /* HOST array [n_classes] (its tables live on the device) */
+    const int32_t* team_size;   /* HOST array [n_classes]: lanes per problem, 8/16/32 */
+    const int32_t* items;       /* [n_items*3] work items: first slot in order[], count <= 32/team, class */
+    const int32_t* order;       /* [n_problems] problem index of each slot          */
+    const int32_t* n_targets;   /* [n_problems] 1..max_targets                       */
+    const int32_t* frames;      /* [n_problems*max_targets] frame ids of the class  */
+    const float* targets;       /* [n_problems*max_targets*7] target poses          */
+    const int64_t* q_offset;    /* [n_problems] float offset of the problem's q     */
+    const float* x0;            /* packed initial configurations                    */
+    const float* q_rest;        /* packed rest configurations (RestResidual q_rest) */
+} br_ik_batch_t;
+
+typedef struct br_ik_result {
+    float* x;                   /* packed solutions, same offsets as x0             */
+    int32_t* iters;             /* [n_problems] completed iterations (SolverState.iters) */
+    int32_t* status;            /* [n_problems] BR_IK_* | flags << 8                */
+    float* cost;                /* [n_problems] final 0.5 |r|^2                     */
+} br_ik_result_t;
+
+/*
+ * Solve every problem of `batch` in one persistent launch (one team of lanes per
+ * problem, see lm_solve.cu).  `scratch` is caller-provided device memory of at
+ * least BR_LM_SCRATCH_BYTES; the entry point zeroes it on `stream` before the
+ * launch.  Replaces solve_ik (src/better_robot/tasks/ik.py:150-266) called once
+ * per problem, i.e. LevenbergMarquardt.minimize / GaussNewton.minimize
+ * (optim/optimizers/levenberg_marquardt.py:61-135, gauss_newton.py:27-76) over
+ * the pose + limit + rest CostStack.
+ */
+BR_API int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
+                       int32_t warps_per_cta, void* scratch, int64_t scratch_bytes, void* stream);
+
+/* Shared-memory floats one problem of `tree` with `max_targets` targets needs
+ * (for choosing team sizes and warps per CTA). No reference counterpart. */
+BR_API int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets);
+
+/* Library build information (for logging): returns a static string. */
+BR_API const char* br_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BR_B200_H */

@@ -1,0 +1,85 @@
+"""CPU-side checks: the C-ABI library loads and exports every declared symbol; the tree packer."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from betterrobot_b200 import _lib, synthetic as syn
+from betterrobot_b200.tree import TreeArrays
+
+from conftest import REPO
+
+
+def _declared_symbols():
+    names = []
+    for fn in os.listdir(os.path.join(REPO, "include")):
+        if fn.endswith(".h"):
+            src = open(os.path.join(REPO, "include", fn)).read()
+            names += re.findall(r"^\s*BR_API\s+(?:int|int64_t|const char\s*\*)\s+(br_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = _declared_symbols()
+    assert "br_frame_jacobians" in names and "br_forward_kinematics" in names
+    # the ctypes table covers every declared symbol and nothing else
+    assert sorted(_lib.SIGNATURES) == names
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    for name in _declared_symbols():
+        assert hasattr(lib, name), name
+    assert b"sm_100a" in lib.br_version()
+
+
+def test_tree_struct_layout_matches_header():
+    # 5 int32 + 3 reserved, then 14 pointers
+    assert ctypes.sizeof(_lib.BrTree) == 32 + 14 * 8
+    assert _lib.BrTree.parent.offset == 32
+
+
+@pytest.mark.parametrize("spec", [syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()])
+def test_tree_arrays(spec):
+    m = syn.model_from_spec(spec)
+    a = TreeArrays(m)
+    assert a.nj == m.njoints and a.nv == m.nv
+    for j in range(m.njoints):
+        sup = set(m.supports[j])
+        bits = {k for k in range(m.njoints) if (int(a.support[j]) >> k) & 1}
+        assert bits == sup
+    depth = max(len(s) - 1 for s in m.supports)
+    assert 2 ** a.rounds >= depth + 1 and 2 ** max(a.rounds - 1, 0) < depth + 1
+    for c in range(m.nv):
+        j = a.col_joint[c]
+        assert m.idx_vs[j] <= c < m.idx_vs[j] + m.nvs[j]
+    buf, offs = a.blob()
+    assert all(o % 16 == 0 for o in offs.values())
+
+
+def test_unsupported_joint_kind_rejected():
+    from betterrobot_b200.exceptions import UnsupportedJointError
+    from betterrobot_b200.model import joint_model
+    with pytest.raises(UnsupportedJointError):
+        joint_model("spherical")
+
+
+def test_cpu_tensor_rejected_without_fallback():
+    """No CPU fallback: a CPU tensor never reaches a kernel and raises."""
+    from betterrobot_b200 import forward_kinematics
+    from betterrobot_b200.exceptions import BackendNotAvailableError, DeviceMismatchError
+    m = syn.model_from_spec(syn.chain_spec())
+    with pytest.raises((BackendNotAvailableError, DeviceMismatchError)):
+        forward_kinematics(m, torch.zeros(4, m.nq))
+
+
+def test_shape_error_before_device_check():
+    from betterrobot_b200 import forward_kinematics
+    from betterrobot_b200.exceptions import ShapeError
+    m = syn.model_from_spec(syn.chain_spec())
+    with pytest.raises(ShapeError):
+        forward_kinematics(m, torch.zeros(4, m.nq + 1))
