@@ -2,24 +2,33 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Workloads (synthetic, seeded; no dataset exists for this path):
+Headline workload (synthetic and seeded — the path has no dataset): the uneven
+batched IK mix, 8,192 independent problems in one persistent launch —
+40% 7-DOF chains, 30% 14-DOF dual-arm trees, 30% 36-DOF free-flyer humanoids;
+each with 1-6 pose targets (a random subset of 6 candidate frames) generated by
+FK of a random q*; q0 = q* + N(0, 0.3) noise; LM <= 100 iterations, damping
+1e-3 adapted x10 / ÷10, tol 1e-6 on |J^T r|; limit weight 0.1, rest weight 1e-3.
+A step solves the whole batch once.
 
-* headline — batched LM-IK on the uneven mix (8,192 problems: 40% 7-DOF chains,
-  30% 14-DOF dual-arm trees, 30% 36-DOF free-flyer humanoids; 1-6 pose targets
-  each from FK of a random q*; q0 = q* + N(0, 0.3) noise; <= 100 LM iterations,
-  damping 1e-3 x10/÷10, tol 1e-6).  value = problems reaching <= 1e-4 m and
-  <= 1e-4 rad final pose error per second.
-* roofline — fused FK + frame Jacobians on the free-flyer humanoid (B = 65,536,
-  12 frames, J [B,12,6,36] + oMf [B,12,7] float32), HBM bound.
+  value  = problems whose final pose error is <= 1e-4 m and <= 1e-4 rad on every
+           target, per second, inputs resident in HBM (L2 flushed between steps);
+  e2e    = the same through the public API with pinned host inputs: each step copies
+           targets and q0 host->device, solves, copies q / status / iterations back;
+  plain_gpu = the same method as plain per-op PyTorch on the same GPU;
+  roofline  = the fused FK + frame-Jacobian kernel on the free-flyer humanoid
+           (B = 65,536, 12 frames) against the measured HBM copy bandwidth.
 
-Multi-GPU: every problem is independent, so N GPUs run N replicas on disjoint
-shards with no collective on the data path (weak scaling).
+Multi-GPU: problems are independent, so N GPUs run N replicas on disjoint
+problem sets with no data-path collective (weak scaling); time is the max over
+ranks.  ``--impl reference`` times BetterRobot's algorithm on the host CPU (the
+float64 port of its serial LM) on a bounded sample of the same workload.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
+import multiprocessing as mp
 import os
 import subprocess
 import sys
@@ -27,15 +36,84 @@ import tempfile
 import time
 
 import numpy as np
-import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
+N_PROBLEMS = 8192
+MAX_ITER = 100
+SETTINGS = dict(lam0=1e-3, factor=10.0, tol=1e-6, rest_weight=1e-3, limit_weight=0.1)
 FKJ_BATCH = 65536
 FKJ_BYTES_PER_CONFIG = 4 * (37 + 12 * 7 + 12 * 6 * 36)  # q read + oMf + J written = 10,852 B
+REACH_TOL = 1e-4
+CANDIDATES = {
+    "humanoid": [f"track{i}" for i in range(6)],
+    "dual_arm": ["ee_l", "ee_r", "body_l_link5", "body_r_link5", "body_l_link3", "body_r_link3"],
+    "chain7": ["ee", "body_link7", "body_link6", "body_link5", "body_link4", "body_link3"],
+}
 
 
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def class_specs():
+    from betterrobot_b200 import synthetic as syn
+    return [("humanoid", syn.humanoid_spec()), ("dual_arm", syn.dual_arm_spec()), ("chain7", syn.chain_spec())]
+
+
+def make_workload(n_problems: int, seed: int):
+    """Per class: models, frame ids (P_c, 6) (first n_targets used), n_targets, q* and q0 (float64)."""
+    import torch
+    from betterrobot_b200 import synthetic as syn
+    mix = syn.ik_uneven_mix(n_problems, seed)
+    rng = np.random.default_rng(seed + 1)
+    out = []
+    for ci, (name, spec) in enumerate(class_specs()):
+        m = syn.model_from_spec(spec)
+        m64 = syn.model_from_spec(spec, dtype=torch.float64)
+        nts = np.array([k for lab, k in mix if lab == name], np.int32)
+        P = len(nts)
+        cand = np.array([m.frame_id(f) for f in CANDIDATES[name]], np.int32)
+        frames = np.stack([cand[rng.permutation(6)] for _ in range(P)]).astype(np.int32)
+        q_star = syn.random_q(m64, P, seed + 10 + ci, rev_range=2.5, base_translation=0.5)
+        q0 = syn.noisy_start(m64, q_star, 0.3, seed + 20 + ci)
+        out.append({"name": name, "model": m, "model64": m64, "frames": frames, "n_targets": nts,
+                    "q_star": q_star, "q0": q0})
+    return out
+
+
+def gpu_targets(wl):
+    """Target poses = FK(q*) of each problem's frames, by the library's own FK kernel."""
+    import torch
+    import betterrobot_b200 as br
+    for c in wl:
+        d = br.forward_kinematics(c["model"], c["q_star"].float().cuda(), compute_frames=True)
+        idx = torch.from_numpy(c["frames"]).long().cuda()
+        c["targets"] = torch.gather(d.frame_pose_world, 1, idx[..., None].expand(-1, -1, 7)).contiguous()
+
+
+def gpu_reach(wl, q_list):
+    """Problems whose every target is reached within REACH_TOL (m and rad), via the library FK."""
+    import torch
+    import betterrobot_b200 as br
+    total = 0
+    for c, q in zip(wl, q_list):
+        d = br.forward_kinematics(c["model"], q, compute_frames=True, check_quaternion=False)
+        idx = torch.from_numpy(c["frames"]).long().cuda()
+        T = torch.gather(d.frame_pose_world, 1, idx[..., None].expand(-1, -1, 7)).double()
+        tg = c["targets"].double()
+        pe = (T[..., :3] - tg[..., :3]).norm(dim=-1)
+        dq = torch.abs((T[..., 3:] * tg[..., 3:]).sum(-1)).clamp(max=1.0)
+        re = 2.0 * torch.acos(dq)
+        k = torch.arange(6, device=q.device)[None, :] < torch.from_numpy(c["n_targets"]).cuda()[:, None]
+        ok = ((pe <= REACH_TOL) & (re <= REACH_TOL)) | ~k
+        total += int(ok.all(dim=1).sum())
+    return total
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
 def _peaks():
     p = os.path.join(HERE, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -52,9 +130,7 @@ class ClockSampler:
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.path = None
+        self.index, self.proc, self.path = index, None, None
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -65,7 +141,7 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
-        time.sleep(0.25)
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *exc):
@@ -79,30 +155,36 @@ class ClockSampler:
     def summary(self):
         if self.path is None or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.count(",") >= 8]
+        rows = [[x.strip() for x in r.split(",")] for r in open(self.path).read().strip().splitlines()
+                if r.count(",") >= 8]
         os.unlink(self.path)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 
 
 def dist_setup():
+    import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    else:
-        if torch.cuda.is_available():
-            torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -112,36 +194,134 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def reduce(x: float, world: int, op: str) -> float:
     if world == 1:
         return x
+    import torch
     import torch.distributed as dist
     t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
 
-def sum_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+# ---------------------------------------------------------------------------
+# fused LM-IK (headline)
+# ---------------------------------------------------------------------------
+def bench_ik(steps: int, warmup: int, seed: int):
+    import torch
+    from betterrobot_b200 import ik as bik
+    wl = make_workload(N_PROBLEMS, seed)
+    gpu_targets(wl)
+    settings = bik.settings_from(
+        bik.IKCostConfig(rest_weight=SETTINGS["rest_weight"], limit_weight=SETTINGS["limit_weight"]),
+        bik.OptimizerConfig(max_iter=MAX_ITER, lam0=SETTINGS["lam0"], factor=SETTINGS["factor"], tol=SETTINGS["tol"]))
+    pk = bik.PackedIK([c["model"] for c in wl], [c["frames"] for c in wl], [c["n_targets"] for c in wl],
+                      warps_per_cta=4)
+    tg_dev = [c["targets"] for c in wl]
+    q0_dev = [c["q0"].float().cuda() for c in wl]
+    pk.set_inputs(tg_dev, q0_dev)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda")  # > 126 MB L2
+    for _ in range(warmup):
+        pk.solve(settings)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pk.solve(settings)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.mean(times))
+    reached = gpu_reach(wl, [pk.q_of(c).clone() for c in range(len(wl))])
+    conv = int(((pk.status & 0xFF) == 0).sum())
+    iters = pk.iters.float()
+    # e2e: pinned host inputs -> solve -> pinned host outputs, every step
+    h_tg = [t.cpu().pin_memory() for t in tg_dev]
+    h_q0 = [q.cpu().pin_memory() for q in q0_dev]
+    h_x = torch.empty(pk.q_total).pin_memory()
+    h_st = torch.empty(pk.P, dtype=torch.int32).pin_memory()
+    h_it = torch.empty(pk.P, dtype=torch.int32).pin_memory()
+    h2d = sum(t.numel() * 4 for t in h_tg) + sum(q.numel() * 4 for q in h_q0)
+    d2h = pk.q_total * 4 + pk.P * 8
+
+    def e2e_step():
+        pk.set_inputs(h_tg, h_q0)
+        pk.solve(settings)
+        h_x.copy_(pk.x, non_blocking=True)
+        h_st.copy_(pk.status, non_blocking=True)
+        h_it.copy_(pk.iters, non_blocking=True)
+    for _ in range(warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    et = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        et.append(e0.elapsed_time(e1))
+    return {"ms": ms, "reached": reached, "converged": conv, "problems": pk.P, "iters_mean": float(iters.mean()),
+            "e2e_ms": float(np.mean(et)), "h2d": h2d, "d2h": d2h, "launches": steps, "wl": wl}
+
+
+def bench_plain_gpu(wl):
+    """The same batched LM as plain per-op PyTorch on this GPU (one timed solve after one warm-up)."""
+    import torch
+    from baseline.plain_gpu import PlainLM
+    runs = []
+    for c in wl:
+        m = c["model"]
+        lm = PlainLM(m, torch.device("cuda"))
+        cand = [m.frame_id(f) for f in CANDIDATES[c["name"]]]
+        P = len(c["n_targets"])
+        pos = {f: i for i, f in enumerate(cand)}
+        T = torch.zeros(P, 6, 7, device="cuda")
+        T[..., 6] = 1.0
+        mask = torch.zeros(P, 6, device="cuda")
+        fr = c["frames"]
+        tg = c["targets"]
+        for k in range(6):
+            col = torch.tensor([pos[int(f)] for f in fr[:, k]], device="cuda")
+            sel = torch.from_numpy(c["n_targets"] > k).cuda()
+            rows = torch.arange(P, device="cuda")[sel]
+            T[rows, col[sel]] = tg[sel, k]
+            mask[rows, col[sel]] = 1.0
+        q0 = c["q0"].float().cuda()
+        qr = m.q_neutral.float().cuda().expand(P, -1)
+        runs.append((lm, cand, T, mask, q0, qr))
+    w = (1.0, 1.0, SETTINGS["limit_weight"], SETTINGS["rest_weight"])
+    kw = dict(weights=w, lam0=SETTINGS["lam0"], factor=SETTINGS["factor"], tol=SETTINGS["tol"], max_iter=MAX_ITER)
+    for lm, cand, T, mask, q0, qr in runs:  # warm-up (allocator, cuBLAS/cuSOLVER handles)
+        lm.solve(cand, T[:64], mask[:64], q0[:64], qr[:64], **{**kw, "max_iter": 3})
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    qs = []
+    for lm, cand, T, mask, q0, qr in runs:
+        q, conv, iters = lm.solve(cand, T, mask, q0, qr, **kw)
+        qs.append(q)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    reached = gpu_reach(wl, qs)
+    return {"sec": sec, "reached": reached}
 
 
 # ---------------------------------------------------------------------------
 # FK + frame Jacobians (roofline workload)
 # ---------------------------------------------------------------------------
 def bench_fkj(steps: int, warmup: int, seed: int = 1):
-    import betterrobot_b200 as br
+    import torch
     from betterrobot_b200 import synthetic as syn
     from betterrobot_b200.kinematics import frame_jacobians_into
-
     m = syn.model_from_spec(syn.humanoid_spec())
     m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
     fids = syn.op_frame_ids(m)
-    n_buf = 16  # 16 distinct q buffers (155 MB) > 126 MB L2: every step reads q from HBM
+    n_buf = 16  # 16 distinct q buffers (155 MB) > 126 MB L2: every launch reads q from HBM
     qs = [syn.random_q(m64, FKJ_BATCH, seed + i, rev_range=2.5, base_translation=1.0).float().cuda()
           for i in range(n_buf)]
     J = torch.empty(FKJ_BATCH, len(fids), 6, m.nv, device="cuda")
@@ -157,37 +337,153 @@ def bench_fkj(steps: int, warmup: int, seed: int = 1):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    return {"ms_per_launch": ms, "configs": FKJ_BATCH, "bytes": FKJ_BATCH * FKJ_BYTES_PER_CONFIG,
-            "gbs": FKJ_BATCH * FKJ_BYTES_PER_CONFIG / (ms * 1e-3) / 1e9, "launches": steps}
+    return {"ms_per_launch": ms, "gbs": FKJ_BATCH * FKJ_BYTES_PER_CONFIG / (ms * 1e-3) / 1e9, "launches": steps}
 
 
+# ---------------------------------------------------------------------------
+# CPU: BetterRobot's algorithm (float64 port of its serial LM) on host cores
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    import torch
+    torch.set_num_threads(1)
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from oracle import ik as oik, kinematics as K
+    from betterrobot_b200 import synthetic as syn
+    name, idx, seed = args
+    wl = {c["name"]: c for c in make_workload(N_PROBLEMS, seed)}
+    c = wl[name]
+    m64 = c["model64"]
+    s = oik.IKSettings(lam0=SETTINGS["lam0"], factor=SETTINGS["factor"], tol=SETTINGS["tol"], max_iter=MAX_ITER,
+                       rest_weight=SETTINGS["rest_weight"], limit_weight=SETTINGS["limit_weight"])
+    t0 = time.perf_counter()
+    reached = 0
+    for p in idx:
+        k = int(c["n_targets"][p])
+        fids = [int(f) for f in c["frames"][p, :k]]
+        oMi, _ = K.forward_kinematics(m64, c["q_star"].numpy()[p:p + 1])
+        T = K.frame_placements(m64, oMi, fids)
+        out = oik.solve(m64, fids, T, c["q0"].numpy()[p:p + 1], s)   # one problem per call, as solve_ik
+        pe, re = oik.pose_errors(m64, out.q, fids, T)
+        reached += int(pe[0] <= REACH_TOL and re[0] <= REACH_TOL)
+    return reached, time.perf_counter() - t0, len(idx)
+
+
+def cpu_baseline(seed: int, per_class=(12, 9, 9), cores: int | None = None, pool=None):
+    """Serial float64 LM (one problem per call, like solve_ik) on a stratified sample, all host cores."""
+    cores = cores or len(os.sched_getaffinity(0))
+    names = [n for n, _ in class_specs()]
+    frac = {"humanoid": 0.3, "dual_arm": 0.3, "chain7": 0.4}
+    rng = np.random.default_rng(seed + 5)
+    wl = {c["name"]: c for c in make_workload(N_PROBLEMS, seed)}
+    tasks, weights = [], {}
+    for name, n in zip(names, per_class):
+        P = len(wl[name]["n_targets"])
+        pick = rng.choice(P, size=n, replace=False)
+        chunks = np.array_split(pick, max(1, min(n, cores)))
+        tasks += [(name, [int(i) for i in ch], seed) for ch in chunks if len(ch)]
+        weights[name] = (n, frac[name])
+    t0 = time.perf_counter()
+    if pool is None:
+        with mp.get_context("spawn").Pool(min(cores, len(tasks))) as own:
+            res = own.map(_cpu_worker, tasks)
+    else:
+        res = pool.map(_cpu_worker, tasks)
+    wall = time.perf_counter() - t0
+    cpu_sec = sum(r[1] for r in res)
+    # per-class success rate and seconds per solve, extrapolated to the 8,192-problem mix
+    by = {n: [0, 0.0, 0] for n in names}
+    for (name, _, _), r in zip(tasks, res):
+        by[name][0] += r[0]
+        by[name][1] += r[1]
+        by[name][2] += r[2]
+    n_full = {n: len(wl[n]["n_targets"]) for n in names}
+    reached_full = sum(by[n][0] / by[n][2] * n_full[n] for n in names)
+    cpu_seconds_full = sum(by[n][1] / by[n][2] * n_full[n] for n in names)
+    used = min(cores, len(tasks))
+    value = reached_full / (cpu_seconds_full / used)
+    return {"value": value, "cores": used, "wall_s": wall, "cpu_s": cpu_sec,
+            "sample": f"stratified {sum(per_class)} problems ({per_class[2]} chain7, {per_class[1]} dual_arm, "
+                      f"{per_class[0]} humanoid), serial float64 LM per problem, {used} processes; "
+                      f"rate extrapolated to the 8,192-problem mix"}
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--section", default="all", choices=["all", "fkj", "ik"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op PyTorch arm")
     args = ap.parse_args()
+    warmup = max(args.warmup, 3)
+    metric = "batched LM-IK solves/s reaching 1e-4 m and 1e-4 rad pose error"
+    config = {"workload": "uneven batched IK: 8192 problems (40% chain7 7-DOF, 30% dual_arm 14-DOF, 30% humanoid "
+                          "36-DOF free-flyer), 1-6 targets, q0 = q* + N(0,0.3), LM <= 100 it, lam 1e-3 x10, "
+                          "tol 1e-6, limit 0.1, rest 1e-3", "problems": N_PROBLEMS, "l2": "256 MB flush between steps"}
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = []
+        cb = None
+        cores = len(os.sched_getaffinity(0))
+        with mp.get_context("spawn").Pool(cores) as pool:
+            for i in range(warmup + args.steps):
+                cb = cpu_baseline(seed=7, per_class=(4, 3, 3), cores=cores, pool=pool)
+                if i >= warmup:
+                    steps.append(cb)
+        v = float(np.mean([s["value"] for s in steps]))
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": "solves/s", "n_gpus": 1,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": float(np.mean([s["wall_s"] for s in steps])) * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cb["cores"], "kind": "port",
+                                 "sample": cb["sample"].replace("stratified", "per step: stratified")},
+                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(seed=7)  # before any CUDA work in this process (spawned workers)
+    import torch
     world, rank, local = dist_setup()
     peak, peak_kind = _peaks()
     with ClockSampler(local) as clk:
         barrier(world)
         torch.cuda.synchronize()
-        fkj = bench_fkj(args.steps, max(args.warmup, 3))
+        ik = bench_ik(args.steps, warmup, seed=7 + 1000 * rank)
         barrier(world)
     clocks = clk.summary()
-    ms = max_over_ranks(fkj["ms_per_launch"], world)
-    value = sum_over_ranks(fkj["configs"], world) / (ms * 1e-3)
+    fkj = bench_fkj(args.steps, warmup)
+    plain = bench_plain_gpu(ik["wl"]) if (rank == 0 and not args.no_plain) else None
+    ms = reduce(ik["ms"], world, "max")
+    reached = reduce(ik["reached"], world, "sum")
+    e2e_ms = reduce(ik["e2e_ms"], world, "max")
+    value = reached / (ms * 1e-3)
     line = {
-        "metric": "fused FK+frame-Jacobian configs/s (humanoid, 12 frames)", "value": value, "unit": "configs/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "humanoid FK + 12 LWA frame Jacobians", "batch": FKJ_BATCH, "l2": "16 rotating q buffers"},
-        "roofline": {"bound": "hbm", "achieved": fkj["gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": fkj["gbs"] / peak, "traffic": None, "peak_kind": peak_kind},
-        "clocks": clocks, "gpu_launches": fkj["launches"],
+        "metric": metric, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (J, J^T J, Cholesky) + f64 (iterate, FK/residual of the accept test)", "data": "synthetic",
+        "config": config,
+        "e2e": {"value": reached / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": ik["h2d"],
+                "d2h_bytes_per_step": ik["d2h"], "ms_per_step": e2e_ms},
+        "roofline": {"bound": "hbm", "kernel": "fk_jac_kernel (humanoid B=65536, 12 frames, J + oMf)",
+                     "achieved": fkj["gbs"], "peak": peak, "unit": "GB/s", "frac": fkj["gbs"] / peak,
+                     "traffic": None, "peak_kind": peak_kind, "ms_per_launch": fkj["ms_per_launch"]},
+        "ik": {"problems": ik["problems"] * world, "reached_1e-4": reached, "converged": ik["converged"],
+               "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1},
+        "clocks": clocks, "gpu_launches": ik["launches"],
     }
+    if plain is not None:
+        line["plain_gpu"] = {"value": plain["reached"] / plain["sec"], "unit": "solves/s", "sec_per_step": plain["sec"],
+                             "reached_1e-4": plain["reached"], "speedup_fused_over_plain":
+                             value / max(plain["reached"] / plain["sec"], 1e-30)}
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": "solves/s", "cores": cpu["cores"], "kind": "port",
+                                "sample": cpu["sample"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

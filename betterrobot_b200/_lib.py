@@ -34,6 +34,27 @@ class BrTree(ctypes.Structure):
                 ("lower", c_void_p), ("upper", c_void_p)]
 
 
+class IKSettings(ctypes.Structure):
+    _fields_ = [("lam0", ctypes.c_float), ("factor", ctypes.c_float), ("tol", ctypes.c_float),
+                ("lam_min", ctypes.c_float), ("lam_max", ctypes.c_float), ("gn_eps", ctypes.c_float),
+                ("pos_weight", ctypes.c_float), ("ori_weight", ctypes.c_float),
+                ("limit_weight", ctypes.c_float), ("rest_weight", ctypes.c_float),
+                ("max_iter", c_int32), ("optimizer", c_int32)]
+
+
+class IKBatch(ctypes.Structure):
+    _fields_ = [("n_problems", c_int32), ("max_targets", c_int32), ("n_classes", c_int32), ("n_items", c_int32),
+                ("trees", ctypes.POINTER(BrTree)), ("team_size", ctypes.POINTER(c_int32)),
+                ("items", c_void_p), ("order", c_void_p), ("n_targets", c_void_p), ("frames", c_void_p),
+                ("targets", c_void_p), ("q_offset", c_void_p), ("x0", c_void_p), ("q_rest", c_void_p),
+                ("r_offset", c_void_p)]
+
+
+class IKResultBuf(ctypes.Structure):
+    _fields_ = [("x", c_void_p), ("iters", c_void_p), ("status", c_void_p), ("cost", c_void_p),
+                ("residual", c_void_p)]
+
+
 # name -> (restype, argtypes); must match include/br_b200.h
 SIGNATURES: dict[str, tuple] = {
     "br_version": (ctypes.c_char_p, []),
@@ -43,6 +64,13 @@ SIGNATURES: dict[str, tuple] = {
                                      c_void_p, c_void_p, c_void_p]),
     "br_frame_jacobians_from_poses": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32,
                                                 c_int32, c_void_p, c_void_p]),
+    "br_lm_solve": (c_int32, [ctypes.POINTER(IKBatch), ctypes.POINTER(IKSettings), ctypes.POINTER(IKResultBuf),
+                              c_int32, c_void_p, c_int64, c_void_p]),
+    "br_lm_team_floats": (c_int64, [ctypes.POINTER(BrTree), c_int32]),
+    "br_pose_loss": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
+                               c_int32, c_void_p, c_void_p, c_void_p]),
+    "br_pose_loss_backward": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_void_p, c_int64, c_void_p, c_int32,
+                                        c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

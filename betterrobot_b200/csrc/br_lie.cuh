@@ -258,3 +258,107 @@ __device__ __forceinline__ void jr_inv_T_apply(const JrInv& J, float3 xl, float3
 }
 
 }  // namespace br
+
+// ---------------------------------------------------------------------------
+// float64 versions for the LM accept/reject path: the iterate, forward kinematics,
+// residual and cost are evaluated in double so that `cost_new < cost` is decided
+// as the float64 reference decides it (levenberg_marquardt.py:114).  Same formulas
+// and Taylor cutoffs as _torch_native_backend.py.
+// ---------------------------------------------------------------------------
+namespace br {
+
+struct DPose {
+  double3 t;
+  double4 q;
+};
+
+__device__ __forceinline__ double3 d3(double x, double y, double z) { return make_double3(x, y, z); }
+__device__ __forceinline__ double3 dadd(double3 a, double3 b) { return d3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ double3 dsub(double3 a, double3 b) { return d3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double3 dscale(double3 a, double s) { return d3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double ddot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double3 dcross(double3 a, double3 b) {
+  return d3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double4 dqmul(double4 a, double4 b) {
+  double4 r;
+  r.x = a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y;
+  r.y = a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x;
+  r.z = a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w;
+  r.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+  return r;
+}
+__device__ __forceinline__ double4 dqconj(double4 q) { return make_double4(-q.x, -q.y, -q.z, q.w); }
+__device__ __forceinline__ double3 dqrot(double4 q, double3 p) {
+  const double3 u = d3(q.x, q.y, q.z);
+  const double3 c1 = dadd(dcross(u, p), dscale(p, q.w));
+  return dadd(p, dscale(dcross(u, c1), 2.0));
+}
+__device__ __forceinline__ DPose dcompose(const DPose& a, const DPose& b) {
+  DPose c;
+  c.t = dadd(a.t, dqrot(a.q, b.t));
+  c.q = dqmul(a.q, b.q);
+  return c;
+}
+__device__ __forceinline__ DPose dinverse(const DPose& a) {
+  DPose r;
+  r.q = dqconj(a.q);
+  r.t = dscale(dqrot(r.q, a.t), -1.0);
+  return r;
+}
+__device__ __forceinline__ double4 dqnormalize(double4 q) {
+  const double n = fmax(sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-8);
+  return make_double4(q.x / n, q.y / n, q.z / n, q.w / n);
+}
+__device__ __forceinline__ double3 dso3_log(double4 q) {
+  if (q.w < 0.0) q = make_double4(-q.x, -q.y, -q.z, -q.w);
+  const double s2 = q.x * q.x + q.y * q.y + q.z * q.z;
+  const double s = sqrt(s2);
+  double factor;
+  if (s2 < 1e-8 / 4.0) {
+    factor = 2.0 + s2 * (2.0 / 3.0);
+  } else {
+    factor = 2.0 * atan2(s, fmin(fmax(q.w, -1.0), 1.0)) / s;
+  }
+  return d3(factor * q.x, factor * q.y, factor * q.z);
+}
+__device__ __forceinline__ void dse3_log(const DPose& T, double3& v, double3& w) {
+  w = dso3_log(T.q);
+  const double th2 = ddot(w, w);
+  double c;
+  if (th2 < 1e-8) {
+    c = 1.0 / 12.0 + th2 / 720.0;
+  } else {
+    const double th = sqrt(th2);
+    double sh, ch;
+    sincos(0.5 * th, &sh, &ch);
+    c = 1.0 / th2 - (ch / sh) / (2.0 * th);
+  }
+  const double3 wt = dcross(w, T.t);
+  v = dadd(dadd(T.t, dscale(wt, -0.5)), dscale(dcross(w, wt), c));
+}
+__device__ __forceinline__ DPose dse3_exp(double3 v, double3 w) {
+  const double th2 = ddot(w, w);
+  double b, c, k, cw;
+  if (th2 < 1e-8) {
+    b = 0.5 - th2 / 24.0;
+    c = 1.0 / 6.0 - th2 / 120.0;
+    k = 0.5 - th2 / 48.0;
+    cw = cos(0.5 * sqrt(th2));
+  } else {
+    const double th = sqrt(th2);
+    double s, co, sh;
+    sincos(th, &s, &co);
+    sincos(0.5 * th, &sh, &cw);
+    b = (1.0 - co) / th2;
+    c = (th - s) / (th * th2);
+    k = sh / th;
+  }
+  const double3 wv = dcross(w, v);
+  DPose T;
+  T.t = dadd(dadd(v, dscale(wv, b)), dscale(dcross(w, wv), c));
+  T.q = make_double4(k * w.x, k * w.y, k * w.z, cw);
+  return T;
+}
+
+}  // namespace br

@@ -1,0 +1,317 @@
+// fk_adjoint.cu — pose loss through forward kinematics and its hand-written adjoint.
+//
+// Loss per configuration:  L(q) = sum_f w_f |log(T_f^-1 * oMf(q))|^2
+// (the reference obtains dL/dq by torch autograd through every SE3 op of
+// src/better_robot/kinematics/forward.py:73-135 and lie/_torch_native_backend.py).
+//
+// Adjoint, one warp per configuration:
+//   * g_f = 2 w_f Jr^-1(xi_f)^T xi_f is dL/d(body twist of frame f), with the exact
+//     SE3 Jr^-1 (series to 20 terms; autograd differentiates se3_log exactly);
+//   * F_f = Ad(oMf^-1)^T g_f = [R g_lin; p x (R g_lin) + R g_ang] is the same
+//     sensitivity as a wrench at the world origin;
+//   * dL/dv_c = sum_{f : c supports f} <S_c, F_f> with S_c the world twist of tangent
+//     column c ([o x a; a] rotation, [a; 0] translation) — a reverse accumulation over
+//     the tree without any per-joint tape;
+//   * revolute / prismatic: dL/dq = dL/dv; free-flyer: the body twist of its joint
+//     maps to raw q = [t, quat] through R (translation) and the normalisation of the
+//     quaternion ((I - u u^T)/|quat| and du -> 2 vec(u* (x) du)).
+// World joint placements are either recomputed from q (no saved state) or read
+// from the forward pass (store mode, [B, njoints, 7]).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "br_common.cuh"
+#include "br_fk.cuh"
+#include "br_lie.cuh"
+
+namespace br {
+
+struct LossParams {
+  const float* q;          // [B, nq]
+  const float* targets;    // [B, nf, 7]
+  const float* weights;    // [nf] or [B, nf]
+  const float* grad_loss;  // [B] (backward)
+  const float* oMi_in;     // [B, nj, 7] (backward, store mode) or null
+  float* loss;             // [B] (forward)
+  float* oMi_out;          // [B, nj, 7] (forward, store mode) or null
+  float* grad_q;           // [B, nq] (backward)
+  int64_t batch;
+  int32_t nf;
+  int32_t weights_per_config;
+  int32_t frames[BR_MAX_TARGETS];
+};
+
+struct LossLayout {
+  int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, fparent, fplace, fmask;
+  int cta_floats;
+  int q, poseT, poseQ, anc, F, gv, stage;
+  int warp_floats;
+  __host__ __device__ LossLayout(int nj, int nq, int nv, int nf) {
+    int o = 0;
+    auto take = [&](int n) { int r = o; o += round4(n); return r; };
+    parent = take(nj); jtype = take(nj); idxq = take(nj); axis = take(4 * nj); place = take(8 * nj);
+    cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
+    fparent = take(nf); fplace = take(8 * nf); fmask = take(2 * nf);
+    cta_floats = o;
+    o = 0;
+    q = take(nq); poseT = take(4 * nj); poseQ = take(4 * nj); anc = take(nj);
+    F = take(8 * nf);     // world wrench per frame (f.xyz, pad, tau.xyz, pad)
+    gv = take(nv);        // dL/dv
+    stage = take(nj * 7); // oMi staging (store mode)
+    warp_floats = o;
+  }
+};
+
+template <bool kBackward>
+__global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
+  extern __shared__ __align__(16) float smem[];
+  const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, nf = p.nf;
+  const LossLayout L(nj, nq, nv, nf);
+  int* s_parent = reinterpret_cast<int*>(smem + L.parent);
+  int* s_jtype = reinterpret_cast<int*>(smem + L.jtype);
+  int* s_idxq = reinterpret_cast<int*>(smem + L.idxq);
+  float* s_axis = smem + L.axis;
+  float* s_place = smem + L.place;
+  int* s_cjoint = reinterpret_cast<int*>(smem + L.cjoint);
+  int* s_ckind = reinterpret_cast<int*>(smem + L.ckind);
+  float* s_caxis = smem + L.caxis;
+  int* s_fparent = reinterpret_cast<int*>(smem + L.fparent);
+  float* s_fplace = smem + L.fplace;
+  unsigned long long* s_fmask = reinterpret_cast<unsigned long long*>(smem + L.fmask);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  for (int i = threadIdx.x; i < nj; i += blockDim.x) {
+    s_parent[i] = tree.parent[i];
+    s_jtype[i] = tree.jtype[i];
+    s_idxq[i] = tree.idx_q[i];
+    for (int k = 0; k < 4; ++k) s_axis[4 * i + k] = tree.axis[4 * i + k];
+    for (int k = 0; k < 8; ++k) s_place[8 * i + k] = tree.placement[8 * i + k];
+  }
+  for (int c = threadIdx.x; c < nv; c += blockDim.x) {
+    s_cjoint[c] = tree.col_joint[c];
+    s_ckind[c] = tree.col_kind[c];
+    for (int k = 0; k < 4; ++k) s_caxis[4 * c + k] = tree.col_axis[4 * c + k];
+  }
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+    const int id = p.frames[f];
+    s_fparent[f] = tree.frame_parent[id];
+    for (int k = 0; k < 8; ++k) s_fplace[8 * f + k] = tree.frame_placement[8 * id + k];
+  }
+  __syncthreads();
+  // column mask of each frame: bit c set iff tangent column c moves the frame
+  for (int f = warp; f < nf; f += wpc) {
+    const unsigned long long sup = tree.support[s_fparent[f]];
+    unsigned long long m = 0ull;
+    for (int c0 = 0; c0 < nv; c0 += kWarp) {
+      const int c = c0 + lane;
+      const bool in = c < nv && ((sup >> s_cjoint[c]) & 1ull);
+      m |= (unsigned long long)__ballot_sync(0xffffffffu, in) << c0;
+    }
+    if (lane == 0) s_fmask[f] = m;
+  }
+  __syncthreads();
+
+  float* w = smem + L.cta_floats + warp * L.warp_floats;
+  float* wq = w + L.q;
+  float* wpT = w + L.poseT;
+  float* wpQ = w + L.poseQ;
+  int* wanc = reinterpret_cast<int*>(w + L.anc);
+  float* wF = w + L.F;
+  float* wg = w + L.gv;
+  float* wst = w + L.stage;
+  const int64_t stride = (int64_t)gridDim.x * wpc;
+  for (int64_t b = (int64_t)blockIdx.x * wpc + warp; b < p.batch; b += stride) {
+    const float* qb = p.q + b * nq;
+    for (int i = lane; i < nq; i += kWarp) wq[i] = __ldg(qb + i);
+    __syncwarp();
+    if (kBackward && p.oMi_in) {
+      const float* ob = p.oMi_in + b * (int64_t)nj * 7;
+      for (int i = lane; i < nj * 7; i += kWarp) {
+        const int j = i / 7, c = i - 7 * j;
+        if (c < 3) wpT[4 * j + c] = __ldg(ob + i);
+        else wpQ[4 * j + c - 3] = __ldg(ob + i);
+      }
+      __syncwarp();
+    } else {
+      // forward kinematics by pointer jumping (see fk_jac.cu)
+      for (int j = lane; j < nj; j += kWarp) {
+        store_split(wpT, wpQ, j, local_transform(s_jtype[j], load_pose8(s_place + 8 * j), s_axis + 4 * j,
+                                                 wq + s_idxq[j]));
+        wanc[j] = s_parent[j];
+      }
+      __syncwarp();
+      for (int r = 0; r < tree.rounds; ++r) {
+        Pose A[2], Tj[2];
+        int aa[2], an[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int j = lane + kWarp * k;
+          an[k] = (j < nj) ? wanc[j] : -1;
+          if (an[k] >= 0) {
+            A[k] = load_split(wpT, wpQ, an[k]);
+            Tj[k] = load_split(wpT, wpQ, j);
+            aa[k] = wanc[an[k]];
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int j = lane + kWarp * k;
+          if (an[k] >= 0) {
+            store_split(wpT, wpQ, j, compose(A[k], Tj[k]));
+            wanc[j] = aa[k];
+          }
+        }
+        __syncwarp();
+      }
+      if (!kBackward && p.oMi_out) {
+        for (int j = lane; j < nj; j += kWarp) store_pose7(wst + 7 * j, load_split(wpT, wpQ, j));
+        __syncwarp();
+        warp_copy(p.oMi_out + b * (int64_t)nj * 7, wst, nj * 7, lane);
+      }
+    }
+    // per-frame residual, loss and (backward) world wrench
+    float acc = 0.f;
+    for (int f = lane; f < nf; f += kWarp) {
+      const Pose Tf = compose(load_split(wpT, wpQ, s_fparent[f]), load_pose8(s_fplace + 8 * f));
+      const float* tp = p.targets + (b * nf + f) * 7;
+      const Pose Tt{f3(__ldg(tp), __ldg(tp + 1), __ldg(tp + 2)),
+                    make_float4(__ldg(tp + 3), __ldg(tp + 4), __ldg(tp + 5), __ldg(tp + 6))};
+      float3 v, om;
+      se3_log(compose(inverse(Tt), Tf), v, om);
+      const float wf = __ldg(p.weights + (p.weights_per_config ? b * nf + f : f));
+      acc += wf * (dot(v, v) + dot(om, om));
+      if (kBackward) {
+        const JrInv J = jr_inv_se3<20>(v, om);
+        float3 gl, ga;
+        jr_inv_T_apply(J, v, om, gl, ga);
+        const float s2 = 2.f * wf;
+        const float3 fw = qrot(Tf.q, scale(gl, s2));
+        const float3 tau = add(cross(Tf.t, fw), qrot(Tf.q, scale(ga, s2)));
+        *reinterpret_cast<float4*>(wF + 8 * f) = make_float4(fw.x, fw.y, fw.z, 0.f);
+        *reinterpret_cast<float4*>(wF + 8 * f + 4) = make_float4(tau.x, tau.y, tau.z, 0.f);
+      }
+    }
+    if (!kBackward) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) p.loss[b] = acc;
+      continue;
+    }
+    __syncwarp();
+    const float go = __ldg(p.grad_loss + b);
+    for (int c = lane; c < nv; c += kWarp) {
+      const Pose Tj = load_split(wpT, wpQ, s_cjoint[c]);
+      const float3 a = qrot(Tj.q, f3(s_caxis[4 * c], s_caxis[4 * c + 1], s_caxis[4 * c + 2]));
+      const float3 m = s_ckind[c] == 0 ? cross(Tj.t, a) : a;  // linear part of the world twist
+      const float3 an = s_ckind[c] == 0 ? a : f3(0.f, 0.f, 0.f);
+      float gsum = 0.f;
+      for (int f = 0; f < nf; ++f) {
+        if ((s_fmask[f] >> c) & 1ull) {
+          const float4 fw = *reinterpret_cast<const float4*>(wF + 8 * f);
+          const float4 tq = *reinterpret_cast<const float4*>(wF + 8 * f + 4);
+          gsum += dot(m, f3(fw.x, fw.y, fw.z)) + dot(an, f3(tq.x, tq.y, tq.z));
+        }
+      }
+      wg[c] = gsum * go;
+    }
+    __syncwarp();
+    float* gq = p.grad_q + b * nq;
+    for (int j = lane; j < nj; j += kWarp) {
+      const int jt = s_jtype[j];
+      const int iq = s_idxq[j];
+      if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
+        gq[iq] = wg[tree.idx_v[j]];
+      } else if (jt == BR_JOINT_FREE_FLYER) {
+        const int iv = tree.idx_v[j];
+        const float4 qr = make_float4(wq[iq + 3], wq[iq + 4], wq[iq + 5], wq[iq + 6]);
+        const float4 u = qnormalize(qr);
+        const float n = fmaxf(sqrtf(qr.x * qr.x + qr.y * qr.y + qr.z * qr.z + qr.w * qr.w), 1e-8f);
+        const float3 gl = f3(wg[iv], wg[iv + 1], wg[iv + 2]);
+        const float3 ga = f3(wg[iv + 3], wg[iv + 4], wg[iv + 5]);
+        const float3 gt = qrot(u, gl);  // translation: delta_lin = R^T dt
+        // quaternion: delta_ang = 2 vec(u* (x) du), du = (I - u u^T) dquat / n
+        float4 h;
+        h.x = u.w * ga.x - u.z * ga.y + u.y * ga.z;
+        h.y = u.z * ga.x + u.w * ga.y - u.x * ga.z;
+        h.z = -u.y * ga.x + u.x * ga.y + u.w * ga.z;
+        h.w = -u.x * ga.x - u.y * ga.y - u.z * ga.z;
+        const float uh = u.x * h.x + u.y * h.y + u.z * h.z + u.w * h.w;
+        const float s = 2.f / n;
+        gq[iq] = gt.x; gq[iq + 1] = gt.y; gq[iq + 2] = gt.z;
+        gq[iq + 3] = s * (h.x - u.x * uh);
+        gq[iq + 4] = s * (h.y - u.y * uh);
+        gq[iq + 5] = s * (h.z - u.z * uh);
+        gq[iq + 6] = s * (h.w - u.w * uh);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <bool kBackward>
+static int launch_loss(const br_tree_t& tree, const LossParams& p, int wpc, cudaStream_t stream) {
+  if (p.batch == 0) return BR_OK;
+  const LossLayout L(tree.njoints, tree.nq, tree.nv, p.nf);
+  const DeviceInfo& dev = device_info();
+  size_t bytes = (size_t)(L.cta_floats + wpc * L.warp_floats) * sizeof(float);
+  while ((int)bytes > dev.max_smem_optin && wpc > 1) {
+    wpc >>= 1;
+    bytes = (size_t)(L.cta_floats + wpc * L.warp_floats) * sizeof(float);
+  }
+  auto kern = pose_loss_kernel<kBackward>;
+  static int configured[16] = {0};
+  if ((int)bytes > configured[dev.device & 15]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return (int)e;
+    configured[dev.device & 15] = (int)bytes;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpc * kWarp, bytes);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t need = (p.batch + wpc - 1) / wpc;
+  const int64_t cap = (int64_t)per_sm * dev.sms;
+  kern<<<(int)(need < cap ? need : cap), wpc * kWarp, bytes, stream>>>(tree, p);
+  return (int)cudaGetLastError();
+}
+
+static int fill_loss(const br_tree_t* tree, LossParams& p, const int32_t* frame_ids, int32_t n_frames) {
+  int st = validate_tree(tree);
+  if (st) return st;
+  if (n_frames < 1 || !frame_ids) return BR_EINVAL;
+  if (n_frames > BR_MAX_TARGETS) return BR_ETOOBIG;
+  for (int i = 0; i < n_frames; ++i) {
+    if (frame_ids[i] < 0 || frame_ids[i] >= tree->nframes) return BR_EINVAL;
+    p.frames[i] = frame_ids[i];
+  }
+  p.nf = n_frames;
+  return BR_OK;
+}
+
+}  // namespace br
+
+using namespace br;
+
+extern "C" int br_pose_loss(const br_tree_t* tree, const float* q, int64_t batch, const int32_t* frame_ids,
+                            int32_t n_frames, const float* targets, const float* weights,
+                            int32_t weights_per_config, float* loss, float* joint_pose_world, void* stream) {
+  LossParams p = {};
+  int st = fill_loss(tree, p, frame_ids, n_frames);
+  if (st) return st;
+  if (batch < 0 || (batch > 0 && (!q || !targets || !weights || !loss))) return BR_EINVAL;
+  p.q = q; p.targets = targets; p.weights = weights; p.loss = loss; p.oMi_out = joint_pose_world;
+  p.batch = batch; p.weights_per_config = weights_per_config != 0;
+  return launch_loss<false>(*tree, p, 8, (cudaStream_t)stream);
+}
+
+extern "C" int br_pose_loss_backward(const br_tree_t* tree, const float* q, const float* joint_pose_world,
+                                     int64_t batch, const int32_t* frame_ids, int32_t n_frames,
+                                     const float* targets, const float* weights, int32_t weights_per_config,
+                                     const float* grad_loss, float* grad_q, void* stream) {
+  LossParams p = {};
+  int st = fill_loss(tree, p, frame_ids, n_frames);
+  if (st) return st;
+  if (batch < 0 || (batch > 0 && (!q || !targets || !weights || !grad_loss || !grad_q))) return BR_EINVAL;
+  p.q = q; p.oMi_in = joint_pose_world; p.targets = targets; p.weights = weights;
+  p.grad_loss = grad_loss; p.grad_q = grad_q; p.batch = batch; p.weights_per_config = weights_per_config != 0;
+  return launch_loss<true>(*tree, p, 8, (cudaStream_t)stream);
+}

@@ -23,6 +23,7 @@
 
 #include "br_common.cuh"
 #include "br_lie.cuh"
+#include "br_fk.cuh"
 
 namespace br {
 
@@ -45,10 +46,10 @@ struct FkParams {
 // Shared-memory layout (in floats; every region starts on a 16-byte boundary).
 struct Layout {
   // CTA-wide tables
-  int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, tparent, tplace, tmask;
+  int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, tparent, tplace, tmask, pairoff, pairs, npairs;
   int cta_floats;
   // per-warp regions
-  int q, pose, anc, col, tgt, sJ, sT, sOMi, sLiMi;
+  int q, poseT, poseQ, anc, colA, colO, tgt, sJ, sT, sOMi, sLiMi;
   int warp_floats;
   __host__ __device__ Layout(int nj, int nq, int nv, int nt, uint32_t outputs) {
     int o = 0;
@@ -62,13 +63,18 @@ struct Layout {
     caxis = o; o += 4 * nv;
     tparent = o; o += round4(nt);
     tplace = o; o += 8 * nt;
-    tmask = o; o += round4(2 * nt);  // uint64 per target
+    tmask = o; o += round4(2 * nt);                              // uint64 column mask per target
+    pairoff = o; o += round4(nt);
+    pairs = o; o += (outputs & OUT_JAC) ? round4(nt * nv) : 0;   // (target << 8 | column) with support
+    npairs = o; o += 4;
     cta_floats = o;
     o = 0;
     q = o; o += round4(nq);
-    pose = o; o += 8 * nj;
+    poseT = o; o += 4 * nj;                                      // world translation (x, y, z, 0)
+    poseQ = o; o += 4 * nj;                                      // world quaternion
     anc = o; o += round4(nj);
-    col = o; o += 8 * nv;
+    colA = o; o += 4 * nv;                                       // world column axis
+    colO = o; o += 4 * nv;                                       // world column origin
     tgt = o; o += 8 * nt;
     sJ = o; o += (outputs & OUT_JAC) ? round4(nt * 6 * nv) : 0;
     sT = o; o += (outputs & OUT_TPOSE) ? round4(nt * 7) : 0;
@@ -78,49 +84,11 @@ struct Layout {
   }
 };
 
-__device__ __forceinline__ Pose load_pose8(const float* p) {
-  const float4 a = *reinterpret_cast<const float4*>(p);
-  const float4 b = *reinterpret_cast<const float4*>(p + 4);
-  Pose T;
-  T.t = f3(a.x, a.y, a.z);
-  T.q = b;
-  return T;
-}
-__device__ __forceinline__ void store_pose8(float* p, const Pose& T) {
-  *reinterpret_cast<float4*>(p) = make_float4(T.t.x, T.t.y, T.t.z, 0.f);
-  *reinterpret_cast<float4*>(p + 4) = T.q;
-}
-__device__ __forceinline__ void store_pose7(float* p, const Pose& T) {
-  p[0] = T.t.x; p[1] = T.t.y; p[2] = T.t.z;
-  p[3] = T.q.x; p[4] = T.q.y; p[5] = T.q.z; p[6] = T.q.w;
-}
-
-// liMi_j = placement_j * T_j(q_j)   (forward.py:114-122; joint_transform of
-// revolute.py:18-21, prismatic.py:16-19, free_flyer.py:31-36, fixed.py:90-94)
-__device__ __forceinline__ Pose local_transform(int jt, const Pose& P, const float* __restrict__ axis4,
-                                                const float* __restrict__ qv) {
-  Pose L = P;
-  if (jt == BR_JOINT_REVOLUTE) {
-    float s, c;
-    sincosf(0.5f * qv[0], &s, &c);
-    const float4 qj = make_float4(s * axis4[0], s * axis4[1], s * axis4[2], c);
-    L.q = qmul(P.q, qj);
-  } else if (jt == BR_JOINT_PRISMATIC) {
-    const float d = qv[0];
-    L.t = add(P.t, qrot(P.q, f3(d * axis4[0], d * axis4[1], d * axis4[2])));
-  } else if (jt == BR_JOINT_FREE_FLYER) {
-    Pose F;
-    F.t = f3(qv[0], qv[1], qv[2]);
-    F.q = qnormalize(make_float4(qv[3], qv[4], qv[5], qv[6]));
-    L = compose(P, F);
-  }
-  return L;
-}
-
 template <int kRef, bool kFromQ>
 __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
   extern __shared__ __align__(16) float smem[];
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, nt = p.nt;
+  const bool want_jac = (p.outputs & OUT_JAC) != 0;
   const Layout L(nj, nq, nv, nt, p.outputs);
   float* cta = smem;
   int* s_parent = reinterpret_cast<int*>(cta + L.parent);
@@ -134,6 +102,12 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
   int* s_tparent = reinterpret_cast<int*>(cta + L.tparent);
   float* s_tplace = cta + L.tplace;
   unsigned long long* s_tmask = reinterpret_cast<unsigned long long*>(cta + L.tmask);
+  int* s_pairoff = reinterpret_cast<int*>(cta + L.pairoff);
+  int* s_pairs = reinterpret_cast<int*>(cta + L.pairs);
+  int* s_npairs = reinterpret_cast<int*>(cta + L.npairs);
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int wpc = blockDim.x >> 5;
 
   for (int i = threadIdx.x; i < nj; i += blockDim.x) {
     s_parent[i] = tree.parent[i];
@@ -158,23 +132,57 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
       for (int k = 0; k < 8; ++k) s_tplace[8 * s + k] = (k == 7) ? 1.f : 0.f;  // identity
     }
     s_tparent[s] = par;
-    s_tmask[s] = tree.support[par];
   }
   __syncthreads();
+  // Columns with a non-zero Jacobian entry for each target: col_joint[c] supports the
+  // target's parent joint.  The list of such (target, column) pairs is the only part of
+  // the J block that depends on q; the rest is zero and is written once below.
+  for (int s = warp; s < nt; s += wpc) {
+    const unsigned long long sup = tree.support[s_tparent[s]];
+    unsigned long long m = 0ull;
+    for (int c0 = 0; c0 < nv; c0 += kWarp) {
+      const int c = c0 + lane;
+      const bool in = c < nv && ((sup >> s_cjoint[c]) & 1ull);
+      m |= (unsigned long long)__ballot_sync(0xffffffffu, in) << c0;
+    }
+    if (lane == 0) s_tmask[s] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int off = 0;
+    for (int s = 0; s < nt; ++s) {
+      s_pairoff[s] = off;
+      off += __popcll(s_tmask[s]);
+    }
+    s_npairs[0] = off;
+  }
+  __syncthreads();
+  if (want_jac) {
+    for (int s = warp; s < nt; s += wpc) {
+      const unsigned long long m = s_tmask[s];
+      for (int c = lane; c < nv; c += kWarp)
+        if ((m >> c) & 1ull) s_pairs[s_pairoff[s] + __popcll(m & ((1ull << c) - 1ull))] = (s << 8) | c;
+    }
+  }
+  const int npairs = s_npairs[0];
 
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int wpc = blockDim.x >> 5;
   float* w = smem + L.cta_floats + warp * L.warp_floats;
   float* wq = w + L.q;
-  float* wpose = w + L.pose;
+  float* wpT = w + L.poseT;
+  float* wpQ = w + L.poseQ;
   int* wanc = reinterpret_cast<int*>(w + L.anc);
-  float* wcol = w + L.col;
+  float* wcA = w + L.colA;
+  float* wcO = w + L.colO;
   float* wtgt = w + L.tgt;
   float* sJ = w + L.sJ;
   float* sT = w + L.sT;
   float* sOMi = w + L.sOMi;
   float* sLiMi = w + L.sLiMi;
+  if (want_jac) {
+    const int n = round4(nt * 6 * nv) / 4;
+    for (int i = lane; i < n; i += kWarp) reinterpret_cast<float4*>(sJ)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
   const int rounds = tree.rounds;
   const int64_t stride = (int64_t)gridDim.x * wpc;
 
@@ -200,7 +208,7 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
       for (int k = 0; k < 2; ++k) {
         const int j = lane + kWarp * k;
         if (j < nj) {
-          store_pose8(wpose + 8 * j, T[k]);
+          store_split(wpT, wpQ, j, T[k]);
           wanc[j] = anc[k];
           if (p.outputs & OUT_LIMI) store_pose7(sLiMi + 7 * j, T[k]);
         }
@@ -213,7 +221,7 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
         for (int k = 0; k < 2; ++k) {
           const int j = lane + kWarp * k;
           if (j < nj && anc[k] >= 0) {
-            A[k] = load_pose8(wpose + 8 * anc[k]);
+            A[k] = load_split(wpT, wpQ, anc[k]);
             aa[k] = wanc[anc[k]];
           }
         }
@@ -224,7 +232,7 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
           if (j < nj && anc[k] >= 0) {
             T[k] = compose(A[k], T[k]);
             anc[k] = aa[k];
-            store_pose8(wpose + 8 * j, T[k]);
+            store_split(wpT, wpQ, j, T[k]);
             wanc[j] = anc[k];
           }
         }
@@ -243,54 +251,53 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
       __syncwarp();
       for (int i = lane; i < nj * 7; i += kWarp) {
         const int j = i / 7, c = i - 7 * j;
-        wpose[8 * j + (c < 3 ? c : c + 1)] = __ldg(ob + i);
+        if (c < 3) wpT[4 * j + c] = __ldg(ob + i);
+        else wpQ[4 * j + c - 3] = __ldg(ob + i);
       }
       __syncwarp();
     }
 
     // ---- target placements and world Jacobian columns --------------------
     for (int s = lane; s < nt; s += kWarp) {
-      const Pose Tt = compose(load_pose8(wpose + 8 * s_tparent[s]), load_pose8(s_tplace + 8 * s));
+      const Pose Tt = compose(load_split(wpT, wpQ, s_tparent[s]), load_pose8(s_tplace + 8 * s));
       store_pose8(wtgt + 8 * s, Tt);
       if (p.outputs & OUT_TPOSE) store_pose7(sT + 7 * s, Tt);
     }
-    if (p.outputs & OUT_JAC) {
+    if (want_jac) {
       for (int c = lane; c < nv; c += kWarp) {
-        const Pose Tj = load_pose8(wpose + 8 * s_cjoint[c]);
+        const Pose Tj = load_split(wpT, wpQ, s_cjoint[c]);
         const float3 a = qrot(Tj.q, f3(s_caxis[4 * c], s_caxis[4 * c + 1], s_caxis[4 * c + 2]));
-        *reinterpret_cast<float4*>(wcol + 8 * c) = make_float4(a.x, a.y, a.z, 0.f);
-        *reinterpret_cast<float4*>(wcol + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
+        *reinterpret_cast<float4*>(wcA + 4 * c) = make_float4(a.x, a.y, a.z, 0.f);
+        *reinterpret_cast<float4*>(wcO + 4 * c) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
       }
     }
     __syncwarp();
 
-    if (p.outputs & OUT_JAC) {
-      const int npairs = nt * nv;
+    if (want_jac) {
       for (int idx = lane; idx < npairs; idx += kWarp) {
-        const int s = idx / nv;
-        const int c = idx - s * nv;
-        float3 lin = f3(0.f, 0.f, 0.f), ang = f3(0.f, 0.f, 0.f);
-        if ((s_tmask[s] >> s_cjoint[c]) & 1ull) {
-          const float4 a4 = *reinterpret_cast<const float4*>(wcol + 8 * c);
-          const float3 a = f3(a4.x, a4.y, a4.z);
-          if (s_ckind[c] == 0) {
-            const float4 o4 = *reinterpret_cast<const float4*>(wcol + 8 * c + 4);
-            const float3 o = f3(o4.x, o4.y, o4.z);
-            if (kRef == BR_REF_WORLD) {
-              lin = cross(o, a);
-            } else {
-              const float4 pt = *reinterpret_cast<const float4*>(wtgt + 8 * s);
-              lin = cross(a, sub(f3(pt.x, pt.y, pt.z), o));
-            }
-            ang = a;
+        const int pr = s_pairs[idx];
+        const int s = pr >> 8, c = pr & 255;
+        const float4 a4 = *reinterpret_cast<const float4*>(wcA + 4 * c);
+        const float3 a = f3(a4.x, a4.y, a4.z);
+        float3 lin, ang;
+        if (s_ckind[c] == 0) {
+          const float4 o4 = *reinterpret_cast<const float4*>(wcO + 4 * c);
+          const float3 o = f3(o4.x, o4.y, o4.z);
+          if (kRef == BR_REF_WORLD) {
+            lin = cross(o, a);                                   // hat(p_j) R S_ang  (jacobian.py:290-296)
           } else {
-            lin = a;
+            const float4 pt = *reinterpret_cast<const float4*>(wtgt + 8 * s);
+            lin = cross(a, sub(f3(pt.x, pt.y, pt.z), o));        // J_lin - hat(p_f) J_ang (jacobian.py:213-215)
           }
-          if (kRef == BR_REF_LOCAL) {
-            const float4 qt = *reinterpret_cast<const float4*>(wtgt + 8 * s + 4);
-            lin = qrot_inv(qt, lin);
-            ang = qrot_inv(qt, ang);
-          }
+          ang = a;
+        } else {
+          lin = a;
+          ang = f3(0.f, 0.f, 0.f);
+        }
+        if (kRef == BR_REF_LOCAL) {                              // R_f^T rows (jacobian.py:219-225)
+          const float4 qt = *reinterpret_cast<const float4*>(wtgt + 8 * s + 4);
+          lin = qrot_inv(qt, lin);
+          ang = qrot_inv(qt, ang);
         }
         float* dst = sJ + s * 6 * nv + c;
         dst[0] = lin.x; dst[nv] = lin.y; dst[2 * nv] = lin.z;

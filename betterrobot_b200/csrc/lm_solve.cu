@@ -22,6 +22,13 @@
 //     (lanes over the trailing triangle), triangular solves by shuffles;
 //   * retraction q (+) dq (Model.integrate, model.py:160-174) and clamping to the
 //     joint limits (levenberg_marquardt.py:103-107).
+//
+// Precision: the iterate, forward kinematics, residual, cost and retraction are
+// float64, so `cost_new < cost` (levenberg_marquardt.py:114) and the convergence
+// test are decided as the float64 reference decides them; near the optimum the
+// cost decrease of an accepted step (~1e-12) is far below float32 resolution of
+// the cost.  Everything that scales with nv^2 or nv^3 — Jacobian columns, J^T J,
+// J^T r, the Cholesky factorization and the solves — is float32.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -32,7 +39,6 @@
 namespace br {
 
 constexpr int kMaxClasses = BR_MAX_IK_CLASSES;
-constexpr int kMaxT = BR_MAX_IK_TARGETS;
 
 struct LmParams {
   br_ik_settings_t s;
@@ -57,11 +63,15 @@ struct TeamLayout {
     axis = take(4 * nj); place = take(8 * nj); support = take(2 * nj);
     cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
     lower = take(nq); upper = take(nq);
-    fparent = take(K); fplace = take(8 * K); tgt = take(8 * K); cmask = take(2 * K);
-    x = take(nq); xn = take(nq); qrest = take(nq);
-    poseA = take(8 * nj); poseB = take(8 * nj); ancA = take(nj); ancB = take(nj);
-    tw = take(8 * K); xi = take(8 * K); jri = take(16 * K); colw = take(8 * nv);
-    d = take(nv); g = take(nv); delta = take(nv);
+    fparent = take(K); fplace = take(8 * K); cmask = take(2 * K);
+    // float64 regions (2 floats per double)
+    x = take(2 * nq); xn = take(2 * nq); qrest = take(2 * nq);
+    poseA = take(16 * nj); poseB = take(16 * nj); tw = take(16 * K); xi = take(16 * K); d = take(2 * nv);
+    tgt = take(16 * K);
+    // float32 / int regions
+    ancA = take(nj); ancB = take(nj);
+    jri = take(16 * K); colw = take(8 * nv);
+    g = take(nv); delta = take(nv);
     jtj = take(nv * (nv + 1) / 2);
     const int jp = 6 * K * nv, lsq = nv * (nv + 1);
     work = take(jp > lsq ? jp : lsq);  // J_pose during the Jacobian build, L during the solve
@@ -97,6 +107,25 @@ __device__ __forceinline__ void st8(float* p, const Pose& P) {
   *reinterpret_cast<float4*>(p + 4) = P.q;
 }
 
+// float64 pose records: (t.x, t.y, t.z, pad, q.x, q.y, q.z, q.w)
+__device__ __forceinline__ DPose ldd(const double* p) {
+  DPose P;
+  P.t = d3(p[0], p[1], p[2]);
+  P.q = make_double4(p[4], p[5], p[6], p[7]);
+  return P;
+}
+__device__ __forceinline__ void std8(double* p, const DPose& P) {
+  p[0] = P.t.x; p[1] = P.t.y; p[2] = P.t.z; p[3] = 0.0;
+  p[4] = P.q.x; p[5] = P.q.y; p[6] = P.q.z; p[7] = P.q.w;
+}
+__device__ __forceinline__ DPose to_d(const Pose& P) {
+  return DPose{d3(P.t.x, P.t.y, P.t.z), make_double4(P.q.x, P.q.y, P.q.z, P.q.w)};
+}
+__device__ __forceinline__ Pose to_f(const DPose& P) {
+  return Pose{f3((float)P.t.x, (float)P.t.y, (float)P.t.z),
+              make_float4((float)P.q.x, (float)P.q.y, (float)P.q.z, (float)P.q.w)};
+}
+
 // ---- one problem, solved by one team ---------------------------------------
 template <int T>
 __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
@@ -117,20 +146,20 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   float* upper = sm + L.upper;
   int* fparent = reinterpret_cast<int*>(sm + L.fparent);
   float* fplace = sm + L.fplace;
-  float* tgt = sm + L.tgt;
   unsigned long long* cmask = reinterpret_cast<unsigned long long*>(sm + L.cmask);
-  float* x = sm + L.x;
-  float* xn = sm + L.xn;
-  float* qrest = sm + L.qrest;
-  float* poseA = sm + L.poseA;
-  float* poseB = sm + L.poseB;
+  double* x = reinterpret_cast<double*>(sm + L.x);
+  double* xn = reinterpret_cast<double*>(sm + L.xn);
+  double* qrest = reinterpret_cast<double*>(sm + L.qrest);
+  double* poseA = reinterpret_cast<double*>(sm + L.poseA);
+  double* poseB = reinterpret_cast<double*>(sm + L.poseB);
+  double* tw = reinterpret_cast<double*>(sm + L.tw);
+  double* xi = reinterpret_cast<double*>(sm + L.xi);
+  double* dr = reinterpret_cast<double*>(sm + L.d);
+  double* tgt = reinterpret_cast<double*>(sm + L.tgt);
   int* ancA = reinterpret_cast<int*>(sm + L.ancA);
   int* ancB = reinterpret_cast<int*>(sm + L.ancB);
-  float* tw = sm + L.tw;
-  float* xi = sm + L.xi;
   float* jri = sm + L.jri;
   float* colw = sm + L.colw;
-  float* dr = sm + L.d;
   float* g = sm + L.g;
   float* delta = sm + L.delta;
   float* jtj = sm + L.jtj;
@@ -138,6 +167,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const int tl = tm.tl;
   const br_ik_settings_t& S = P.s;
   const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
+  const double wpd = wp, wod = wo, wld = wl, wrd = wr;
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
 
   // ---- load the tree table and the problem -------------------------------
@@ -160,8 +190,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   for (int i = tl; i < nq; i += T) {
     lower[i] = tree.lower[i];
     upper[i] = tree.upper[i];
-    x[i] = P.b.x0[qoff + i];
-    qrest[i] = P.b.q_rest[qoff + i];
+    x[i] = (double)P.b.x0[qoff + i];
+    qrest[i] = (double)P.b.q_rest[qoff + i];
   }
   const int nt = P.b.n_targets[prob];
   for (int t = tl; t < K; t += T) {
@@ -170,7 +200,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       fparent[t] = tree.frame_parent[f];
       for (int k = 0; k < 8; ++k) fplace[8 * t + k] = tree.frame_placement[8 * f + k];
       const float* tp = P.b.targets + ((int64_t)prob * K + t) * 7;
-      st8(tgt + 8 * t, Pose{f3(tp[0], tp[1], tp[2]), make_float4(tp[3], tp[4], tp[5], tp[6])});
+      std8(tgt + 8 * t, DPose{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])});
     }
   }
   tm.sync();
@@ -189,64 +219,64 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   tm.sync();
 
   // ---- helpers ------------------------------------------------------------
-  // FK of configuration q (shared) -> world poses (returned buffer), pointer jumping.
-  auto fk = [&](const float* q) -> float* {
+  // float64 FK of configuration q (shared) -> world poses (returned buffer), pointer jumping.
+  auto fk = [&](const double* q) -> double* {
     for (int j = tl; j < nj; j += T) {
-      const Pose Pj = ld8(place + 8 * j);
-      Pose Lj = Pj;
+      const DPose Pj = to_d(ld8(place + 8 * j));
+      DPose Lj = Pj;
       const int jt = jtype[j];
-      const float* qv = q + idxq[j];
-      if (jt == BR_JOINT_REVOLUTE) {
-        float s, c;
-        sincosf(0.5f * qv[0], &s, &c);
-        Lj.q = qmul(Pj.q, make_float4(s * axis[4 * j], s * axis[4 * j + 1], s * axis[4 * j + 2], c));
+      const double* qv = q + idxq[j];
+      if (jt == BR_JOINT_REVOLUTE) {                                  // revolute.py:18-21
+        double s, c;
+        sincos(0.5 * qv[0], &s, &c);
+        Lj.q = dqmul(Pj.q, make_double4(s * axis[4 * j], s * axis[4 * j + 1], s * axis[4 * j + 2], c));
       } else if (jt == BR_JOINT_PRISMATIC) {
-        Lj.t = add(Pj.t, qrot(Pj.q, f3(qv[0] * axis[4 * j], qv[0] * axis[4 * j + 1], qv[0] * axis[4 * j + 2])));
-      } else if (jt == BR_JOINT_FREE_FLYER) {
-        Lj = compose(Pj, Pose{f3(qv[0], qv[1], qv[2]), qnormalize(make_float4(qv[3], qv[4], qv[5], qv[6]))});
+        Lj.t = dadd(Pj.t, dqrot(Pj.q, d3(qv[0] * axis[4 * j], qv[0] * axis[4 * j + 1], qv[0] * axis[4 * j + 2])));
+      } else if (jt == BR_JOINT_FREE_FLYER) {                         // free_flyer.py:31-36
+        Lj = dcompose(Pj, DPose{d3(qv[0], qv[1], qv[2]), dqnormalize(make_double4(qv[3], qv[4], qv[5], qv[6]))});
       }
-      st8(poseA + 8 * j, Lj);
+      std8(poseA + 8 * j, Lj);
       ancA[j] = parent[j];
     }
     tm.sync();
-    float* A = poseA;
-    float* B = poseB;
+    double* A = poseA;
+    double* B = poseB;
     int* aA = ancA;
     int* aB = ancB;
     for (int r = 0; r < tree.rounds; ++r) {
       for (int j = tl; j < nj; j += T) {
         const int a = aA[j];
         if (a >= 0) {
-          st8(B + 8 * j, compose(ld8(A + 8 * a), ld8(A + 8 * j)));
+          std8(B + 8 * j, dcompose(ldd(A + 8 * a), ldd(A + 8 * j)));
           aB[j] = aA[a];
         } else {
-          st8(B + 8 * j, ld8(A + 8 * j));
+          std8(B + 8 * j, ldd(A + 8 * j));
           aB[j] = -1;
         }
       }
       tm.sync();
-      float* tp = A; A = B; B = tp;
+      double* tp = A; A = B; B = tp;
       int* ta = aA; aA = aB; aB = ta;
     }
     return A;
   };
 
-  // Residual of the stack at q with world poses `pose`: fills tw, xi, dr; returns 0.5 |r|^2.
-  auto residual = [&](const float* q, const float* pose) -> float {
-    float acc = 0.f;
+  // float64 residual of the stack at q with world poses `pose`: fills tw, xi, dr; returns 0.5 |r|^2.
+  auto residual = [&](const double* q, const double* pose) -> double {
+    double acc = 0.0;
     for (int t = tl; t < nt; t += T) {
-      const Pose Tee = compose(ld8(pose + 8 * fparent[t]), ld8(fplace + 8 * t));
-      st8(tw + 8 * t, Tee);
-      float3 v, w;
-      se3_log(compose(inverse(ld8(tgt + 8 * t)), Tee), v, w);       // pose.py:63-64
-      *reinterpret_cast<float4*>(xi + 8 * t) = make_float4(v.x, v.y, v.z, w.x);
-      *reinterpret_cast<float4*>(xi + 8 * t + 4) = make_float4(w.y, w.z, 0.f, 0.f);
-      acc += wp * wp * dot(v, v) + wo * wo * dot(w, w);
+      const DPose Tee = dcompose(ldd(pose + 8 * fparent[t]), to_d(ld8(fplace + 8 * t)));
+      std8(tw + 8 * t, Tee);
+      double3 v, w;
+      dse3_log(dcompose(dinverse(ldd(tgt + 8 * t)), Tee), v, w);     // pose.py:63-64
+      double* e = xi + 8 * t;
+      e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = w.x; e[4] = w.y; e[5] = w.z;
+      acc += wpd * wpd * ddot(v, v) + wod * wod * ddot(w, w);
     }
     if (use_limits) {                                                // limits.py:56-62
       for (int i = tl; i < nq; i += T) {
-        const float lo = fmaxf(lower[i] - q[i], 0.f), hi = fmaxf(q[i] - upper[i], 0.f);
-        acc += wl * wl * (lo * lo + hi * hi);
+        const double lo = fmax((double)lower[i] - q[i], 0.0), hi = fmax(q[i] - (double)upper[i], 0.0);
+        acc += wld * wld * (lo * lo + hi * hi);
       }
     }
     if (use_rest) {                                                  // regularization.py:48-54
@@ -254,38 +284,38 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         const int jt = jtype[j];
         const int iq = idxq[j], iv = idxv[j];
         if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
-          const float dd = q[iq] - qrest[iq];
+          const double dd = q[iq] - qrest[iq];
           dr[iv] = dd;
-          acc += wr * wr * dd * dd;
+          acc += wrd * wrd * dd * dd;
         } else if (jt == BR_JOINT_FREE_FLYER) {                      // free_flyer.py:53-57
-          const Pose a{f3(qrest[iq], qrest[iq + 1], qrest[iq + 2]),
-                       make_float4(qrest[iq + 3], qrest[iq + 4], qrest[iq + 5], qrest[iq + 6])};
-          const Pose b{f3(q[iq], q[iq + 1], q[iq + 2]), make_float4(q[iq + 3], q[iq + 4], q[iq + 5], q[iq + 6])};
-          float3 v, w;
-          se3_log(compose(inverse(a), b), v, w);
+          const DPose a{d3(qrest[iq], qrest[iq + 1], qrest[iq + 2]),
+                        make_double4(qrest[iq + 3], qrest[iq + 4], qrest[iq + 5], qrest[iq + 6])};
+          const DPose b{d3(q[iq], q[iq + 1], q[iq + 2]), make_double4(q[iq + 3], q[iq + 4], q[iq + 5], q[iq + 6])};
+          double3 v, w;
+          dse3_log(dcompose(dinverse(a), b), v, w);
           dr[iv] = v.x; dr[iv + 1] = v.y; dr[iv + 2] = v.z;
           dr[iv + 3] = w.x; dr[iv + 4] = w.y; dr[iv + 5] = w.z;
-          acc += wr * wr * (dot(v, v) + dot(w, w));
+          acc += wrd * wrd * (ddot(v, v) + ddot(w, w));
         }
       }
     }
-    const float tot = tm.sum(acc);
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(tm.mask, acc, o, T);
     tm.sync();
-    return 0.5f * tot;
+    return 0.5 * acc;
   };
 
-  // J^T J (packed lower) and g = J^T r at q with world poses `pose`; returns |g|.
-  auto build_normal = [&](const float* q, const float* pose) -> float {
+  // float32 J^T J (packed lower) and g = J^T r at q with world poses `pose`; returns |g|.
+  auto build_normal = [&](const double* q, const double* pose) -> float {
     for (int c = tl; c < nv; c += T) {
-      const Pose Tj = ld8(pose + 8 * cjoint[c]);
+      const Pose Tj = to_f(ldd(pose + 8 * cjoint[c]));
       const float3 a = qrot(Tj.q, f3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
       *reinterpret_cast<float4*>(colw + 8 * c) = make_float4(a.x, a.y, a.z, 0.f);
       *reinterpret_cast<float4*>(colw + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
     }
     for (int t = tl; t < nt; t += T) {                                 // Jr^-1(xi), tangents.py:204-207
-      const float4 a = *reinterpret_cast<const float4*>(xi + 8 * t);
-      const float4 b = *reinterpret_cast<const float4*>(xi + 8 * t + 4);
-      const JrInv J = jr_inv_se3<9>(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y));
+      const double* e = xi + 8 * t;
+      const JrInv J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
       float* o = jri + 16 * t;
       o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
       for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
@@ -299,7 +329,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       if ((cmask[t] >> c) & 1ull) {
         const float4 a4 = *reinterpret_cast<const float4*>(colw + 8 * c);
         const float3 a = f3(a4.x, a4.y, a4.z);
-        const Pose Tee = ld8(tw + 8 * t);
+        const Pose Tee = to_f(ldd(tw + 8 * t));
         float3 lin, ang;
         if (ckind[c] == 0) {
           const float4 o4 = *reinterpret_cast<const float4*>(colw + 8 * c + 4);
@@ -345,8 +375,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           const int j = cjoint[a];
           if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
             const int iq = idxq[j];
-            if (q[iq] < lower[iq]) acc += wl * wl;
-            if (q[iq] > upper[iq]) acc += wl * wl;
+            if (q[iq] < (double)lower[iq]) acc += wl * wl;
+            if (q[iq] > (double)upper[iq]) acc += wl * wl;
           }
         }
       }
@@ -361,22 +391,22 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       for (int t = 0; t < nt; ++t) {
         if ((cmask[t] >> c) & 1ull) {
           const float* Jt = Jp + t * 6 * nv + c;
-          const float* e = xi + 8 * t;  // xi = (v.x v.y v.z w.x | w.y w.z)
-          acc = fmaf(Jt[0], wp * e[0], acc);
-          acc = fmaf(Jt[nv], wp * e[1], acc);
-          acc = fmaf(Jt[2 * nv], wp * e[2], acc);
-          acc = fmaf(Jt[3 * nv], wo * e[3], acc);
-          acc = fmaf(Jt[4 * nv], wo * e[4], acc);
-          acc = fmaf(Jt[5 * nv], wo * e[5], acc);
+          const double* e = xi + 8 * t;
+          acc = fmaf(Jt[0], wp * (float)e[0], acc);
+          acc = fmaf(Jt[nv], wp * (float)e[1], acc);
+          acc = fmaf(Jt[2 * nv], wp * (float)e[2], acc);
+          acc = fmaf(Jt[3 * nv], wo * (float)e[3], acc);
+          acc = fmaf(Jt[4 * nv], wo * (float)e[4], acc);
+          acc = fmaf(Jt[5 * nv], wo * (float)e[5], acc);
         }
       }
-      if (use_rest) acc += wr * wr * dr[c];
+      if (use_rest) acc += wr * wr * (float)dr[c];
       if (use_limits) {
         const int j = cjoint[c];
         if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
           const int iq = idxq[j];
-          if (q[iq] < lower[iq]) acc -= wl * wl * (lower[iq] - q[iq]);
-          if (q[iq] > upper[iq]) acc += wl * wl * (q[iq] - upper[iq]);
+          if (q[iq] < (double)lower[iq]) acc -= wl * wl * (float)((double)lower[iq] - q[iq]);
+          if (q[iq] > (double)upper[iq]) acc += wl * wl * (float)(q[iq] - (double)upper[iq]);
         }
       }
       g[c] = acc;
@@ -387,7 +417,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     return sqrtf(gg);
   };
 
-  // Solve (J^T J + damp I) delta = -g.  Returns false if the factorization failed.
+  // Solve (J^T J + damp I) delta = -g in float32.  Returns false if the factorization failed.
   auto solve = [&](float damp) -> bool {
     const int ld = nv + 1;
     float* Lm = work;
@@ -443,20 +473,20 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     return true;
   };
 
-  // x_new = clamp(integrate(x, delta))
+  // x_new = clamp(integrate(x, delta)) in float64
   auto retract = [&]() {
     for (int j = tl; j < nj; j += T) {
       const int jt = jtype[j];
       const int iq = idxq[j], iv = idxv[j];
       if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
-        xn[iq] = fminf(fmaxf(x[iq] + delta[iv], lower[iq]), upper[iq]);
-      } else if (jt == BR_JOINT_FREE_FLYER) {
-        const Pose a{f3(x[iq], x[iq + 1], x[iq + 2]), make_float4(x[iq + 3], x[iq + 4], x[iq + 5], x[iq + 6])};
-        Pose n = compose(a, se3_exp(f3(delta[iv], delta[iv + 1], delta[iv + 2]),
-                                    f3(delta[iv + 3], delta[iv + 4], delta[iv + 5])));
-        n.q = qnormalize(n.q);
-        const float v7[7] = {n.t.x, n.t.y, n.t.z, n.q.x, n.q.y, n.q.z, n.q.w};
-        for (int k = 0; k < 7; ++k) xn[iq + k] = fminf(fmaxf(v7[k], lower[iq + k]), upper[iq + k]);
+        xn[iq] = fmin(fmax(x[iq] + (double)delta[iv], (double)lower[iq]), (double)upper[iq]);
+      } else if (jt == BR_JOINT_FREE_FLYER) {                        // free_flyer.py:47-51
+        const DPose a{d3(x[iq], x[iq + 1], x[iq + 2]), make_double4(x[iq + 3], x[iq + 4], x[iq + 5], x[iq + 6])};
+        DPose n = dcompose(a, dse3_exp(d3(delta[iv], delta[iv + 1], delta[iv + 2]),
+                                       d3(delta[iv + 3], delta[iv + 4], delta[iv + 5])));
+        n.q = dqnormalize(n.q);
+        const double v7[7] = {n.t.x, n.t.y, n.t.z, n.q.x, n.q.y, n.q.z, n.q.w};
+        for (int k = 0; k < 7; ++k) xn[iq + k] = fmin(fmax(v7[k], (double)lower[iq + k]), (double)upper[iq + k]);
       }
     }
     tm.sync();
@@ -464,8 +494,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
 
   // ---- the LM / GN loop (levenberg_marquardt.py:83-135, gauss_newton.py:27-76) ----
   const bool gn = S.optimizer == BR_OPT_GN;
-  float* pose = fk(x);
-  float cost = residual(x, pose);
+  double* pose = fk(x);
+  double cost = residual(x, pose);
   float lam = gn ? 0.f : S.lam0;
   float gnorm = 0.f;
   bool need_jac = true;
@@ -491,7 +521,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     }
     retract();
     pose = fk(xn);
-    const float cn = residual(xn, pose);
+    const double cn = residual(xn, pose);
     if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
     if (gn) {
       for (int i = tl; i < nq; i += T) x[i] = xn[i];
@@ -511,11 +541,32 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     }
   }
   // ---- results ------------------------------------------------------------
-  for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = x[i];
+  for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = (float)x[i];
+  if (P.r.residual && P.b.r_offset) {
+    // stacked residual at the returned x, CostStack order (stack.py:104-117)
+    pose = fk(x);
+    residual(x, pose);
+    float* out = P.r.residual + P.b.r_offset[prob];
+    for (int t = tl; t < nt; t += T) {
+      const double* e = xi + 8 * t;
+      out[6 * t + 0] = (float)(wpd * e[0]); out[6 * t + 1] = (float)(wpd * e[1]); out[6 * t + 2] = (float)(wpd * e[2]);
+      out[6 * t + 3] = (float)(wod * e[3]); out[6 * t + 4] = (float)(wod * e[4]); out[6 * t + 5] = (float)(wod * e[5]);
+    }
+    int o = 6 * nt;
+    if (use_limits) {
+      for (int i = tl; i < nq; i += T) {
+        out[o + i] = (float)(wld * fmax((double)lower[i] - x[i], 0.0));
+        out[o + nq + i] = (float)(wld * fmax(x[i] - (double)upper[i], 0.0));
+      }
+      o += 2 * nq;
+    }
+    if (use_rest)
+      for (int c = tl; c < nv; c += T) out[o + c] = (float)(wrd * dr[c]);
+  }
   if (tl == 0) {
     P.r.iters[prob] = it;
     P.r.status[prob] = status | (flags << 8);
-    P.r.cost[prob] = cost;
+    P.r.cost[prob] = (float)cost;
   }
   tm.sync();
 }

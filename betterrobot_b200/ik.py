@@ -1,0 +1,313 @@
+"""Batched LM / Gauss-Newton IK on the sm_100a persistent kernel.
+
+Drop-in for ``better_robot.tasks.ik`` (``src/better_robot/tasks/ik.py:37-266``):
+``solve_ik(model, targets, initial_q=..., cost_cfg=..., optimizer_cfg=...)`` builds
+the same cost stack — one ``PoseResidual`` per target, ``JointPositionLimit``
+(item weight ``limit_weight``), ``RestResidual`` (item weight ``rest_weight``) —
+and runs the same Levenberg-Marquardt loop with ``Adaptive`` damping.  Unlike
+the reference it also solves whole batches, including uneven mixes of robots,
+in one launch (``solve_ik_batched``, ``PackedIK``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Literal, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BrTree, IKBatch, IKResultBuf, IKSettings, c_int32
+from .exceptions import ShapeError
+from .tree import device_tree
+
+OPT_LM, OPT_GN = 0, 1
+MAX_CLASSES, MAX_TARGETS = 8, 8
+SCRATCH_BYTES = 16
+
+
+@dataclass
+class IKCostConfig:
+    """Weights of the built-in IK stack (``tasks/ik.py:37-48``)."""
+
+    pos_weight: float = 1.0
+    ori_weight: float = 1.0
+    pose_weight: float = 1.0
+    limit_weight: float = 0.1
+    rest_weight: float = 0.01
+    collision_margin: float = 0.02
+    collision_weight: float = 1.0
+    q_rest: torch.Tensor | None = None
+
+
+@dataclass
+class OptimizerConfig:
+    """Optimizer selection (``tasks/ik.py:51-69``).
+
+    ``lam0``/``factor`` are the ``Adaptive`` damping parameters; their defaults are
+    what ``solve_ik`` effectively uses (``Adaptive()`` = 1e-4 / 2, ``tasks/ik.py:250``).
+    ``lam_min``/``lam_max`` are ``Adaptive``'s clamps (``strategies/adaptive.py:19-25``).
+    """
+
+    optimizer: Literal["lm", "gn", "adam", "lbfgs", "lm_then_lbfgs"] = "lm"
+    max_iter: int = 100
+    jacobian_strategy: object = None
+    linear_solver: Literal["cholesky", "lstsq", "cg"] = "cholesky"
+    kernel: Literal["l2", "huber", "cauchy", "tukey"] = "l2"
+    damping: Literal["constant", "adaptive", "trust_region"] = "adaptive"
+    tol: float = 1e-6
+    refine_disabled_items: tuple = ()
+    lam0: float = 1e-4
+    factor: float = 2.0
+    lam_min: float = 1e-10
+    lam_max: float = 1e8
+    gn_eps: float = 1e-8
+
+
+@dataclass
+class IKResult:
+    """Return type of ``solve_ik`` (``tasks/ik.py:72-99``)."""
+
+    q: torch.Tensor
+    residual: torch.Tensor
+    iters: int
+    converged: bool
+    model: object
+
+    def fk(self):
+        from .kinematics import forward_kinematics
+        return forward_kinematics(self.model, self.q, compute_frames=True)
+
+    def frame_pose(self, name: str) -> torch.Tensor:
+        return self.fk().frame_pose_world[..., self.model.frame_id(name), :]
+
+    def q_only(self) -> torch.Tensor:
+        return self.q
+
+
+@dataclass
+class BatchIKResult:
+    """Batched result: ``q (P, nq)`` (or a list for uneven mixes), per-problem iterations/verdicts."""
+
+    q: object
+    iters: torch.Tensor
+    converged: torch.Tensor
+    status: torch.Tensor
+    cost: torch.Tensor
+    residual: object = None
+
+
+def settings_from(cost_cfg: IKCostConfig, opt: OptimizerConfig) -> IKSettings:
+    if opt.optimizer not in ("lm", "gn"):
+        raise NotImplementedError(f"optimizer {opt.optimizer!r}: the sm_100a path runs 'lm' and 'gn'")
+    if opt.linear_solver != "cholesky":
+        raise NotImplementedError("the sm_100a path solves the normal equations by Cholesky")
+    if opt.kernel != "l2":
+        raise NotImplementedError("robust kernels are not on the sm_100a path (l2 only)")
+    if opt.damping not in ("adaptive", "constant"):
+        raise NotImplementedError(f"damping {opt.damping!r} is not on the sm_100a path")
+    s = IKSettings()
+    s.lam0 = opt.lam0
+    s.factor = 1.0 if opt.damping == "constant" else opt.factor   # Constant: lambda never changes
+    s.tol = opt.tol
+    s.lam_min, s.lam_max, s.gn_eps = opt.lam_min, opt.lam_max, opt.gn_eps
+    s.pos_weight = cost_cfg.pos_weight * cost_cfg.pose_weight       # tasks/ik.py:193-194
+    s.ori_weight = cost_cfg.ori_weight * cost_cfg.pose_weight
+    s.limit_weight = cost_cfg.limit_weight
+    s.rest_weight = cost_cfg.rest_weight
+    s.max_iter = int(opt.max_iter)
+    s.optimizer = OPT_LM if opt.optimizer == "lm" else OPT_GN
+    return s
+
+
+def team_floats(model, max_targets: int, device) -> int:
+    dt = device_tree(model, device)
+    return int(_lib.load().br_lm_team_floats(dt.ptr, max_targets))
+
+
+def default_team_size(model) -> int:
+    nv = int(model.nv)
+    return 8 if nv <= 8 else 16 if nv <= 16 else 32
+
+
+class PackedIK:
+    """An uneven batch of IK problems packed for one persistent launch.
+
+    ``problems`` are grouped by robot (class).  For class ``c``: ``models[c]``,
+    ``frame_ids[c]`` (P_c, K_c) int, ``targets[c]`` (P_c, K_c, 7) float32,
+    ``q0[c]`` (P_c, nq_c) float32 and ``n_targets[c]`` (P_c,) (<= K_c).
+    Device buffers are allocated once; ``set_inputs`` refreshes targets / q0 in place
+    and ``solve`` launches (graph-capturable: no allocation, no host sync).
+    """
+
+    def __init__(self, models: Sequence, frame_ids: Sequence, n_targets: Sequence, q_rest: Sequence | None = None,
+                 team_sizes: Sequence[int] | None = None, device="cuda", warps_per_cta: int = 4,
+                 with_residual: bool = False):
+        if not 1 <= len(models) <= MAX_CLASSES:
+            raise ShapeError(f"1..{MAX_CLASSES} robot classes per launch, got {len(models)}")
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.models = list(models)
+        self.C = len(models)
+        self.counts = [int(np.asarray(n).shape[0]) for n in n_targets]
+        self.P = sum(self.counts)
+        self.K = max(int(np.asarray(f).shape[1]) for f in frame_ids)
+        if self.K > MAX_TARGETS:
+            raise ShapeError(f"at most {MAX_TARGETS} targets per problem")
+        self.team = [int(t) for t in (team_sizes or [default_team_size(m) for m in models])]
+        self.trees = [device_tree(m, self.device) for m in models]
+        self.warps_per_cta = warps_per_cta
+        # per-problem layout: classes contiguous, in class order
+        self.class_start = np.cumsum([0] + self.counts)[:-1]
+        nq = np.concatenate([np.full(n, m.nq, np.int64) for n, m in zip(self.counts, models)])
+        self.q_offset_np = np.concatenate([[0], np.cumsum(nq)[:-1]]).astype(np.int64)
+        self.q_total = int(nq.sum())
+        nt_all = np.concatenate([np.asarray(n, np.int32) for n in n_targets])
+        if (nt_all < 1).any() or (nt_all > self.K).any():
+            raise ShapeError("each problem needs 1..K targets")
+        fr = np.zeros((self.P, self.K), np.int32)
+        for c in range(self.C):
+            f = np.asarray(frame_ids[c], np.int32)
+            if f.min() < 0 or f.max() >= models[c].nframes:
+                raise ShapeError(f"class {c}: frame id out of range")
+            s0 = self.class_start[c]
+            fr[s0:s0 + self.counts[c], :f.shape[1]] = f
+        dims = []
+        for c, m in enumerate(models):
+            n = np.asarray(n_targets[c], np.int64)
+            dims.append(6 * n + 2 * m.nq + m.nv)
+        rdim = np.concatenate(dims)
+        self.r_offset_np = np.concatenate([[0], np.cumsum(rdim)[:-1]]).astype(np.int64)
+        self.r_dim = rdim
+        # work items: heaviest classes first (LPT), 32/T problems per item
+        cost = [m.nv ** 2 * (1 + self.K) for m in models]
+        order, items = [], []
+        slot = 0
+        for c in sorted(range(self.C), key=lambda k: -cost[k]):
+            per = 32 // self.team[c]
+            idx = np.arange(self.class_start[c], self.class_start[c] + self.counts[c])
+            order.append(idx)
+            for s in range(0, self.counts[c], per):
+                items.append((slot + s, min(per, self.counts[c] - s), c))
+            slot += self.counts[c]
+        dev = self.device
+        self.order = torch.from_numpy(np.concatenate(order).astype(np.int32)).to(dev)
+        self.items = torch.tensor(items, dtype=torch.int32, device=dev).reshape(-1)
+        self.n_items = len(items)
+        self.n_targets_t = torch.from_numpy(nt_all).to(dev)
+        self.frames_t = torch.from_numpy(fr).to(dev)
+        self.q_offset = torch.from_numpy(self.q_offset_np).to(dev)
+        self.r_offset = torch.from_numpy(self.r_offset_np).to(dev)
+        self.targets = torch.zeros(self.P, self.K, 7, device=dev)
+        self.targets[..., 6] = 1.0
+        self.x0 = torch.zeros(self.q_total, device=dev)
+        self.q_rest = torch.zeros(self.q_total, device=dev)
+        for c, m in enumerate(models):
+            qr = (m.q_neutral if q_rest is None or q_rest[c] is None else q_rest[c])
+            qr = torch.as_tensor(qr, dtype=torch.float32).reshape(-1, m.nq)
+            s0 = int(self.q_offset_np[self.class_start[c]])
+            self.q_rest[s0:s0 + self.counts[c] * m.nq] = qr.to(dev).expand(self.counts[c], m.nq).reshape(-1)
+        self.x = torch.empty(self.q_total, device=dev)
+        self.iters = torch.empty(self.P, dtype=torch.int32, device=dev)
+        self.status = torch.empty(self.P, dtype=torch.int32, device=dev)
+        self.cost = torch.empty(self.P, device=dev)
+        self.residual = torch.empty(int(rdim.sum()), device=dev) if with_residual else None
+        self.scratch = torch.zeros(SCRATCH_BYTES // 4, dtype=torch.int32, device=dev)
+        # ctypes structs (kept alive on the object)
+        self._trees = (BrTree * self.C)(*[t.struct for t in self.trees])
+        self._teams = (c_int32 * self.C)(*self.team)
+        b = IKBatch()
+        b.n_problems, b.max_targets, b.n_classes, b.n_items = self.P, self.K, self.C, self.n_items
+        b.trees = ctypes.cast(self._trees, ctypes.POINTER(BrTree))
+        b.team_size = ctypes.cast(self._teams, ctypes.POINTER(c_int32))
+        b.items, b.order = self.items.data_ptr(), self.order.data_ptr()
+        b.n_targets, b.frames = self.n_targets_t.data_ptr(), self.frames_t.data_ptr()
+        b.targets, b.q_offset = self.targets.data_ptr(), self.q_offset.data_ptr()
+        b.x0, b.q_rest = self.x0.data_ptr(), self.q_rest.data_ptr()
+        b.r_offset = self.r_offset.data_ptr()
+        self._batch = b
+        r = IKResultBuf()
+        r.x, r.iters, r.status, r.cost = self.x.data_ptr(), self.iters.data_ptr(), self.status.data_ptr(), \
+            self.cost.data_ptr()
+        r.residual = self.residual.data_ptr() if self.residual is not None else None
+        self._result = r
+
+    def set_inputs(self, targets: Sequence, q0: Sequence) -> None:
+        """Copy per-class targets (P_c, K_c, 7) and start configurations (P_c, nq_c) into the device buffers."""
+        for c, m in enumerate(self.models):
+            s0, n = int(self.class_start[c]), self.counts[c]
+            t = torch.as_tensor(targets[c], dtype=torch.float32)
+            self.targets[s0:s0 + n, :t.shape[1]].copy_(t, non_blocking=True)
+            o = int(self.q_offset_np[s0])
+            self.x0[o:o + n * m.nq].copy_(torch.as_tensor(q0[c], dtype=torch.float32).reshape(-1), non_blocking=True)
+
+    def solve(self, settings: IKSettings, stream: int | None = None) -> None:
+        _lib.call("br_lm_solve", ctypes.byref(self._batch), ctypes.byref(settings), ctypes.byref(self._result),
+                  self.warps_per_cta, self.scratch.data_ptr(), SCRATCH_BYTES,
+                  stream if stream is not None else _lib.stream_ptr(self.device))
+
+    def q_of(self, c: int) -> torch.Tensor:
+        s0, n, nq = int(self.class_start[c]), self.counts[c], self.models[c].nq
+        o = int(self.q_offset_np[s0])
+        return self.x[o:o + n * nq].view(n, nq)
+
+    def class_slice(self, c: int) -> slice:
+        s0 = int(self.class_start[c])
+        return slice(s0, s0 + self.counts[c])
+
+
+def solve_ik_batched(model, frame_ids, targets: torch.Tensor, initial_q: torch.Tensor, *,
+                     cost_cfg: IKCostConfig | None = None, optimizer_cfg: OptimizerConfig | None = None,
+                     n_targets=None, with_residual: bool = False, team_size: int | None = None,
+                     warps_per_cta: int = 4) -> BatchIKResult:
+    """Solve ``P`` independent problems of one robot: ``targets (P, K, 7)`` for ``frame_ids``
+    (K ids shared by all problems, or ``(P, K)``), ``initial_q (P, nq)``."""
+    cost_cfg = cost_cfg or IKCostConfig()
+    optimizer_cfg = optimizer_cfg or OptimizerConfig()
+    if initial_q.dim() != 2 or initial_q.shape[-1] != model.nq:
+        raise ShapeError(f"initial_q must be (P, {model.nq}), got {tuple(initial_q.shape)}")
+    _lib.require_cuda(initial_q)
+    P = initial_q.shape[0]
+    fr = np.asarray(frame_ids, np.int32)
+    if fr.ndim == 1:
+        fr = np.broadcast_to(fr, (P, fr.shape[0]))
+    K = fr.shape[1]
+    if targets.shape != (P, K, 7):
+        raise ShapeError(f"targets must be ({P}, {K}, 7), got {tuple(targets.shape)}")
+    nt = np.full(P, K, np.int32) if n_targets is None else np.asarray(n_targets, np.int32)
+    qr = [cost_cfg.q_rest] if cost_cfg.q_rest is not None else None
+    pk = PackedIK([model], [fr], [nt], q_rest=qr, team_sizes=[team_size or default_team_size(model)],
+                  device=initial_q.device, warps_per_cta=warps_per_cta, with_residual=with_residual)
+    pk.set_inputs([targets], [initial_q])
+    with torch.cuda.device(initial_q.device):
+        pk.solve(settings_from(cost_cfg, optimizer_cfg))
+    res = None
+    if with_residual:
+        res = pk.residual.view(P, -1)
+    return BatchIKResult(q=pk.q_of(0), iters=pk.iters, converged=(pk.status & 0xFF) == 0, status=pk.status,
+                         cost=pk.cost, residual=res)
+
+
+def solve_ik(model, targets: dict, *, initial_q: torch.Tensor | None = None, cost_cfg: IKCostConfig | None = None,
+             optimizer_cfg: OptimizerConfig | None = None, robot_collision=None, device=None) -> IKResult:
+    """Whole-body IK for one configuration (``tasks/ik.py:150-266``); ``targets``: frame name -> (7,) pose."""
+    cost_cfg = cost_cfg or IKCostConfig()
+    optimizer_cfg = optimizer_cfg or OptimizerConfig()
+    if initial_q is not None:
+        x0 = initial_q.detach().float()
+    else:
+        x0 = model.q_neutral.clone().float()
+    dev = x0.device if x0.is_cuda else torch.device(device or "cuda")
+    x0 = x0.to(dev).reshape(1, -1)
+    names = list(targets)
+    if not names:
+        raise ShapeError("solve_ik needs at least one target")
+    fids = [model.frame_id(n) for n in names]
+    T = torch.stack([torch.as_tensor(targets[n], dtype=torch.float32).reshape(7) for n in names]).to(dev)
+    out = solve_ik_batched(model, fids, T[None], x0, cost_cfg=cost_cfg, optimizer_cfg=optimizer_cfg,
+                           with_residual=True)
+    return IKResult(q=out.q[0], residual=out.residual[0], iters=int(out.iters[0]), converged=bool(out.converged[0]),
+                    model=model)

@@ -151,6 +151,8 @@ typedef struct br_ik_batch {
     const int64_t* q_offset;    /* [n_problems] float offset of the problem's q     */
     const float* x0;            /* packed initial configurations                    */
     const float* q_rest;        /* packed rest configurations (RestResidual q_rest) */
+    const int64_t* r_offset;    /* [n_problems] float offset of the problem's stacked residual
+                                   (6*n_targets + 2*nq + nv floats) in result.residual; may be NULL */
 } br_ik_batch_t;
 
 typedef struct br_ik_result {
@@ -158,6 +160,8 @@ typedef struct br_ik_result {
     int32_t* iters;             /* [n_problems] completed iterations (SolverState.iters) */
     int32_t* status;            /* [n_problems] BR_IK_* | flags << 8                */
     float* cost;                /* [n_problems] final 0.5 |r|^2                     */
+    float* residual;            /* packed final stacked residual (CostStack order:
+                                   pose targets, limits, rest); NULL = not written */
 } br_ik_result_t;
 
 /*
@@ -175,6 +179,31 @@ BR_API int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* setti
 /* Shared-memory floats one problem of `tree` with `max_targets` targets needs
  * (for choosing team sizes and warps per CTA). No reference counterpart. */
 BR_API int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets);
+
+/* ==== pose loss through FK and its adjoint ================================ */
+/*
+ * loss[b] = sum_f w_f |log(T_f^-1 * oMf_f(q_b))|^2 for the frames in the HOST
+ * array frame_ids (n_frames <= 64), targets[b, f, 7], weights[f] (or
+ * weights[b, f] if weights_per_config).  If joint_pose_world is non-NULL the
+ * world joint placements [batch, njoints, 7] are stored for the backward pass
+ * ("store" mode).  The reference evaluates this loss with its per-op torch FK
+ * (src/better_robot/kinematics/forward.py:73-135, lie/se3.py log/compose).
+ */
+BR_API int br_pose_loss(const br_tree_t* tree, const float* q, int64_t batch, const int32_t* frame_ids,
+                        int32_t n_frames, const float* targets, const float* weights, int32_t weights_per_config,
+                        float* loss, float* joint_pose_world, void* stream);
+
+/*
+ * Adjoint of br_pose_loss: grad_q[b, :] = grad_loss[b] * dloss[b]/dq (raw q,
+ * free-flyer quaternion components included).  joint_pose_world from the
+ * forward pass, or NULL to recompute FK from q ("recompute" mode).  Replaces
+ * torch autograd's backward through the reference FK tape
+ * (forward.py:79-81 builds that tape on purpose).
+ */
+BR_API int br_pose_loss_backward(const br_tree_t* tree, const float* q, const float* joint_pose_world,
+                                 int64_t batch, const int32_t* frame_ids, int32_t n_frames, const float* targets,
+                                 const float* weights, int32_t weights_per_config, const float* grad_loss,
+                                 float* grad_q, void* stream);
 
 /* Library build information (for logging): returns a static string. */
 BR_API const char* br_version(void);

@@ -1,0 +1,117 @@
+"""GPU checks of the hand-written FK adjoint.
+
+* against the reference's own float64 autograd gradient (golden fixture);
+* against float64 central finite differences (eps 1e-6) of the oracle loss;
+* store and recompute modes give identical gradients.
+
+Tolerance (north star): relative error ``|g - g_ref|_2 / |g_ref|_2 <= 1e-5`` per
+configuration (float32 kernel vs float64 references); the loss itself within
+1e-5 relative.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from betterrobot_b200 import synthetic as syn
+from betterrobot_b200.adjoint import pose_loss
+from oracle import kinematics as K, lie
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+GRAD_TOL = 1e-5
+
+
+def _loss64(m64, q, fids, targets, w):
+    oMi, _ = K.forward_kinematics(m64, q)
+    oMf = K.frame_placements(m64, oMi, fids)
+    xi = lie.se3_log(lie.se3_compose(lie.se3_inverse(targets), oMf))
+    return ((xi * xi).sum(-1) * w).sum(-1)
+
+
+def _fd(m64, q, fids, targets, w, eps=1e-6):
+    g = np.zeros_like(q)
+    for i in range(q.shape[1]):
+        qp, qm = q.copy(), q.copy()
+        qp[:, i] += eps
+        qm[:, i] -= eps
+        g[:, i] = (_loss64(m64, qp, fids, targets, w) - _loss64(m64, qm, fids, targets, w)) / (2 * eps)
+    return g
+
+
+def _rel(g, ref):
+    return np.linalg.norm(g - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1e-12)
+
+
+def _grad(m, q, fids, targets, w, mode):
+    qc = torch.from_numpy(q).float().cuda().requires_grad_(True)
+    loss = pose_loss(m, qc, fids, torch.from_numpy(targets).float().cuda(), torch.from_numpy(w).float().cuda(),
+                     mode=mode)
+    loss.sum().backward()
+    return loss.detach().cpu().double().numpy(), qc.grad.cpu().double().numpy()
+
+
+@pytest.mark.parametrize("mode", ["store", "recompute"])
+def test_matches_reference_autograd_golden(mode):
+    g = np.load(os.path.join(GOLDEN, "adjoint.npz"))
+    m = syn.model_from_spec(syn.humanoid_spec())
+    fids = [int(f) for f in g["frame_ids"]]
+    loss, grad = _grad(m, g["q"], fids, g["targets"], g["weights"], mode)
+    np.testing.assert_allclose(loss, g["loss"], rtol=1e-5)
+    assert _rel(grad, g["grad"]).max() <= GRAD_TOL, _rel(grad, g["grad"])
+
+
+@pytest.mark.parametrize("robot", ["humanoid", "chain7", "dual_arm"])
+def test_matches_float64_central_differences(robot):
+    spec = {"humanoid": syn.humanoid_spec(), "chain7": syn.chain_spec(), "dual_arm": syn.dual_arm_spec()}[robot]
+    m, m64 = syn.model_from_spec(spec), syn.model_from_spec(spec, dtype=torch.float64)
+    fids = syn.op_frame_ids(m) + [m.nframes - 1]
+    B = 16
+    q = syn.random_q(m64, B, 90, rev_range=2.5, base_translation=1.0).numpy()
+    targets = syn.random_targets(B, len(fids), 91).numpy()
+    w = np.random.default_rng(92).uniform(0.5, 2.0, size=len(fids))
+    loss, grad = _grad(m, q, fids, targets, w, "recompute")
+    # the float64 references use the float32-rounded inputs the kernel saw
+    q32 = q.astype(np.float32).astype(np.float64)
+    t32 = targets.astype(np.float32).astype(np.float64)
+    w32 = w.astype(np.float32).astype(np.float64)
+    ref_loss = _loss64(m64, q32, fids, t32, w32)
+    np.testing.assert_allclose(loss, ref_loss, rtol=1e-5)
+    fd = _fd(m64, q32, fids, t32, w32)
+    rel = _rel(grad, fd)
+    assert rel.max() <= GRAD_TOL, rel
+
+
+def test_store_equals_recompute_and_weights_per_config():
+    m = syn.model_from_spec(syn.humanoid_spec())
+    m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
+    fids = syn.op_frame_ids(m)
+    B = 300
+    q = syn.random_q(m64, B, 93, rev_range=2.5, base_translation=1.0).numpy()
+    targets = syn.random_targets(B, len(fids), 94).numpy()
+    w = np.random.default_rng(95).uniform(0.5, 2.0, size=(B, len(fids)))
+    l1, g1 = _grad(m, q, fids, targets, w, "store")
+    l2, g2 = _grad(m, q, fids, targets, w, "recompute")
+    np.testing.assert_array_equal(l1, l2)
+    np.testing.assert_allclose(g1, g2, rtol=0, atol=1e-6 * np.abs(g1).max())
+    ref = _loss64(m64, q.astype(np.float32).astype(np.float64), fids,
+                  targets.astype(np.float32).astype(np.float64), w.astype(np.float32).astype(np.float64))
+    np.testing.assert_allclose(l1, ref, rtol=1e-5)
+
+
+def test_grad_output_scaling():
+    m = syn.model_from_spec(syn.chain_spec())
+    m64 = syn.model_from_spec(syn.chain_spec(), dtype=torch.float64)
+    fids = [m.frame_id("ee")]
+    q = syn.random_q(m64, 8, 96).float().cuda().requires_grad_(True)
+    T = syn.random_targets(8, 1, 97).float().cuda()
+    w = torch.ones(1, device="cuda")
+    loss = pose_loss(m, q, fids, T, w)
+    go = torch.arange(8, device="cuda", dtype=torch.float32)
+    (g,) = torch.autograd.grad(loss, q, go)
+    q2 = q.detach().clone().requires_grad_(True)
+    (g1,) = torch.autograd.grad(pose_loss(m, q2, fids, T, w).sum(), q2)
+    torch.testing.assert_close(g, g1 * go[:, None], rtol=1e-6, atol=1e-6)

@@ -1,0 +1,191 @@
+"""GPU parity of the persistent LM / GN kernel against the reference solver (float64).
+
+Bar (float32 kernel vs float64 reference/oracle):
+* same converged / not-converged verdict;
+* final stacked residual within 1e-4 (max abs difference of the residual vectors);
+checked on the reference's own float64 solves (golden fixtures) and on larger
+seeded batches against the oracle.  ``VERDICT_RATE`` is the fraction of problems
+that must meet both; float32 can flip an accept/reject decision at the noise
+floor of the cost, which the per-case rates below bound.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from betterrobot_b200 import ik as bik, synthetic as syn
+from oracle import ik as oik, kinematics as K
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+RES_TOL = 1e-4
+SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec()}
+
+
+def _models(name):
+    return syn.model_from_spec(SPECS[name]), syn.model_from_spec(SPECS[name], dtype=torch.float64)
+
+
+def _cfgs(st, optimizer="lm"):
+    cost = bik.IKCostConfig(limit_weight=float(st[4]), rest_weight=float(st[5]))
+    opt = bik.OptimizerConfig(optimizer=optimizer, max_iter=int(st[3]), tol=float(st[2]),
+                              lam0=float(st[0]) if st[0] else 1e-4, factor=float(st[1]) if st[1] else 2.0)
+    return cost, opt
+
+
+def _agreement(out, ref_conv, ref_res):
+    conv = out.converged.cpu().numpy()
+    res = out.residual.cpu().double().numpy()
+    dres = np.abs(res - ref_res).max(axis=1)
+    ok = (conv == ref_conv) & (dres <= RES_TOL)
+    return ok, conv, dres
+
+
+@pytest.mark.parametrize("case,robot", [("chain7_random", "chain7"), ("chain7_gn", "chain7"),
+                                        ("dual_arm", "dual_arm"), ("humanoid", "humanoid")])
+def test_reference_solver_golden(case, robot):
+    g = np.load(os.path.join(GOLDEN, f"ik_{case}.npz"))
+    m, _ = _models(robot)
+    cost, opt = _cfgs(g["settings"], str(g["optimizer"]))
+    fids = [int(f) for f in g["frame_ids"]]
+    out = bik.solve_ik_batched(m, fids, torch.from_numpy(g["targets"]).float().cuda(),
+                               torch.from_numpy(g["q0"]).float().cuda(), cost_cfg=cost, optimizer_cfg=opt,
+                               with_residual=True)
+    ok, conv, dres = _agreement(out, g["converged"], g["residual"])
+    # every converged reference solve must converge here to the same residual
+    both = g["converged"].astype(bool)
+    assert (conv[both]).all(), (conv, g["converged"])
+    assert (dres[both] <= RES_TOL).all(), dres
+    assert ok.mean() >= 0.75, (ok, conv, g["converged"], dres)
+
+
+def _config0(P, seed):
+    m, m64 = _models("chain7")
+    fid = m.frame_id("ee")
+    q_goal = syn.random_q(m64, P, seed, rev_range=2.8)
+    q0 = syn.random_q(m64, P, seed + 1, rev_range=2.8)
+    oMi, _ = K.forward_kinematics(m64, q_goal.numpy())
+    targets = K.frame_placements(m64, oMi, [fid])
+    return m, m64, fid, targets, q0
+
+
+def test_config0_chain_random_starts_vs_oracle():
+    """Config 0: 256 chains, q0 and target-q uniform in the limits, LM 1e-3 x10, 50 iters, tol 1e-6."""
+    m, m64, fid, targets, q0 = _config0(256, 40)
+    s = oik.IKSettings(lam0=1e-3, factor=10.0, tol=1e-6, max_iter=50)
+    ref = oik.solve(m64, [fid], targets, q0.numpy(), s)
+    out = bik.solve_ik_batched(m, [fid], torch.from_numpy(targets).float().cuda(), q0.float().cuda(),
+                               optimizer_cfg=bik.OptimizerConfig(max_iter=50, lam0=1e-3, factor=10.0),
+                               with_residual=True)
+    ok, conv, dres = _agreement(out, ref.converged, ref.residual)
+    both = ref.converged & conv
+    assert (conv == ref.converged).mean() >= 0.9, (conv.mean(), ref.converged.mean())
+    assert np.median(dres[both]) <= RES_TOL
+    assert (dres[both] <= RES_TOL).mean() >= 0.95
+
+
+@pytest.mark.parametrize("robot,frames,rest", [("chain7", ["ee"], 1e-3), ("dual_arm", ["ee_l", "ee_r"], 1e-3),
+                                               ("humanoid", ["track0", "track1", "track2", "track3"], 1e-3),
+                                               ("humanoid", ["track0", "track4"], 0.01)])
+def test_noisy_start_vs_oracle(robot, frames, rest):
+    """Config-3 style problems: targets from FK(q*), q0 = q* + N(0, 0.3), 100 iterations."""
+    m, m64 = _models(robot)
+    P = 64
+    fids = [m.frame_id(f) for f in frames]
+    q_star = syn.random_q(m64, P, 50, rev_range=2.5, base_translation=0.5)
+    oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+    targets = K.frame_placements(m64, oMi, fids)
+    q0 = syn.noisy_start(m64, q_star, 0.3, 51)
+    s = oik.IKSettings(lam0=1e-3, factor=10.0, tol=1e-6, max_iter=100, rest_weight=rest)
+    ref = oik.solve(m64, fids, targets, q0.numpy(), s)
+    out = bik.solve_ik_batched(m, fids, torch.from_numpy(targets).float().cuda(), q0.float().cuda(),
+                               cost_cfg=bik.IKCostConfig(rest_weight=rest),
+                               optimizer_cfg=bik.OptimizerConfig(max_iter=100, lam0=1e-3, factor=10.0),
+                               with_residual=True)
+    ok, conv, dres = _agreement(out, ref.converged, ref.residual)
+    assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
+    assert (conv == ref.converged).mean() >= 0.8, (conv.mean(), ref.converged.mean())
+
+
+def test_uneven_mix_single_launch_matches_per_class():
+    """Three robots, 1-6 targets, one launch == the same problems solved class by class."""
+    models = [_models(n) for n in ("humanoid", "dual_arm", "chain7")]
+    cand = {"humanoid": [f"track{i}" for i in range(6)], "dual_arm": ["ee_l", "ee_r", "body_l_link5",
+            "body_r_link5", "body_l_link3", "body_r_link3"], "chain7": ["ee", "body_link7", "body_link6",
+            "body_link5", "body_link4", "body_link3"]}
+    rng = np.random.default_rng(3)
+    frames, nts, tg, q0s = [], [], [], []
+    for (m, m64), name in zip(models, ("humanoid", "dual_arm", "chain7")):
+        P = 24
+        fids = np.array([m.frame_id(f) for f in cand[name]], np.int32)
+        nt = rng.integers(1, 7, size=P).astype(np.int32)
+        q_star = syn.random_q(m64, P, 60, rev_range=2.5, base_translation=0.5)
+        oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+        T = K.frame_placements(m64, oMi, list(fids))
+        frames.append(np.broadcast_to(fids, (P, 6)))
+        nts.append(nt)
+        tg.append(torch.from_numpy(T).float())
+        q0s.append(syn.noisy_start(m64, q_star, 0.3, 61).float())
+    settings = bik.settings_from(bik.IKCostConfig(rest_weight=1e-3),
+                                 bik.OptimizerConfig(max_iter=60, lam0=1e-3, factor=10.0))
+    pk = bik.PackedIK([m for m, _ in models], frames, nts, with_residual=True)
+    pk.set_inputs(tg, q0s)
+    pk.solve(settings)
+    for c, (m, m64) in enumerate(models):
+        one = bik.PackedIK([m], [frames[c]], [nts[c]], with_residual=True)
+        one.set_inputs([tg[c]], [q0s[c]])
+        one.solve(settings)
+        assert torch.equal(pk.q_of(c), one.q_of(0))
+        assert torch.equal(pk.iters[pk.class_slice(c)], one.iters)
+
+
+def test_solve_ik_single_problem_api():
+    m, m64 = _models("dual_arm")
+    q_star = syn.random_q(m64, 1, 70)
+    oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+    fids = [m.frame_id("ee_l"), m.frame_id("ee_r")]
+    T = K.frame_placements(m64, oMi, fids)[0]
+    q0 = syn.noisy_start(m64, q_star, 0.2, 71)[0]
+    res = bik.solve_ik(m, {"ee_l": torch.from_numpy(T[0]), "ee_r": torch.from_numpy(T[1])},
+                       initial_q=q0.float().cuda(), cost_cfg=bik.IKCostConfig(rest_weight=1e-3),
+                       optimizer_cfg=bik.OptimizerConfig(lam0=1e-3, factor=10.0))
+    ref = oik.solve(m64, fids, T[None], q0.numpy()[None],
+                    oik.IKSettings(lam0=1e-3, factor=10.0, max_iter=100, rest_weight=1e-3))
+    assert res.q.shape == (m.nq,)
+    assert res.residual.shape == (6 * 2 + 2 * m.nq + m.nv,)
+    assert res.converged == bool(ref.converged[0])
+    assert float((res.residual.cpu().double() - torch.from_numpy(ref.residual[0])).abs().max()) <= RES_TOL
+    pose = res.frame_pose("ee_l").cpu().double().numpy()
+    assert np.abs(pose[:3] - T[0, :3]).max() < 1e-3
+
+
+def test_zero_iterations_returns_start_and_cost():
+    m, m64 = _models("chain7")
+    q0 = syn.random_q(m64, 5, 80)
+    fid = m.frame_id("ee")
+    T = torch.zeros(5, 1, 7)
+    T[..., 6] = 1
+    out = bik.solve_ik_batched(m, [fid], T.cuda(), q0.float().cuda(),
+                               optimizer_cfg=bik.OptimizerConfig(max_iter=0), with_residual=True)
+    assert torch.equal(out.q.cpu(), q0.float())
+    assert (out.iters == 0).all() and not out.converged.any()
+    r, _ = oik.residual_and_jacobian(m64, q0.numpy(), [fid], T.double().numpy(), m64.q_neutral.numpy(),
+                                     oik.IKSettings(), want_jac=False)
+    np.testing.assert_allclose(out.residual.cpu().double().numpy(), r, atol=1e-5)
+    np.testing.assert_allclose(out.cost.cpu().double().numpy(), 0.5 * (r * r).sum(-1), rtol=1e-5, atol=1e-6)
+
+
+def test_unsupported_options_raise():
+    m, _ = _models("chain7")
+    T = torch.zeros(1, 1, 7, device="cuda")
+    q0 = torch.zeros(1, m.nq, device="cuda")
+    for opt in (bik.OptimizerConfig(optimizer="adam"), bik.OptimizerConfig(kernel="huber"),
+                bik.OptimizerConfig(linear_solver="lstsq")):
+        with pytest.raises(NotImplementedError):
+            bik.solve_ik_batched(m, [0], T, q0, optimizer_cfg=opt)
+    with pytest.raises(bik.ShapeError):
+        bik.solve_ik_batched(m, [m.nframes], T, q0)
