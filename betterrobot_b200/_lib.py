@@ -67,6 +67,8 @@ SIGNATURES: dict[str, tuple] = {
     "br_lm_solve": (c_int32, [ctypes.POINTER(IKBatch), ctypes.POINTER(IKSettings), ctypes.POINTER(IKResultBuf),
                               c_int32, c_void_p, c_int64, c_void_p]),
     "br_lm_team_floats": (c_int64, [ctypes.POINTER(BrTree), c_int32]),
+    "br_lm_solve_noalloc": (c_int32, [ctypes.POINTER(IKBatch), ctypes.POINTER(IKSettings),
+                                      ctypes.POINTER(IKResultBuf), c_int32, c_void_p]),
     "br_pose_loss": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
                                c_int32, c_void_p, c_void_p, c_void_p]),
     "br_pose_loss_backward": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_void_p, c_int64, c_void_p, c_int32,

@@ -671,3 +671,104 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
   lm_solve_kernel<<<grid, wpc * kWarp, bytes, s>>>(p);
   return (int)cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of br_lm_solve.
+//
+// br_lm_solve needs 16 bytes of device scratch (its work-queue counter) from the
+// caller.  Some callers cannot provide it because they cannot call cudaMalloc at
+// all: an IK call made from a robot controller's real-time loop, where a device
+// allocation can block for milliseconds and serialise the whole device; or a host
+// program that receives its input and output buffers from a framework and has no
+// CUDA allocator of its own.  br_lm_solve_noalloc runs the same kernel with the
+// scratch taken from the file-scope array below, so a call allocates nothing.
+//
+// The array exists once per device that loads this library and lives until the
+// process exits.  All calls on a device share it: two calls that run at the same
+// time on the GPU (e.g. on two streams) race on the work queue and must not
+// overlap.  Each call zeroes the part it uses before its launch.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+static __device__ __align__(256) unsigned char g_lm_noalloc_scratch[BR_LM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};  // device address of g_lm_noalloc_scratch, per device ordinal
+}  // namespace
+
+// Host code cannot use g_lm_noalloc_scratch as a device address; look the address
+// up once per device, with that device current (the first call on each device).
+static int noalloc_scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= 64) return BR_EINVAL;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_lm_noalloc_scratch);
+    if (e != cudaSuccess) return (int)e;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return BR_OK;
+}
+
+extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_settings_t* settings,
+                                   br_ik_result_t* result, int32_t warps_per_cta, void* stream) {
+  const int64_t need = BR_LM_SCRATCH_BYTES;  // scratch one launch of lm_solve_kernel uses
+  if (need > BR_LM_NOALLOC_SCRATCH_BYTES) return BR_ETOOBIG;
+  if (!batch || !settings || !result) return BR_EINVAL;
+  const br_ik_batch_t& b = *batch;
+  if (b.n_problems < 0 || b.n_items < 0 || b.n_classes < 1) return BR_EINVAL;
+  if (b.n_classes > BR_MAX_IK_CLASSES || b.max_targets > BR_MAX_IK_TARGETS) return BR_ETOOBIG;
+  if (b.max_targets < 1 || !b.trees || !b.team_size) return BR_EINVAL;
+  if (b.n_problems == 0 || b.n_items == 0) return BR_OK;
+  if (!b.items || !b.order || !b.n_targets || !b.frames || !b.targets || !b.q_offset || !b.x0 || !b.q_rest)
+    return BR_EINVAL;
+  if (!result->x || !result->iters || !result->status || !result->cost) return BR_EINVAL;
+  if (settings->max_iter < 0) return BR_EINVAL;
+  if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
+  void* scratch = nullptr;
+  int st = noalloc_scratch_address(&scratch);
+  if (st) return st;
+  LmParams p = {};
+  p.s = *settings;
+  p.b = b;
+  p.r = *result;
+  int warp_floats = 0;
+  for (int c = 0; c < b.n_classes; ++c) {
+    st = validate_tree(&b.trees[c]);
+    if (st) return st;
+    const int T = b.team_size[c];
+    if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
+    p.trees[c] = b.trees[c];
+    p.team[c] = T;
+    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets).total;
+    if (f > warp_floats) warp_floats = f;
+  }
+  p.warp_floats = warp_floats;
+  p.queue = reinterpret_cast<int32_t*>(scratch);
+  const DeviceInfo& dev = device_info();
+  int wpc = warps_per_cta;
+  size_t bytes = (size_t)wpc * warp_floats * sizeof(float);
+  while ((int64_t)bytes > dev.max_smem_optin && wpc > 1) {
+    wpc >>= 1;
+    bytes = (size_t)wpc * warp_floats * sizeof(float);
+  }
+  if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
+  cudaError_t e = cudaFuncSetAttribute(lm_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return (int)e;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lm_solve_kernel, wpc * kWarp, bytes);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t want = (b.n_items + wpc - 1) / wpc;
+  const int64_t cap = (int64_t)per_sm * dev.sms;
+  const int grid = (int)(want < cap ? want : cap);
+  cudaStream_t s = (cudaStream_t)stream;
+  e = cudaMemsetAsync(scratch, 0, (size_t)need, s);  // the queue counter must start at zero
+  if (e != cudaSuccess) return (int)e;
+  lm_solve_kernel<<<grid, wpc * kWarp, bytes, s>>>(p);
+  return (int)cudaGetLastError();
+}

@@ -176,6 +176,22 @@ typedef struct br_ik_result {
 BR_API int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
                        int32_t warps_per_cta, void* scratch, int64_t scratch_bytes, void* stream);
 
+/*
+ * Same solve as br_lm_solve for callers that cannot allocate device memory at all
+ * (e.g. a robot controller's real-time loop, where cudaMalloc may block and
+ * serialise the device, or a host with no CUDA allocator that only owns its
+ * inputs and outputs).  The work-queue scratch comes from a static device array
+ * of BR_LM_NOALLOC_SCRATCH_BYTES inside the library (one per device, kept until
+ * the process exits) instead of a caller pointer; a launch needing more than that
+ * returns BR_ETOOBIG.  The first call on each device looks up the array's device
+ * address and should be made before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.  No
+ * counterpart in the reference (BetterRobot has no native code).
+ */
+#define BR_LM_NOALLOC_SCRATCH_BYTES 256
+BR_API int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_settings_t* settings,
+                               br_ik_result_t* result, int32_t warps_per_cta, void* stream);
+
 /* Shared-memory floats one problem of `tree` with `max_targets` targets needs
  * (for choosing team sizes and warps per CTA). No reference counterpart. */
 BR_API int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets);
