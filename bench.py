@@ -341,6 +341,41 @@ def bench_fkj(steps: int, warmup: int, seed: int = 1):
 
 
 # ---------------------------------------------------------------------------
+# FK pose-loss adjoint (config 2)
+# ---------------------------------------------------------------------------
+def bench_adjoint(steps: int, warmup: int):
+    """Forward + backward of the pose loss on the humanoid, 12 frames: B = 16,384 (auto mode), and
+    store vs recompute at B = 262,144."""
+    import torch
+    from betterrobot_b200 import synthetic as syn
+    from betterrobot_b200.adjoint import pose_loss
+    m = syn.model_from_spec(syn.humanoid_spec())
+    m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
+    fids = syn.op_frame_ids(m)
+    out = {}
+    stream = torch.cuda.current_stream()
+    for B, modes in ((16384, ("auto",)), (262144, ("store", "recompute"))):
+        q = syn.random_q(m64, B, 31, rev_range=2.5, base_translation=1.0).float().cuda()
+        T = syn.random_targets(B, len(fids), 32).float().cuda()
+        w = torch.from_numpy(np.random.default_rng(33).uniform(0.5, 2.0, size=len(fids))).float().cuda()
+        for mode in modes:
+            qg = q.clone().requires_grad_(True)
+            for _ in range(warmup):
+                pose_loss(m, qg, fids, T, w, mode=mode).sum().backward()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                qg.grad = None
+                pose_loss(m, qg, fids, T, w, mode=mode).sum().backward()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            out[f"B{B}_{mode}"] = {"ms_fwd_bwd": ms, "configs_per_s": B / (ms * 1e-3)}
+    return out
+
+
+# ---------------------------------------------------------------------------
 # CPU: BetterRobot's algorithm (float64 port of its serial LM) on host cores
 # ---------------------------------------------------------------------------
 def _cpu_worker(args):
@@ -416,6 +451,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op PyTorch arm")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
+    ap.add_argument("--only", choices=["ik", "fkj", "adjoint"], default=None,
+                    help="run one section and print its raw timings (for profiling)")
     args = ap.parse_args()
     warmup = max(args.warmup, 3)
     metric = "batched LM-IK solves/s reaching 1e-4 m and 1e-4 rad pose error"
@@ -445,6 +483,18 @@ def main():
                 "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
+    if args.only:
+        import torch
+        dist_setup()
+        if args.only == "ik":
+            r = bench_ik(args.steps, warmup, seed=7)
+            r.pop("wl")
+        elif args.only == "fkj":
+            r = bench_fkj(args.steps, warmup)
+        else:
+            r = bench_adjoint(args.steps, warmup)
+        print(json.dumps({"section": args.only, **r}), flush=True)
+        return
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(seed=7)  # before any CUDA work in this process (spawned workers)
@@ -458,6 +508,7 @@ def main():
         barrier(world)
     clocks = clk.summary()
     fkj = bench_fkj(args.steps, warmup)
+    adj = bench_adjoint(args.steps, warmup) if not args.no_adjoint else None
     plain = bench_plain_gpu(ik["wl"]) if (rank == 0 and not args.no_plain) else None
     ms = reduce(ik["ms"], world, "max")
     reached = reduce(ik["reached"], world, "sum")
@@ -477,6 +528,8 @@ def main():
                "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1},
         "clocks": clocks, "gpu_launches": ik["launches"],
     }
+    if adj is not None:
+        line["adjoint"] = adj
     if plain is not None:
         line["plain_gpu"] = {"value": plain["reached"] / plain["sec"], "unit": "solves/s", "sec_per_step": plain["sec"],
                              "reached_1e-4": plain["reached"], "speedup_fused_over_plain":

@@ -55,6 +55,14 @@ class IKResultBuf(ctypes.Structure):
                 ("residual", c_void_p)]
 
 
+class TrajSettings(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("w_goal", ctypes.c_float), ("w_start", ctypes.c_float),
+                ("w_accel", ctypes.c_float), ("w_limit", ctypes.c_float), ("w_ref", ctypes.c_float),
+                ("tol", ctypes.c_float), ("gn_eps", ctypes.c_float), ("lam0", ctypes.c_float),
+                ("factor", ctypes.c_float), ("lam_min", ctypes.c_float), ("lam_max", ctypes.c_float),
+                ("max_iter", c_int32), ("optimizer", c_int32)]
+
+
 # name -> (restype, argtypes); must match include/br_b200.h
 SIGNATURES: dict[str, tuple] = {
     "br_version": (ctypes.c_char_p, []),
@@ -69,6 +77,9 @@ SIGNATURES: dict[str, tuple] = {
     "br_lm_team_floats": (c_int64, [ctypes.POINTER(BrTree), c_int32]),
     "br_lm_solve_noalloc": (c_int32, [ctypes.POINTER(IKBatch), ctypes.POINTER(IKSettings),
                                       ctypes.POINTER(IKResultBuf), c_int32, c_void_p]),
+    "br_trajopt_solve": (c_int32, [ctypes.POINTER(BrTree), c_int32, c_int64, c_int32, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, ctypes.POINTER(TrajSettings), c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_void_p]),
     "br_pose_loss": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
                                c_int32, c_void_p, c_void_p, c_void_p]),
     "br_pose_loss_backward": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_void_p, c_int64, c_void_p, c_int32,

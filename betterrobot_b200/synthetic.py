@@ -160,6 +160,17 @@ def _quat_mul_np(a: np.ndarray, b: np.ndarray) -> np.ndarray:
                      aw * bw - ax * bx - ay * by - az * bz], axis=1)
 
 
+def trajopt_endpoints(model: Model, n: int, seed: int, spread: float = 1.0):
+    """Start and goal configurations (float64) for trajectory problems: start uniform in
+    +-2.5 rad, goal = start + U(+-spread) per joint, both clamped to the joint limits."""
+    rng = np.random.default_rng(seed)
+    lo = model.lower_pos_limit.double().numpy()
+    hi = model.upper_pos_limit.double().numpy()
+    q0 = rng.uniform(-2.5, 2.5, size=(n, model.nq))
+    q1 = np.clip(q0 + rng.uniform(-spread, spread, size=(n, model.nq)), lo, hi)
+    return torch.from_numpy(np.clip(q0, lo, hi)), torch.from_numpy(q1)
+
+
 def ik_uneven_mix(n_problems: int, seed: int = 3) -> list[tuple[str, int]]:
     """Class label and target count for each problem of the uneven batch:
     40% chain7, 30% dual_arm, 30% humanoid; 1-6 targets each."""

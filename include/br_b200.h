@@ -221,6 +221,39 @@ BR_API int br_pose_loss_backward(const br_tree_t* tree, const float* q, const fl
                                  const float* weights, int32_t weights_per_config, const float* grad_loss,
                                  float* grad_q, void* stream);
 
+/* ==== batched trajectory optimisation (Gauss-Newton / LM) ================ */
+#define BR_MAX_TRAJ_KNOTS 128
+#define BR_MAX_TRAJ_NV 8
+
+/* Cost stack weights (CostStack item weights) and solver settings.  Terms with
+ * weight 0 are left out. */
+typedef struct br_traj_settings {
+    float dt;                   /* knot spacing of the acceleration residual        */
+    float w_goal, w_start;      /* PoseResidual at knot T-1 / knot 0                */
+    float w_accel;              /* AccelerationResidual                             */
+    float w_limit;              /* JointPositionLimit at every knot                 */
+    float w_ref;                /* ReferenceTrajectoryResidual (toward x_ref)       */
+    float tol, gn_eps, lam0, factor, lam_min, lam_max;
+    int32_t max_iter;
+    int32_t optimizer;          /* BR_OPT_GN or BR_OPT_LM                           */
+} br_traj_settings_t;
+
+/*
+ * Solve n_traj independent trajectories of `knots` configurations each, one warp
+ * per trajectory, with a bandwidth-2 block Cholesky of the block-pentadiagonal
+ * normal equations.  x0 / x_ref / x are [n_traj, knots, nq] (x_ref NULL = x0),
+ * goal / start are [n_traj, 7] poses of frame `frame_id` (start may be NULL).
+ * goal_grad (NULL or [n_traj, 6]) receives d(final cost)/d(eps) for the goal
+ * perturbed as T_goal * exp(eps).  Fixed-base trees only (nq == nv <= 8).
+ * Replaces solve_trajopt with the knot parameterisation and its dense LM / GN
+ * (src/better_robot/tasks/trajopt.py:84-230) on the goal / start / acceleration /
+ * limit / reference-trajectory stack.
+ */
+BR_API int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t n_traj, int32_t knots,
+                            const float* x0, const float* x_ref, const float* goal, const float* start,
+                            const br_traj_settings_t* settings, float* x, int32_t* iters, int32_t* status,
+                            float* cost, float* goal_grad, void* stream);
+
 /* Library build information (for logging): returns a static string. */
 BR_API const char* br_version(void);
 

@@ -205,6 +205,48 @@ def make_adjoint(spec, B, seed, out):
                         loss=loss.detach().numpy(), grad=g.numpy())
 
 
+def make_trajopt(spec, N, T, seed, out, dt=0.05, w_goal=1.0, w_start=1.0, w_accel=1e-2, w_limit=0.1,
+                 w_ref=1e-3, tol=1e-6, max_iter=30):
+    """Reference solve_trajopt (knots, GaussNewton) on the config-4 stack, float64."""
+    from better_robot.costs.stack import CostStack
+    from better_robot.kinematics.forward import forward_kinematics
+    from better_robot.optim.optimizers.gauss_newton import GaussNewton
+    from better_robot.residuals import AccelerationResidual, JointPositionLimit, PoseResidual, TimeIndexedResidual
+    from better_robot.residuals.regularization import ReferenceTrajectoryResidual
+    from better_robot.tasks.trajopt import solve_trajopt
+
+    m = reference_model(spec)
+    mine = syn.model_from_spec(spec, dtype=D)
+    q_start, q_goal = syn.trajopt_endpoints(mine, N, seed)
+    fid = m.frame_id("ee")
+    res = {"X": [], "iters": [], "converged": [], "residual": []}
+    goals, starts = [], []
+    for n in range(N):
+        Tg = forward_kinematics(m, q_goal[n], compute_frames=True).frame_pose_world[fid].clone()
+        Ts = forward_kinematics(m, q_start[n], compute_frames=True).frame_pose_world[fid].clone()
+        X0 = q_start[n].expand(T, -1).clone()
+        stack = CostStack()
+        stack.add("goal", TimeIndexedResidual(PoseResidual(frame_id=fid, target=Tg), t_idx=T - 1), weight=w_goal)
+        stack.add("start", TimeIndexedResidual(PoseResidual(frame_id=fid, target=Ts), t_idx=0), weight=w_start)
+        stack.add("accel", AccelerationResidual(m, dt=dt), weight=w_accel)
+        for t in range(T):
+            stack.add(f"limits_t{t}", TimeIndexedResidual(JointPositionLimit(m), t_idx=t, name=f"limits_t{t}"),
+                      weight=w_limit)
+        stack.add("ref", ReferenceTrajectoryResidual(m, X0.clone()), weight=w_ref)
+        r = solve_trajopt(m, horizon=T, dt=dt, initial_q_traj=X0, cost_stack=stack, optimizer=GaussNewton(tol=tol),
+                          max_iter=max_iter)
+        res["X"].append(r.trajectory.q[0].numpy())
+        res["iters"].append(r.iters)
+        res["converged"].append(r.converged)
+        res["residual"].append(r.residual.numpy())
+        goals.append(Tg.numpy())
+        starts.append(Ts.numpy())
+    np.savez_compressed(out, q_start=q_start.numpy(), q_goal=q_goal.numpy(), goal=np.stack(goals),
+                        start=np.stack(starts), X=np.stack(res["X"]), iters=np.array(res["iters"]),
+                        converged=np.array(res["converged"]), residual=np.stack(res["residual"]),
+                        settings=np.array([T, dt, w_goal, w_start, w_accel, w_limit, w_ref, tol, max_iter]))
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if src:
@@ -225,6 +267,7 @@ def main():
     make_ik("humanoid", hum, ["track0", "track2", "track4"], 4, 24, "noisy",
             os.path.join(HERE, "ik_humanoid.npz"), max_iter=100, rest_w=1e-3, **lm)
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
+    make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
 
 
 if __name__ == "__main__":

@@ -95,3 +95,20 @@ def test_known_answers_one_joint_arm():
     assert abs(oMi[2, 2] - 0.1) < 1e-12
     oMi, _ = K.forward_kinematics(m, np.array([math.pi / 2]))
     assert abs(oMi[2, 5] - math.sin(math.pi / 4)) < 1e-12 and abs(oMi[2, 6] - math.cos(math.pi / 4)) < 1e-12
+
+
+def test_trajopt_matches_reference_solve_trajopt():
+    """GN trajectory optimisation (goal/start pose, acceleration, per-knot limits, reference trajectory)."""
+    from oracle import trajopt as ot
+    g = _load("trajopt_chain7.npz")
+    T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
+    m = syn.model_from_spec(SPECS["chain7"], dtype=torch.float64)
+    s = ot.TrajSettings(dt=dt, w_goal=wg, w_start=ws, w_accel=wa, w_limit=wl, w_ref=wr, tol=tol, max_iter=int(mi))
+    X0 = np.repeat(g["q_start"][:, None, :], int(T), 1)
+    fid = m.frame_id("ee")
+    out = ot.solve(m, X0, fid, g["goal"], g["start"], s)
+    np.testing.assert_array_equal(out.iters, g["iters"])
+    np.testing.assert_array_equal(out.converged, g["converged"])
+    np.testing.assert_allclose(out.X, g["X"], atol=1e-8, rtol=0)
+    r, _ = ot.residual_jacobian(m, out.X, fid, g["goal"], g["start"], X0, s, want_jac=False)
+    np.testing.assert_allclose(r, g["residual"], atol=1e-9, rtol=0)
