@@ -376,6 +376,39 @@ def bench_adjoint(steps: int, warmup: int):
 
 
 # ---------------------------------------------------------------------------
+# trajectory optimisation (config 4)
+# ---------------------------------------------------------------------------
+def bench_trajopt(steps: int, warmup: int, n_traj: int = 256, knots: int = 64):
+    """256 chain7 trajectories x 64 knots (448 variables each), goal = start + U(+-0.5) rad:
+    GN <= 30 iterations + goal adjoint."""
+    import torch
+    import betterrobot_b200 as br
+    from betterrobot_b200 import synthetic as syn
+    from betterrobot_b200 import trajopt as btr
+    m = syn.model_from_spec(syn.chain_spec())
+    m64 = syn.model_from_spec(syn.chain_spec(), dtype=torch.float64)
+    fid = m.frame_id("ee")
+    qs, qg = syn.trajopt_endpoints(m64, n_traj, 81, spread=0.5)
+    goal = br.forward_kinematics(m, qg.float().cuda(), compute_frames=True).frame_pose_world[:, fid].contiguous()
+    start = br.forward_kinematics(m, qs.float().cuda(), compute_frames=True).frame_pose_world[:, fid].contiguous()
+    X0 = qs.float().cuda()[:, None, :].expand(-1, knots, -1).contiguous()
+    cfg = btr.TrajOptConfig(max_iter=30)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        out = btr.solve_trajopt_batched(m, fid, goal, X0, start=start, cfg=cfg)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        out = btr.solve_trajopt_batched(m, fid, goal, X0, start=start, cfg=cfg)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"ms": ms, "trajectories_per_s": n_traj / (ms * 1e-3), "converged": int(out.converged.sum()),
+            "iters_mean": float(out.iters.float().mean()), "n_traj": n_traj, "knots": knots}
+
+
+# ---------------------------------------------------------------------------
 # CPU: BetterRobot's algorithm (float64 port of its serial LM) on host cores
 # ---------------------------------------------------------------------------
 def _cpu_worker(args):
@@ -452,7 +485,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op PyTorch arm")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
-    ap.add_argument("--only", choices=["ik", "fkj", "adjoint"], default=None,
+    ap.add_argument("--only", choices=["ik", "fkj", "adjoint", "trajopt"], default=None,
                     help="run one section and print its raw timings (for profiling)")
     args = ap.parse_args()
     warmup = max(args.warmup, 3)
@@ -491,6 +524,8 @@ def main():
             r.pop("wl")
         elif args.only == "fkj":
             r = bench_fkj(args.steps, warmup)
+        elif args.only == "trajopt":
+            r = bench_trajopt(args.steps, warmup)
         else:
             r = bench_adjoint(args.steps, warmup)
         print(json.dumps({"section": args.only, **r}), flush=True)
@@ -509,6 +544,7 @@ def main():
     clocks = clk.summary()
     fkj = bench_fkj(args.steps, warmup)
     adj = bench_adjoint(args.steps, warmup) if not args.no_adjoint else None
+    trj = bench_trajopt(args.steps, warmup) if not args.no_adjoint else None
     plain = bench_plain_gpu(ik["wl"]) if (rank == 0 and not args.no_plain) else None
     ms = reduce(ik["ms"], world, "max")
     reached = reduce(ik["reached"], world, "sum")
@@ -530,6 +566,8 @@ def main():
     }
     if adj is not None:
         line["adjoint"] = adj
+    if trj is not None:
+        line["trajopt"] = trj
     if plain is not None:
         line["plain_gpu"] = {"value": plain["reached"] / plain["sec"], "unit": "solves/s", "sec_per_step": plain["sec"],
                              "reached_1e-4": plain["reached"], "speedup_fused_over_plain":

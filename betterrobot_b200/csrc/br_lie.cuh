@@ -362,3 +362,81 @@ __device__ __forceinline__ DPose dse3_exp(double3 v, double3 w) {
 }
 
 }  // namespace br
+
+// float64 SE3 Jr^-1 (same block-Horner construction as jr_inv_se3 above), used where the
+// normal equations are ill-conditioned enough that float32 Jacobian rounding is amplified
+// (the trajectory problem, condition ~1e8).
+namespace br {
+
+struct DJrInv {
+  double3 w;
+  double b0, b1, b2;
+  double B[9];
+};
+
+__device__ __forceinline__ double3 dapply_poly(const double3& w, double b0, double b1, double b2, double3 x) {
+  const double3 wx = dcross(w, x);
+  return dadd(dadd(dscale(x, b0), dscale(wx, b1)), dscale(dcross(w, wx), b2));
+}
+
+template <int N>
+__device__ __forceinline__ DJrInv djr_inv_se3(double3 v, double3 w) {
+  double ck[N + 1];
+  {
+    double f = 1.0;
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+      f /= (double)(k + 1);
+      ck[k] = (k & 1) ? -f : f;
+    }
+  }
+  const double th2 = ddot(w, w);
+  double a0 = ck[N], a1 = 0.0, a2 = 0.0;
+  double B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = N - 1; k >= 0; --k) {
+    double nB[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double3 bc = d3(B[c], B[3 + c], B[6 + c]);
+      const double3 e = d3(c == 0 ? 1.0 : 0.0, c == 1 ? 1.0 : 0.0, c == 2 ? 1.0 : 0.0);
+      const double3 ac = dapply_poly(w, a0, a1, a2, e);
+      const double3 r = dadd(dcross(w, bc), dcross(v, ac));
+      nB[c] = r.x; nB[3 + c] = r.y; nB[6 + c] = r.z;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) B[i] = nB[i];
+    const double na1 = a0 - th2 * a2;
+    a2 = a1;
+    a1 = na1;
+    a0 = ck[k];
+  }
+  DJrInv J;
+  J.w = w;
+  const double b0 = 1.0 / a0;
+  const double m = a0 - th2 * a2;
+  const double r0 = -a1 * b0, r1 = -a2 * b0;
+  const double idet = 1.0 / (m * m + th2 * a1 * a1);
+  J.b0 = b0;
+  J.b1 = (r0 * m + th2 * a1 * r1) * idet;
+  J.b2 = (m * r1 - a1 * r0) * idet;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) J.B[i] = B[i];
+  return J;
+}
+
+__device__ __forceinline__ void djr_inv_apply(const DJrInv& J, double3 xl, double3 xa, double3& ol, double3& oa) {
+  oa = dapply_poly(J.w, J.b0, J.b1, J.b2, xa);
+  const double3 Bo = d3(J.B[0] * oa.x + J.B[1] * oa.y + J.B[2] * oa.z, J.B[3] * oa.x + J.B[4] * oa.y + J.B[5] * oa.z,
+                        J.B[6] * oa.x + J.B[7] * oa.y + J.B[8] * oa.z);
+  ol = dapply_poly(J.w, J.b0, J.b1, J.b2, dsub(xl, Bo));
+}
+
+__device__ __forceinline__ void djr_inv_T_apply(const DJrInv& J, double3 xl, double3 xa, double3& ol, double3& oa) {
+  ol = dapply_poly(J.w, J.b0, -J.b1, J.b2, xl);
+  const double3 Bt = d3(J.B[0] * ol.x + J.B[3] * ol.y + J.B[6] * ol.z, J.B[1] * ol.x + J.B[4] * ol.y + J.B[7] * ol.z,
+                        J.B[2] * ol.x + J.B[5] * ol.y + J.B[8] * ol.z);
+  oa = dapply_poly(J.w, J.b0, -J.b1, J.b2, dsub(xa, Bt));
+}
+
+}  // namespace br

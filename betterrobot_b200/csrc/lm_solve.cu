@@ -52,30 +52,37 @@ struct LmParams {
 
 // ---- per-team shared-memory layout (floats) --------------------------------
 struct TeamLayout {
-  int parent, jtype, idxq, idxv, axis, place, support, cjoint, ckind, caxis, lower, upper;
-  int fparent, fplace, tgt, cmask;
-  int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc;
+  int parent, jtype, idxq, idxv, support, cjoint, ckind, caxis, lower, upper;
+  int fparent, fplace, tgt;
+  int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc, trik, coff,
+      dinv, sup, nsup;
   int total;
-  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K) {
+  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += round4(n); return r; };
     parent = take(nj); jtype = take(nj); idxq = take(nj); idxv = take(nj);
-    axis = take(4 * nj); place = take(8 * nj); support = take(2 * nj);
+    support = take(2 * nj);
     cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
     lower = take(nq); upper = take(nq);
-    fparent = take(K); fplace = take(8 * K); cmask = take(2 * K);
+    fparent = take(K); fplace = take(8 * K);
     // float64 regions (2 floats per double)
     x = take(2 * nq); xn = take(2 * nq); qrest = take(2 * nq);
-    poseA = take(16 * nj); poseB = take(16 * nj); tw = take(16 * K); xi = take(16 * K); d = take(2 * nv);
+    poseA = take(14 * nj); poseB = take(14 * nj); tw = take(16 * K); xi = take(16 * K);
+    d = take(2 * nv);
     tgt = take(16 * K);
     // float32 / int regions
     ancA = take(nj); ancB = take(nj);
     jri = take(16 * K); colw = take(8 * nv);
     g = take(nv); delta = take(nv);
-    jtj = take(nv * (nv + 1) / 2);
-    const int jp = 6 * K * nv, lsq = nv * (nv + 1);
-    work = take(jp > lsq ? jp : lsq);  // J_pose during the Jacobian build, L during the solve
+    const int ntri = nv * (nv + 1) / 2;
+    jtj = take(ntri);                          // J^T J, packed lower triangle, column-major
+    work = take(6 * nv > ntri ? 6 * nv : ntri);  // one target's J columns (build) / packed L (solve)
     misc = take(8);
+    trik = take((ntri + 1) / 2);               // uint16 (row i | column k << 8) of packed entry e (column-major)
+    coff = take(nv);                           // packed index of (i, k) = coff[k] + i
+    dinv = take(nv);                           // 1 / L_jj
+    sup = take((K * nv + 3) / 4);              // uint8 support columns of each target, ascending
+    nsup = take(K);
     total = o;
   }
 };
@@ -107,7 +114,20 @@ __device__ __forceinline__ void st8(float* p, const Pose& P) {
   *reinterpret_cast<float4*>(p + 4) = P.q;
 }
 
-// float64 pose records: (t.x, t.y, t.z, pad, q.x, q.y, q.z, q.w)
+// float64 joint poses in structure-of-arrays form: 7 arrays of nj doubles
+// (t.x, t.y, t.z, q.x, q.y, q.z, q.w), so lanes reading consecutive joints hit
+// consecutive 8-byte words (no bank conflicts).
+__device__ __forceinline__ DPose lds(const double* p, int nj, int j) {
+  DPose P;
+  P.t = d3(p[j], p[nj + j], p[2 * nj + j]);
+  P.q = make_double4(p[3 * nj + j], p[4 * nj + j], p[5 * nj + j], p[6 * nj + j]);
+  return P;
+}
+__device__ __forceinline__ void sts(double* p, int nj, int j, const DPose& P) {
+  p[j] = P.t.x; p[nj + j] = P.t.y; p[2 * nj + j] = P.t.z;
+  p[3 * nj + j] = P.q.x; p[4 * nj + j] = P.q.y; p[5 * nj + j] = P.q.z; p[6 * nj + j] = P.q.w;
+}
+// float64 per-target records: (t.x, t.y, t.z, pad, q.x, q.y, q.z, q.w)
 __device__ __forceinline__ DPose ldd(const double* p) {
   DPose P;
   P.t = d3(p[0], p[1], p[2]);
@@ -131,13 +151,13 @@ template <int T>
 __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
   const int K = P.b.max_targets;
-  const TeamLayout L(nj, nq, nv, K);
+  const TeamLayout L(nj, nq, nv, K, T);
   int* parent = reinterpret_cast<int*>(sm + L.parent);
   int* jtype = reinterpret_cast<int*>(sm + L.jtype);
   int* idxq = reinterpret_cast<int*>(sm + L.idxq);
   int* idxv = reinterpret_cast<int*>(sm + L.idxv);
-  float* axis = sm + L.axis;
-  float* place = sm + L.place;
+  const float* __restrict__ axis = tree.axis;         // read-only cache
+  const float* __restrict__ place = tree.placement;
   unsigned long long* support = reinterpret_cast<unsigned long long*>(sm + L.support);
   int* cjoint = reinterpret_cast<int*>(sm + L.cjoint);
   int* ckind = reinterpret_cast<int*>(sm + L.ckind);
@@ -146,7 +166,6 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   float* upper = sm + L.upper;
   int* fparent = reinterpret_cast<int*>(sm + L.fparent);
   float* fplace = sm + L.fplace;
-  unsigned long long* cmask = reinterpret_cast<unsigned long long*>(sm + L.cmask);
   double* x = reinterpret_cast<double*>(sm + L.x);
   double* xn = reinterpret_cast<double*>(sm + L.xn);
   double* qrest = reinterpret_cast<double*>(sm + L.qrest);
@@ -164,6 +183,11 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   float* delta = sm + L.delta;
   float* jtj = sm + L.jtj;
   float* work = sm + L.work;
+  unsigned short* trik = reinterpret_cast<unsigned short*>(sm + L.trik);
+  int* coff = reinterpret_cast<int*>(sm + L.coff);
+  float* dinv = sm + L.dinv;
+  unsigned char* sup = reinterpret_cast<unsigned char*>(sm + L.sup);
+  int* nsup = reinterpret_cast<int*>(sm + L.nsup);
   const int tl = tm.tl;
   const br_ik_settings_t& S = P.s;
   const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
@@ -176,9 +200,6 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     jtype[j] = tree.jtype[j];
     idxq[j] = tree.idx_q[j];
     idxv[j] = tree.idx_v[j];
-    *reinterpret_cast<float4*>(axis + 4 * j) = *reinterpret_cast<const float4*>(tree.axis + 4 * j);
-    *reinterpret_cast<float4*>(place + 8 * j) = *reinterpret_cast<const float4*>(tree.placement + 8 * j);
-    *reinterpret_cast<float4*>(place + 8 * j + 4) = *reinterpret_cast<const float4*>(tree.placement + 8 * j + 4);
     support[j] = tree.support[j];
   }
   for (int c = tl; c < nv; c += T) {
@@ -203,18 +224,27 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       std8(tgt + 8 * t, DPose{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])});
     }
   }
+  // (i, k) of every packed lower-triangle entry, column-major: column k holds rows
+  // k..nv-1 and starts at k*nv - k(k-1)/2
+  for (int k = tl; k < nv; k += T) {
+    const int off = k * nv - k * (k - 1) / 2;
+    coff[k] = off - k;
+    for (int i = k; i < nv; ++i) trik[off + i - k] = (unsigned short)(i | (k << 8));
+  }
   tm.sync();
-  // column support mask of each target frame
+  // ascending list of the tangent columns that move each target frame (its support)
   for (int t = 0; t < nt; ++t) {
-    const unsigned long long sup = support[fparent[t]];
-    unsigned long long m = 0ull;
+    const unsigned long long sp = support[fparent[t]];
+    int base = 0;
     for (int c0 = 0; c0 < nv; c0 += T) {
       const int c = c0 + tl;
-      const bool in = c < nv && ((sup >> cjoint[c]) & 1ull);
-      const unsigned bal = __ballot_sync(tm.mask, in) >> ((threadIdx.x & 31) - tl);
-      m |= (unsigned long long)(bal & (T == 32 ? 0xffffffffu : ((1u << T) - 1u))) << c0;
+      const bool in = c < nv && ((sp >> cjoint[c]) & 1ull);
+      const unsigned bal = (__ballot_sync(tm.mask, in) >> ((threadIdx.x & 31) - tl)) &
+                           (T == 32 ? 0xffffffffu : ((1u << T) - 1u));
+      if (in) sup[t * nv + base + __popc(bal & ((1u << tl) - 1u))] = (unsigned char)c;
+      base += __popc(bal);
     }
-    if (tl == 0) cmask[t] = m;
+    if (tl == 0) nsup[t] = base;
   }
   tm.sync();
 
@@ -235,7 +265,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       } else if (jt == BR_JOINT_FREE_FLYER) {                         // free_flyer.py:31-36
         Lj = dcompose(Pj, DPose{d3(qv[0], qv[1], qv[2]), dqnormalize(make_double4(qv[3], qv[4], qv[5], qv[6]))});
       }
-      std8(poseA + 8 * j, Lj);
+      sts(poseA, nj, j, Lj);
       ancA[j] = parent[j];
     }
     tm.sync();
@@ -247,10 +277,10 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       for (int j = tl; j < nj; j += T) {
         const int a = aA[j];
         if (a >= 0) {
-          std8(B + 8 * j, dcompose(ldd(A + 8 * a), ldd(A + 8 * j)));
+          sts(B, nj, j, dcompose(lds(A, nj, a), lds(A, nj, j)));
           aB[j] = aA[a];
         } else {
-          std8(B + 8 * j, ldd(A + 8 * j));
+          sts(B, nj, j, lds(A, nj, j));
           aB[j] = -1;
         }
       }
@@ -265,7 +295,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   auto residual = [&](const double* q, const double* pose) -> double {
     double acc = 0.0;
     for (int t = tl; t < nt; t += T) {
-      const DPose Tee = dcompose(ldd(pose + 8 * fparent[t]), to_d(ld8(fplace + 8 * t)));
+      const DPose Tee = dcompose(lds(pose, nj, fparent[t]), to_d(ld8(fplace + 8 * t)));
       std8(tw + 8 * t, Tee);
       double3 v, w;
       dse3_log(dcompose(dinverse(ldd(tgt + 8 * t)), Tee), v, w);     // pose.py:63-64
@@ -305,13 +335,17 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     return 0.5 * acc;
   };
 
-  // float32 J^T J (packed lower) and g = J^T r at q with world poses `pose`; returns |g|.
+  // float32 J^T J (packed lower, column-major) and g = J^T r at q with world poses `pose`; returns |g|.
+  // Each target's pose Jacobian diag(w) Jr^-1 blockdiag(R^T, R^T) J_lwa (pose.py:68-103) is
+  // built only on its support columns and accumulated into the (support x support) block.
   auto build_normal = [&](const double* q, const double* pose) -> float {
+    const int ntri = tri(nv);
     for (int c = tl; c < nv; c += T) {
-      const Pose Tj = to_f(ldd(pose + 8 * cjoint[c]));
+      const Pose Tj = to_f(lds(pose, nj, cjoint[c]));
       const float3 a = qrot(Tj.q, f3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
       *reinterpret_cast<float4*>(colw + 8 * c) = make_float4(a.x, a.y, a.z, 0.f);
       *reinterpret_cast<float4*>(colw + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
+      g[c] = 0.f;
     }
     for (int t = tl; t < nt; t += T) {                                 // Jr^-1(xi), tangents.py:204-207
       const double* e = xi + 8 * t;
@@ -320,134 +354,107 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
       for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
     }
+    for (int e = tl; e < ntri; e += T) jtj[e] = 0.f;
     tm.sync();
-    // pose Jacobians J_t = diag(w) Jr^-1 blockdiag(R^T, R^T) J_lwa, stored work[t][row][c]
-    float* Jp = work;
-    for (int idx = tl; idx < nt * nv; idx += T) {
-      const int t = idx / nv, c = idx - t * nv;
-      float3 ol = f3(0.f, 0.f, 0.f), oa = f3(0.f, 0.f, 0.f);
-      if ((cmask[t] >> c) & 1ull) {
+    float* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
+    for (int t = 0; t < nt; ++t) {
+      const int ns = nsup[t];
+      const unsigned char* st = sup + t * nv;
+      const Pose Tee = to_f(ldd(tw + 8 * t));
+      const float* o = jri + 16 * t;
+      JrInv J;
+      J.w = f3(o[0], o[1], o[2]);
+      J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
+      for (int u = tl; u < ns; u += T) {
+        const int c = st[u];
         const float4 a4 = *reinterpret_cast<const float4*>(colw + 8 * c);
         const float3 a = f3(a4.x, a4.y, a4.z);
-        const Pose Tee = to_f(ldd(tw + 8 * t));
         float3 lin, ang;
         if (ckind[c] == 0) {
           const float4 o4 = *reinterpret_cast<const float4*>(colw + 8 * c + 4);
-          lin = cross(a, sub(Tee.t, f3(o4.x, o4.y, o4.z)));           // jacobian.py:213-215
+          lin = cross(a, sub(Tee.t, f3(o4.x, o4.y, o4.z)));             // jacobian.py:213-215
           ang = a;
         } else {
           lin = a;
           ang = f3(0.f, 0.f, 0.f);
         }
-        lin = qrot_inv(Tee.q, lin);                                    // pose.py:91-95
-        ang = qrot_inv(Tee.q, ang);
-        const float* o = jri + 16 * t;
-        JrInv J;
-        J.w = f3(o[0], o[1], o[2]);
-        J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
-        for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
-        jr_inv_apply(J, lin, ang, ol, oa);
-        ol = scale(ol, wp);
-        oa = scale(oa, wo);
+        float3 ol, oa;
+        jr_inv_apply(J, qrot_inv(Tee.q, lin), qrot_inv(Tee.q, ang), ol, oa);   // pose.py:91-99
+        Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
+        Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
       }
-      float* dst = Jp + t * 6 * nv + c;
-      dst[0] = ol.x; dst[nv] = ol.y; dst[2 * nv] = ol.z;
-      dst[3 * nv] = oa.x; dst[4 * nv] = oa.y; dst[5 * nv] = oa.z;
-    }
-    tm.sync();
-    // J^T J, lanes over the packed lower triangle
-    const int ntri = tri(nv);
-    int a = 0, b = tl;
-    while (a < nv && b > a) { b -= a + 1; ++a; }
-    for (int k = tl; k < ntri; k += T) {
-      float acc = 0.f;
-      for (int t = 0; t < nt; ++t) {
-        const unsigned long long m = cmask[t];
-        if (((m >> a) & 1ull) && ((m >> b) & 1ull)) {
-          const float* Jt = Jp + t * 6 * nv;
+      tm.sync();
+      for (int p = tl; p < tri(ns); p += T) {
+        int u = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);   // row-major (u >= v) decode of p
+        if (tri(u + 1) <= p) ++u;
+        if (tri(u) > p) --u;
+        const int v = p - tri(u);
+        float acc = 0.f;
 #pragma unroll
-          for (int r = 0; r < 6; ++r) acc = fmaf(Jt[r * nv + a], Jt[r * nv + b], acc);
-        }
+        for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], Jc[r * nv + v], acc);
+        jtj[coff[st[v]] + st[u]] += acc;
       }
-      if (a == b) {
-        if (use_rest) acc += wr * wr;                                  // regularization.py:56-64
-        if (use_limits) {                                              // limits.py:64-86
-          const int j = cjoint[a];
-          if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
-            const int iq = idxq[j];
-            if (q[iq] < (double)lower[iq]) acc += wl * wl;
-            if (q[iq] > (double)upper[iq]) acc += wl * wl;
-          }
-        }
+      const double* e = xi + 8 * t;
+      const float rw[6] = {wp * (float)e[0], wp * (float)e[1], wp * (float)e[2],
+                           wo * (float)e[3], wo * (float)e[4], wo * (float)e[5]};
+      for (int u = tl; u < ns; u += T) {
+        float acc = 0.f;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], rw[r], acc);
+        g[st[u]] += acc;
       }
-      jtj[k] = acc;
-      b += T;
-      while (a < nv && b > a) { b -= a + 1; ++a; }
+      tm.sync();
     }
-    // g = J^T r
+    // rest (w I, regularization.py:56-64) and limit (+-w on active rows, limits.py:64-86) terms
     float gg = 0.f;
     for (int c = tl; c < nv; c += T) {
-      float acc = 0.f;
-      for (int t = 0; t < nt; ++t) {
-        if ((cmask[t] >> c) & 1ull) {
-          const float* Jt = Jp + t * 6 * nv + c;
-          const double* e = xi + 8 * t;
-          acc = fmaf(Jt[0], wp * (float)e[0], acc);
-          acc = fmaf(Jt[nv], wp * (float)e[1], acc);
-          acc = fmaf(Jt[2 * nv], wp * (float)e[2], acc);
-          acc = fmaf(Jt[3 * nv], wo * (float)e[3], acc);
-          acc = fmaf(Jt[4 * nv], wo * (float)e[4], acc);
-          acc = fmaf(Jt[5 * nv], wo * (float)e[5], acc);
-        }
-      }
-      if (use_rest) acc += wr * wr * (float)dr[c];
+      float dg = 0.f, gc = g[c];
+      if (use_rest) { dg += wr * wr; gc += wr * wr * (float)dr[c]; }
       if (use_limits) {
         const int j = cjoint[c];
         if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
           const int iq = idxq[j];
-          if (q[iq] < (double)lower[iq]) acc -= wl * wl * (float)((double)lower[iq] - q[iq]);
-          if (q[iq] > (double)upper[iq]) acc += wl * wl * (float)(q[iq] - (double)upper[iq]);
+          if (q[iq] < (double)lower[iq]) { dg += wl * wl; gc -= wl * wl * (float)((double)lower[iq] - q[iq]); }
+          if (q[iq] > (double)upper[iq]) { dg += wl * wl; gc += wl * wl * (float)(q[iq] - (double)upper[iq]); }
         }
       }
-      g[c] = acc;
-      gg += acc * acc;
+      jtj[coff[c] + c] += dg;
+      g[c] = gc;
+      gg += gc * gc;
     }
     gg = tm.sum(gg);
     tm.sync();
     return sqrtf(gg);
   };
 
-  // Solve (J^T J + damp I) delta = -g in float32.  Returns false if the factorization failed.
+  // Solve (J^T J + damp I) delta = -g in float32 with a right-looking Cholesky on the packed
+  // column-major triangle (lanes over the trailing entries).  Returns false if it failed.
   auto solve = [&](float damp) -> bool {
-    const int ld = nv + 1;
     float* Lm = work;
-    for (int k = tl; k < tri(nv); k += T) {
-      int i = (int)((sqrtf(8.f * k + 1.f) - 1.f) * 0.5f);
-      while (tri(i + 1) <= k) ++i;
-      while (tri(i) > k) --i;
-      const int j = k - tri(i);
-      Lm[i * ld + j] = jtj[k] + (i == j ? damp : 0.f);
+    const int ntri = tri(nv);
+    for (int e = tl; e < ntri; e += T) {
+      const int ik = trik[e];
+      Lm[e] = jtj[e] + ((ik & 255) == (ik >> 8) ? damp : 0.f);
     }
     tm.sync();
     bool ok = true;
+    int off = 0;  // first packed entry of the columns right of j
     for (int j = 0; j < nv; ++j) {
-      const float djj = Lm[j * ld + j];
+      const int cj = coff[j];
+      const float djj = Lm[cj + j];
       if (!(djj > 0.f) || !isfinite(djj)) { ok = false; break; }
       const float dj = sqrtf(djj);
       const float inv = 1.f / dj;
       tm.sync();
-      if (tl == 0) Lm[j * ld + j] = dj;
-      for (int i = j + 1 + tl; i < nv; i += T) Lm[i * ld + j] *= inv;
+      if (tl == 0) { Lm[cj + j] = dj; dinv[j] = inv; }
+      for (int i = j + 1 + tl; i < nv; i += T) Lm[cj + i] *= inv;
       tm.sync();
-      const int m = nv - j - 1;
-      const int ne = tri(m);
-      for (int e = tl; e < ne; e += T) {
-        int r = (int)((sqrtf(8.f * e + 1.f) - 1.f) * 0.5f);
-        while (tri(r + 1) <= e) ++r;
-        while (tri(r) > e) --r;
-        const int c = e - tri(r);
-        const int i = j + 1 + r, k = j + 1 + c;
-        Lm[i * ld + k] = fmaf(-Lm[i * ld + j], Lm[k * ld + j], Lm[i * ld + k]);
+      off += nv - j;
+      for (int e = off + tl; e < ntri; e += T) {
+        const int ik = trik[e];
+        Lm[e] = fmaf(-Lm[cj + (ik & 255)], Lm[cj + (ik >> 8)], Lm[e]);
       }
       tm.sync();
     }
@@ -457,17 +464,18 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     for (int i = tl; i < nv; i += T) delta[i] = -g[i];
     tm.sync();
     for (int j = 0; j < nv; ++j) {
-      const float yj = delta[j] / Lm[j * ld + j];
+      const float yj = delta[j] * dinv[j];
       tm.sync();
       if (tl == 0) delta[j] = yj;
-      for (int i = j + 1 + tl; i < nv; i += T) delta[i] = fmaf(-Lm[i * ld + j], yj, delta[i]);
+      const int cj = coff[j];
+      for (int i = j + 1 + tl; i < nv; i += T) delta[i] = fmaf(-Lm[cj + i], yj, delta[i]);
       tm.sync();
     }
     for (int j = nv - 1; j >= 0; --j) {
-      const float xj = delta[j] / Lm[j * ld + j];
+      const float xj = delta[j] * dinv[j];
       tm.sync();
       if (tl == 0) delta[j] = xj;
-      for (int i = tl; i < j; i += T) delta[i] = fmaf(-Lm[j * ld + i], xj, delta[i]);
+      for (int i = tl; i < j; i += T) delta[i] = fmaf(-Lm[coff[i] + j], xj, delta[i]);
       tm.sync();
     }
     return true;
@@ -578,7 +586,7 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
   tm.tl = lane % T;
   tm.mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (team * T));
   const br_tree_t& tree = P.trees[cls];
-  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets);
+  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T);
   if (team < count) {
     const int prob = P.b.order[first + team];
     solve_problem<T>(P, tree, prob, wsm + team * L.total, tm);
@@ -611,7 +619,8 @@ using namespace br;
 
 extern "C" int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets) {
   if (!tree || max_targets < 0) return BR_EINVAL;
-  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets).total;
+  const int T = tree->nv <= 8 ? 8 : tree->nv <= 16 ? 16 : 32;
+  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T).total;
 }
 
 extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
@@ -640,7 +649,7 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
     p.trees[c] = b.trees[c];
     p.team[c] = T;
-    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets).total;
+    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;
@@ -745,7 +754,7 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
     p.trees[c] = b.trees[c];
     p.team[c] = T;
-    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets).total;
+    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;

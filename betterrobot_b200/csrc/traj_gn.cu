@@ -20,9 +20,11 @@
 // followed by block forward / backward substitution: O(T nv^3) instead of O((T nv)^3).
 //
 // Precision: the normal matrix has condition ~1e8 (acceleration stiffness
-// (w/dt^2)^2 against a 1e-6 regularisation), beyond a float32 Cholesky, so the
-// iterate, residuals, bands, factorization and solves are float64; the pose
-// Jacobian columns are float32 (as in lm_solve.cu) and promoted.
+// (w/dt^2)^2 against a 1e-6 regularisation).  A float32 factorization fails there,
+// and even float32 Jacobian entries (relative error ~1e-7) move the Gauss-Newton
+// step by ~1e-1 rad along the weakly constrained directions, so the whole
+// trajectory solver — iterate, residuals, pose Jacobians, bands, factorization,
+// solves — is float64.
 //
 // After the solve, the gradient of the final cost w.r.t. the goal pose (a right
 // perturbation T_goal exp(eps)) is the adjoint -w_goal^2 Jl^-1(xi)^T xi of the
@@ -214,24 +216,22 @@ __global__ void traj_gn_kernel(const TrajParams P) {
                                      make_double4(target.q.x, target.q.y, target.q.z, target.q.w)}), Tee), v, w);
     if (lane == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
     if (J) {
-      const JrInv Jr = jr_inv_se3<9>(f3((float)v.x, (float)v.y, (float)v.z), f3((float)w.x, (float)w.y, (float)w.z));
-      const float4 qe = make_float4((float)Tee.q.x, (float)Tee.q.y, (float)Tee.q.z, (float)Tee.q.w);
-      const float3 pe = f3((float)Tee.t.x, (float)Tee.t.y, (float)Tee.t.z);
+      const DJrInv Jr = djr_inv_se3<9>(v, w);
+      const double4 qc = dqconj(Tee.q);
       for (int k = lane; k < nv; k += kWarp) {
-        float3 ol = f3(0.f, 0.f, 0.f), oa = f3(0.f, 0.f, 0.f);
+        double3 ol = d3(0, 0, 0), oa = d3(0, 0, 0);
         if ((sup >> cjoint[k]) & 1ull) {
           const DPose Tj = ldd8(pose + 8 * cjoint[k]);
-          const float4 qj = make_float4((float)Tj.q.x, (float)Tj.q.y, (float)Tj.q.z, (float)Tj.q.w);
-          const float3 a = qrot(qj, f3(caxis[4 * k], caxis[4 * k + 1], caxis[4 * k + 2]));
-          float3 lin, ang;
+          const double3 a = dqrot(Tj.q, d3(caxis[4 * k], caxis[4 * k + 1], caxis[4 * k + 2]));
+          double3 lin, ang;
           if (ckind[k] == 0) {
-            lin = cross(a, sub(pe, f3((float)Tj.t.x, (float)Tj.t.y, (float)Tj.t.z)));
+            lin = dcross(a, dsub(Tee.t, Tj.t));
             ang = a;
           } else {
             lin = a;
-            ang = f3(0.f, 0.f, 0.f);
+            ang = d3(0, 0, 0);
           }
-          jr_inv_apply(Jr, qrot_inv(qe, lin), qrot_inv(qe, ang), ol, oa);
+          djr_inv_apply(Jr, dqrot(qc, lin), dqrot(qc, ang), ol, oa);
         }
         J[0 * nv + k] = ol.x; J[1 * nv + k] = ol.y; J[2 * nv + k] = ol.z;
         J[3 * nv + k] = oa.x; J[4 * nv + k] = oa.y; J[5 * nv + k] = oa.z;
@@ -468,14 +468,15 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   if (P.goal_grad && has_goal) {
     pose_term(x, T - 1, tgt_goal, rg, nullptr);
     if (lane == 0) {
-      const float3 v = f3((float)rg[0], (float)rg[1], (float)rg[2]);
-      const float3 w = f3((float)rg[3], (float)rg[4], (float)rg[5]);
-      const JrInv Jl = jr_inv_se3<20>(scale(v, -1.f), scale(w, -1.f));   // Jl^-1(xi) = Jr^-1(-xi)
-      float3 gl, ga;
-      jr_inv_T_apply(Jl, v, w, gl, ga);
-      const float k = -(float)(wg * wg);
+      const double3 v = d3(rg[0], rg[1], rg[2]);
+      const double3 w = d3(rg[3], rg[4], rg[5]);
+      const DJrInv Jl = djr_inv_se3<20>(dscale(v, -1.0), dscale(w, -1.0));   // Jl^-1(xi) = Jr^-1(-xi)
+      double3 gl, ga;
+      djr_inv_T_apply(Jl, v, w, gl, ga);
+      const double k = -wg * wg;
       float* o = P.goal_grad + traj * 6;
-      o[0] = k * gl.x; o[1] = k * gl.y; o[2] = k * gl.z; o[3] = k * ga.x; o[4] = k * ga.y; o[5] = k * ga.z;
+      o[0] = (float)(k * gl.x); o[1] = (float)(k * gl.y); o[2] = (float)(k * gl.z);
+      o[3] = (float)(k * ga.x); o[4] = (float)(k * ga.y); o[5] = (float)(k * ga.z);
     }
   }
   if (lane == 0) {

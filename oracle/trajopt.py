@@ -30,7 +30,7 @@ from . import lie
 class TrajSettings:
     dt: float = 0.05
     w_goal: float = 1.0
-    w_start: float = 0.0
+    w_start: float = 1.0
     w_accel: float = 1e-2
     w_limit: float = 0.1
     w_ref: float = 1e-3

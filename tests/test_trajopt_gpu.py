@@ -1,0 +1,138 @@
+"""GPU parity of the batched trajectory optimiser (block-banded GN / LM) and its goal adjoint.
+
+Bars:
+* reference ``solve_trajopt`` (golden, float64): same converged verdict, trajectory
+  within 1e-4 rad, final stacked residual within 1e-4;
+* float64 oracle at the config-4 size (chain7, T = 64): same verdicts, trajectories
+  within 1e-4, final cost within 1e-6 absolute + 1e-4 relative;
+* goal-pose gradient (d cost / d eps, goal -> goal exp(eps)): against float64 central
+  differences (eps 1e-6) of the goal term at the returned trajectory,
+  |g - fd| <= 1e-4 |fd| + 2e-6 (the absolute part covers the float32 rounding of the
+  returned trajectory, ~1e-7 rad per joint, which the kernel's float64 iterate does
+  not have); against re-solved float64 optimal costs (envelope theorem), within
+  2e-2 relative, for trajectories whose every solve converged.
+
+Goals are start + U(+-0.5) rad per joint: with +-1 rad, undamped GN oscillates
+without converging on ~20% of trajectories even in float64.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from betterrobot_b200 import synthetic as syn
+from betterrobot_b200 import trajopt as btr
+from oracle import kinematics as K, lie, trajopt as ot
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(N, T, seed, spread=0.5):
+    m, m64 = syn.model_from_spec(syn.chain_spec()), syn.model_from_spec(syn.chain_spec(), dtype=torch.float64)
+    fid = m.frame_id("ee")
+    qs, qg = syn.trajopt_endpoints(m64, N, seed, spread)
+    oMi, _ = K.forward_kinematics(m64, qg.numpy())
+    goal = K.frame_placements(m64, oMi, [fid])[:, 0]
+    oMi, _ = K.forward_kinematics(m64, qs.numpy())
+    start = K.frame_placements(m64, oMi, [fid])[:, 0]
+    X0 = np.repeat(qs.numpy()[:, None, :], T, 1)
+    return m, m64, fid, goal, start, X0
+
+
+def _gpu(m, fid, goal, start, X0, cfg):
+    return btr.solve_trajopt_batched(m, fid, torch.from_numpy(goal).float().cuda(),
+                                     torch.from_numpy(X0).float().cuda(),
+                                     start=torch.from_numpy(start).float().cuda(), cfg=cfg)
+
+
+def test_reference_solve_trajopt_golden():
+    g = np.load(os.path.join(GOLDEN, "trajopt_chain7.npz"))
+    T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
+    m = syn.model_from_spec(syn.chain_spec())
+    m64 = syn.model_from_spec(syn.chain_spec(), dtype=torch.float64)
+    fid = m.frame_id("ee")
+    X0 = np.repeat(g["q_start"][:, None, :], int(T), 1)
+    cfg = btr.TrajOptConfig(dt=float(dt), w_goal=float(wg), w_start=float(ws), w_accel=float(wa), w_limit=float(wl),
+                            w_ref=float(wr), tol=float(tol), max_iter=int(mi))
+    out = _gpu(m, fid, g["goal"], g["start"], X0, cfg)
+    np.testing.assert_array_equal(out.converged.cpu().numpy(), g["converged"])
+    X = out.q.cpu().double().numpy()
+    assert np.abs(X - g["X"]).max() <= 1e-4, np.abs(X - g["X"]).max()
+    s = ot.TrajSettings(dt=dt, w_goal=wg, w_start=ws, w_accel=wa, w_limit=wl, w_ref=wr, tol=tol, max_iter=int(mi))
+    r, _ = ot.residual_jacobian(m64, X, fid, g["goal"], g["start"], X0, s, want_jac=False)
+    assert np.abs(r - g["residual"]).max() <= 1e-4
+
+
+@pytest.mark.parametrize("optimizer", ["gn", "lm"])
+def test_config4_size_vs_oracle(optimizer):
+    T, N = 64, 16
+    m, m64, fid, goal, start, X0 = _setup(N, T, 51)
+    cfg = btr.TrajOptConfig(optimizer=optimizer, max_iter=30)
+    out = _gpu(m, fid, goal, start, X0, cfg)
+    s = ot.TrajSettings(optimizer=optimizer, max_iter=30)
+    ref = ot.solve(m64, X0, fid, goal, start, s)
+    conv = out.converged.cpu().numpy()
+    assert (conv == ref.converged).mean() >= 0.9, (conv, ref.converged)
+    both = conv & ref.converged
+    X = out.q.cpu().double().numpy()
+    assert np.abs(X[both] - ref.X[both]).max() <= 1e-4
+    cost = out.cost.cpu().double().numpy()
+    np.testing.assert_allclose(cost[both], ref.cost[both], rtol=1e-4, atol=1e-6)
+
+
+def test_goal_gradient_adjoint_vs_float64_fd():
+    T, N = 64, 8
+    m, m64, fid, goal, start, X0 = _setup(N, T, 61)
+    cfg = btr.TrajOptConfig(max_iter=30)
+    s = ot.TrajSettings(max_iter=30)
+    out = _gpu(m, fid, goal, start, X0, cfg)
+    X = out.q.cpu().double().numpy()
+    g = out.goal_grad.cpu().double().numpy()
+    goal32 = goal.astype(np.float32).astype(np.float64)
+    h = 1e-6
+    fd = np.zeros((N, 6))
+    for k in range(6):
+        e = np.zeros((N, 6))
+        e[:, k] = h
+        gp = lie.se3_compose(goal32, lie.se3_exp(e))
+        gm = lie.se3_compose(goal32, lie.se3_exp(-e))
+        fd[:, k] = (ot.goal_cost(m64, X, fid, gp, s) - ot.goal_cost(m64, X, fid, gm, s)) / (2 * h)
+    err = np.linalg.norm(g - fd, axis=1)
+    assert (err <= 1e-4 * np.linalg.norm(fd, axis=1) + 2e-6).all(), (err, np.linalg.norm(fd, axis=1))
+
+
+def test_goal_gradient_envelope_vs_resolved_cost():
+    """d(optimal cost)/d(goal) by re-solving in float64 equals the adjoint at convergence."""
+    T, N = 64, 4
+    m, m64, fid, goal, start, X0 = _setup(N, T, 71)
+    cfg = btr.TrajOptConfig(max_iter=60, tol=1e-8)
+    s = ot.TrajSettings(max_iter=60, tol=1e-10)
+    out = _gpu(m, fid, goal, start, X0, cfg)
+    g = out.goal_grad.cpu().double().numpy()
+    ok = out.converged.cpu().numpy().copy()
+    h = 1e-5
+    fd = np.zeros((N, 6))
+    for k in range(6):
+        e = np.zeros((N, 6))
+        e[:, k] = h
+        rp = ot.solve(m64, X0, fid, lie.se3_compose(goal, lie.se3_exp(e)), start, s)
+        rm = ot.solve(m64, X0, fid, lie.se3_compose(goal, lie.se3_exp(-e)), start, s)
+        ok &= rp.converged & rm.converged
+        fd[:, k] = (rp.cost - rm.cost) / (2 * h)
+    assert ok.sum() >= 2, ok
+    rel = np.linalg.norm(g - fd, axis=1) / np.maximum(np.linalg.norm(fd, axis=1), 1e-12)
+    assert (rel[ok] <= 2e-2).all(), rel
+
+
+def test_trajopt_rejects_free_flyer_and_bad_shapes():
+    m = syn.model_from_spec(syn.humanoid_spec())
+    X0 = torch.zeros(2, 8, m.nq, device="cuda")
+    with pytest.raises(Exception):
+        btr.solve_trajopt_batched(m, 0, torch.zeros(2, 7, device="cuda"), X0)
+    mc = syn.model_from_spec(syn.chain_spec())
+    with pytest.raises(btr.ShapeError):
+        btr.solve_trajopt_batched(mc, 0, torch.zeros(3, 7, device="cuda"), torch.zeros(2, 8, mc.nq, device="cuda"))
