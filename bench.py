@@ -174,6 +174,11 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def shard_seed(rank: int) -> int:
+    """Workload seed of a rank: every rank solves its own, disjoint problem set (replicas)."""
+    return 7 + 1000 * rank
+
+
 def dist_setup():
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -199,7 +204,8 @@ def reduce(x: float, world: int, op: str) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -215,11 +221,17 @@ def bench_ik(steps: int, warmup: int, seed: int):
     settings = bik.settings_from(
         bik.IKCostConfig(rest_weight=SETTINGS["rest_weight"], limit_weight=SETTINGS["limit_weight"]),
         bik.OptimizerConfig(max_iter=MAX_ITER, lam0=SETTINGS["lam0"], factor=SETTINGS["factor"], tol=SETTINGS["tol"]))
-    pk = bik.PackedIK([c["model"] for c in wl], [c["frames"] for c in wl], [c["n_targets"] for c in wl],
-                      warps_per_cta=4)
+    from betterrobot_b200 import autotune
     tg_dev = [c["targets"] for c in wl]
     q0_dev = [c["q0"].float().cuda() for c in wl]
-    pk.set_inputs(tg_dev, q0_dev)
+
+    def make(teams, warps):
+        p = bik.PackedIK([c["model"] for c in wl], [c["frames"] for c in wl], [c["n_targets"] for c in wl],
+                         team_sizes=teams, warps_per_cta=warps)
+        p.set_inputs(tg_dev, q0_dev)
+        return p
+    teams, warps, _ = autotune.tune(make, settings)       # outside the timed region
+    pk = make(teams, warps)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda")  # > 126 MB L2
     for _ in range(warmup):
@@ -266,8 +278,21 @@ def bench_ik(steps: int, warmup: int, seed: int):
         e1.record(stream)
         torch.cuda.synchronize()
         et.append(e0.elapsed_time(e1))
+    # the same solve replayed from a CUDA graph
+    g = pk.capture(settings)
+    torch.cuda.synchronize()
+    gt = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.replay()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        gt.append(e0.elapsed_time(e1))
     return {"ms": ms, "reached": reached, "converged": conv, "problems": pk.P, "iters_mean": float(iters.mean()),
-            "e2e_ms": float(np.mean(et)), "h2d": h2d, "d2h": d2h, "launches": steps, "wl": wl}
+            "e2e_ms": float(np.mean(et)), "h2d": h2d, "d2h": d2h, "launches": steps, "wl": wl,
+            "graph_ms": float(np.mean(gt)), "team_sizes": teams, "warps_per_cta": warps}
 
 
 def bench_plain_gpu(wl):
@@ -539,7 +564,7 @@ def main():
     with ClockSampler(local) as clk:
         barrier(world)
         torch.cuda.synchronize()
-        ik = bench_ik(args.steps, warmup, seed=7 + 1000 * rank)
+        ik = bench_ik(args.steps, warmup, seed=shard_seed(rank))
         barrier(world)
     clocks = clk.summary()
     fkj = bench_fkj(args.steps, warmup)
@@ -561,7 +586,9 @@ def main():
                      "achieved": fkj["gbs"], "peak": peak, "unit": "GB/s", "frac": fkj["gbs"] / peak,
                      "traffic": None, "peak_kind": peak_kind, "ms_per_launch": fkj["ms_per_launch"]},
         "ik": {"problems": ik["problems"] * world, "reached_1e-4": reached, "converged": ik["converged"],
-               "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1},
+               "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1,
+               "graph_replay_ms": ik["graph_ms"], "autotuned": {"team_sizes": ik["team_sizes"],
+                                                                "warps_per_cta": ik["warps_per_cta"]}},
         "clocks": clocks, "gpu_launches": ik["launches"],
     }
     if adj is not None:

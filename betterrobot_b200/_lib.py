@@ -80,6 +80,8 @@ SIGNATURES: dict[str, tuple] = {
     "br_trajopt_solve": (c_int32, [ctypes.POINTER(BrTree), c_int32, c_int64, c_int32, c_void_p, c_void_p, c_void_p,
                                    c_void_p, ctypes.POINTER(TrajSettings), c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p]),
+    "br_configuration_op": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int32, c_int32, c_void_p, c_void_p,
+                                      c_int64, c_void_p, c_void_p]),
     "br_pose_loss": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
                                c_int32, c_void_p, c_void_p, c_void_p]),
     "br_pose_loss_backward": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_void_p, c_int64, c_void_p, c_int32,

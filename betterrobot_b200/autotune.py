@@ -1,0 +1,66 @@
+"""Autotuner for the packed persistent LM launch.
+
+Picks, for a given packed batch, the team size (lanes per problem: 8, 16 or 32)
+of every robot class and the number of warps per CTA, by timing candidate
+launches of the real batch with CUDA events.  Results are cached per batch
+signature (robot shapes, target counts, problem counts), so a serving loop pays
+the search once.
+
+Candidates: team sizes from {8, 16, 32} not smaller than the class's default
+bucket minus one step (a 36-DOF humanoid may run on 16 or 32 lanes, a 7-DOF chain
+on 8 or 16), crossed with warps per CTA in {2, 4, 8}.
+"""
+
+from __future__ import annotations
+
+import itertools
+
+import torch
+
+_CACHE: dict = {}
+
+
+def _team_choices(nv: int) -> list[int]:
+    if nv <= 8:
+        return [8, 16]
+    if nv <= 16:
+        return [8, 16, 32]
+    return [16, 32]
+
+
+def signature(pk) -> tuple:
+    return (tuple((m.njoints, m.nq, m.nv) for m in pk.models), tuple(pk.counts), pk.K, str(pk.device))
+
+
+def tune(make_packed, settings, warps=(2, 4, 8), reps: int = 3, max_candidates: int = 24):
+    """Return ``(team_sizes, warps_per_cta, ms)`` of the fastest candidate.
+
+    ``make_packed(team_sizes, warps_per_cta)`` builds a ``PackedIK`` with its inputs set.
+    """
+    base = make_packed(None, 4)
+    key = signature(base)
+    if key in _CACHE:
+        return _CACHE[key]
+    choices = [_team_choices(m.nv) for m in base.models]
+    cands = list(itertools.product(*choices))[:max_candidates]
+    stream = torch.cuda.current_stream()
+    best = None
+    for teams in cands:
+        for w in warps:
+            try:
+                pk = make_packed(list(teams), w)
+                pk.solve(settings)  # warm-up
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(reps):
+                    pk.solve(settings)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+            except Exception:
+                continue
+            if best is None or ms < best[2]:
+                best = (list(teams), w, ms)
+    _CACHE[key] = best
+    return best

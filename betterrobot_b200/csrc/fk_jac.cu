@@ -186,11 +186,34 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
   const int rounds = tree.rounds;
   const int64_t stride = (int64_t)gridDim.x * wpc;
 
-  for (int64_t b = (int64_t)blockIdx.x * wpc + warp; b < p.batch; b += stride) {
+  // q of the warp's next configuration is loaded into registers one iteration
+  // ahead, so its global-load latency overlaps the current configuration's work
+  // (nq <= BR_MAX_NQ = 128: at most 4 values per lane)
+  float qn[4];
+  const int64_t b0 = (int64_t)blockIdx.x * wpc + warp;
+  if (kFromQ && b0 < p.batch) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i = lane + kWarp * k;
+      qn[k] = i < nq ? __ldg(p.q + b0 * nq + i) : 0.f;
+    }
+  }
+  for (int64_t b = b0; b < p.batch; b += stride) {
     // ---- world joint placements --------------------------------------
     if (kFromQ) {
-      const float* qb = p.q + b * nq;
-      for (int i = lane; i < nq; i += kWarp) wq[i] = __ldg(qb + i);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = lane + kWarp * k;
+        if (i < nq) wq[i] = qn[k];
+      }
+      const int64_t bn = b + stride;
+      if (bn < p.batch) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int i = lane + kWarp * k;
+          qn[k] = i < nq ? __ldg(p.q + bn * nq + i) : 0.f;
+        }
+      }
       __syncwarp();
       Pose T[2];
       int anc[2];

@@ -249,6 +249,25 @@ class PackedIK:
                   self.warps_per_cta, self.scratch.data_ptr(), SCRATCH_BYTES,
                   stream if stream is not None else _lib.stream_ptr(self.device))
 
+    def capture(self, settings: IKSettings) -> "torch.cuda.CUDAGraph":
+        """Capture one solve (scratch zeroing + the persistent launch) in a CUDA graph.
+
+        Replaying the graph re-solves from the current contents of the input buffers
+        (``set_inputs`` copies new targets / start configurations into them in place).
+        """
+        self._graph_settings = settings  # the struct must outlive the capture call
+        with torch.cuda.device(self.device):
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                self.solve(settings)           # warm-up outside capture (module load, smem attribute)
+            torch.cuda.current_stream().wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.solve(settings)
+        self.graph = g
+        return g
+
     def q_of(self, c: int) -> torch.Tensor:
         s0, n, nq = int(self.class_start[c]), self.counts[c], self.models[c].nq
         o = int(self.q_offset_np[s0])

@@ -134,6 +134,9 @@ class DeviceTree:
         self.struct = st
         self.ptr = ctypes.pointer(st)
         self.device = device
+        act = [j for j in range(a.nj) if int(model.nqs[j]) > 0]
+        self.active = torch.tensor(act or [0], dtype=torch.int32, device=device)
+        self.n_active = len(act)
 
 
 _CACHE: dict[tuple[int, str], DeviceTree] = {}

@@ -254,6 +254,19 @@ BR_API int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t n_t
                             const br_traj_settings_t* settings, float* x, int32_t* iters, int32_t* status,
                             float* cost, float* goal_grad, void* stream);
 
+/* ==== configuration-space retraction / difference ======================== */
+#define BR_OP_INTEGRATE 0   /* out[B, nq] = a (+) b,  a = q [B, nq], b = v [B, nv]      */
+#define BR_OP_DIFFERENCE 1  /* out[B, nv] = b (-) a,  a = q0 [B, nq], b = q1 [B, nq]    */
+
+/*
+ * Batched Model.integrate / Model.difference
+ * (src/better_robot/data_model/model.py:160-190): per joint q + v / q1 - q0, and for
+ * a free-flyer normalize(q exp(v)) / log(q0^-1 q1).  active_joints is a DEVICE array
+ * of the n_active joint ids with nq > 0.
+ */
+BR_API int br_configuration_op(const br_tree_t* tree, const int32_t* active_joints, int32_t n_active, int32_t op,
+                               const float* a, const float* b, int64_t batch, float* out, void* stream);
+
 /* Library build information (for logging): returns a static string. */
 BR_API const char* br_version(void);
 

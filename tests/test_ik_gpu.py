@@ -4,9 +4,10 @@ Bar (float32 kernel vs float64 reference/oracle):
 * same converged / not-converged verdict;
 * final stacked residual within 1e-4 (max abs difference of the residual vectors);
 checked on the reference's own float64 solves (golden fixtures) and on larger
-seeded batches against the oracle.  ``VERDICT_RATE`` is the fraction of problems
-that must meet both; float32 can flip an accept/reject decision at the noise
-floor of the cost, which the per-case rates below bound.
+seeded batches against the oracle.  The kernel decides accept / reject and
+convergence on a float64 cost; its float32 normal equations still move iterates
+by ~1e-7, which can flip a verdict on problems that end right at the tolerance,
+so the batch tests require the bar on >= 90-95% of problems (measured 94-100%).
 """
 
 import os
@@ -83,7 +84,7 @@ def test_config0_chain_random_starts_vs_oracle():
                                with_residual=True)
     ok, conv, dres = _agreement(out, ref.converged, ref.residual)
     both = ref.converged & conv
-    assert (conv == ref.converged).mean() >= 0.9, (conv.mean(), ref.converged.mean())
+    assert (conv == ref.converged).mean() >= 0.95, (conv.mean(), ref.converged.mean())
     assert np.median(dres[both]) <= RES_TOL
     assert (dres[both] <= RES_TOL).mean() >= 0.95
 
@@ -108,7 +109,7 @@ def test_noisy_start_vs_oracle(robot, frames, rest):
                                with_residual=True)
     ok, conv, dres = _agreement(out, ref.converged, ref.residual)
     assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
-    assert (conv == ref.converged).mean() >= 0.8, (conv.mean(), ref.converged.mean())
+    assert (conv == ref.converged).mean() >= 0.9, (conv.mean(), ref.converged.mean())
 
 
 def test_uneven_mix_single_launch_matches_per_class():
@@ -189,3 +190,38 @@ def test_unsupported_options_raise():
             bik.solve_ik_batched(m, [0], T, q0, optimizer_cfg=opt)
     with pytest.raises(bik.ShapeError):
         bik.solve_ik_batched(m, [m.nframes], T, q0)
+
+
+def test_autotune_and_graph_replay_match_direct_solve():
+    from betterrobot_b200 import autotune
+    models = [_models(n) for n in ("humanoid", "chain7")]
+    frames, nts, tg, q0s = [], [], [], []
+    for (m, m64), names in zip(models, (["track0", "track1"], ["ee", "body_link5"])):
+        P = 48
+        fids = np.array([m.frame_id(f) for f in names], np.int32)
+        q_star = syn.random_q(m64, P, 90, rev_range=2.5, base_translation=0.5)
+        oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+        frames.append(np.broadcast_to(fids, (P, 2)))
+        nts.append(np.full(P, 2, np.int32))
+        tg.append(torch.from_numpy(K.frame_placements(m64, oMi, list(fids))).float().cuda())
+        q0s.append(syn.noisy_start(m64, q_star, 0.3, 91).float().cuda())
+    settings = bik.settings_from(bik.IKCostConfig(rest_weight=1e-3),
+                                 bik.OptimizerConfig(max_iter=40, lam0=1e-3, factor=10.0))
+
+    def make(teams, warps):
+        p = bik.PackedIK([m for m, _ in models], frames, nts, team_sizes=teams, warps_per_cta=warps)
+        p.set_inputs(tg, q0s)
+        return p
+    teams, warps, ms = autotune.tune(make, settings, reps=1)
+    assert ms > 0 and len(teams) == 2
+    ref = make(None, 4)
+    ref.solve(settings)
+    pk = make(teams, warps)
+    g = pk.capture(settings)
+    pk.x.fill_(float("nan"))
+    g.replay()
+    torch.cuda.synchronize()
+    # team size changes the reduction order inside a problem: results agree to float32 rounding
+    for c in range(2):
+        assert float((pk.q_of(c) - ref.q_of(c)).abs().max()) < 1e-3
+    assert (pk.status == ref.status).float().mean() >= 0.95

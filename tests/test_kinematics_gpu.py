@@ -153,3 +153,22 @@ def test_boundary_errors():
     with pytest.raises(ValueError):
         d = br.forward_kinematics(m, torch.tensor([[0, 0, 0, 0, 0, 0, 1.0] + [0.0] * 30], device="cuda"))
         br.get_frame_jacobian(m, d, 0, reference="bogus")
+
+
+@pytest.mark.parametrize("name", ["humanoid", "dual_arm"])
+def test_integrate_difference_match_oracle(name):
+    from betterrobot_b200.configuration import difference, integrate
+    m = syn.model_from_spec(SPECS[name])
+    m64 = syn.model_from_spec(SPECS[name], dtype=torch.float64)
+    q = syn.random_q(m64, 300, 5, rev_range=2.5, base_translation=1.0)
+    v = torch.from_numpy(np.random.default_rng(6).normal(0, 0.4, size=(300, m.nv)))
+    q1 = syn.noisy_start(m64, q, 0.3, 7)
+    qi = integrate(m, q.float().cuda(), v.float().cuda())
+    ref = K.integrate(m64, q.float().double().numpy(), v.float().double().numpy())
+    np.testing.assert_allclose(qi.cpu().double().numpy(), ref, atol=2e-6, rtol=0)
+    dv = difference(m, q.float().cuda(), q1.float().cuda())
+    ref = K.difference(m64, q.float().double().numpy(), q1.float().double().numpy())
+    np.testing.assert_allclose(dv.cpu().double().numpy(), ref, atol=2e-6, rtol=0)
+    # round trip: q (+) (q1 (-) q) == q1
+    back = integrate(m, q.float().cuda(), dv)
+    np.testing.assert_allclose(back.cpu().double().numpy(), q1.float().double().numpy(), atol=1e-5, rtol=0)
