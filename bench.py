@@ -45,6 +45,11 @@ MAX_ITER = 100
 SETTINGS = dict(lam0=1e-3, factor=10.0, tol=1e-6, rest_weight=1e-3, limit_weight=0.1)
 FKJ_BATCH = 65536
 FKJ_BYTES_PER_CONFIG = 4 * (37 + 12 * 7 + 12 * 6 * 36)  # q read + oMf + J written = 10,852 B
+# DRAM bytes (read + write) of one fk_jac_kernel launch at B = 65,536, 12 frames, from an ncu capture
+# of ``bench.py --only fkj`` (dram__bytes_read.sum 9.77 MB + dram__bytes_write.sum 642.18 MB); the
+# rest of the 711 MB of output is still in L2 when the launch ends.
+FKJ_TRAFFIC_BYTES = 9.766e6 + 642.179e6
+JOINT_OPS_BATCH = 1 << 20
 REACH_TOL = 1e-4
 CANDIDATES = {
     "humanoid": [f"track{i}" for i in range(6)],
@@ -213,7 +218,8 @@ def reduce(x: float, world: int, op: str) -> float:
 # ---------------------------------------------------------------------------
 # fused LM-IK (headline)
 # ---------------------------------------------------------------------------
-def bench_ik(steps: int, warmup: int, seed: int):
+def bench_ik(steps: int, warmup: int, seed: int, pinned=None):
+    """``pinned = (team_sizes, warps_per_cta)`` skips the autotuner (used to profile one known launch shape)."""
     import torch
     from betterrobot_b200 import ik as bik
     wl = make_workload(N_PROBLEMS, seed)
@@ -230,7 +236,10 @@ def bench_ik(steps: int, warmup: int, seed: int):
                          team_sizes=teams, warps_per_cta=warps)
         p.set_inputs(tg_dev, q0_dev)
         return p
-    teams, warps, _ = autotune.tune(make, settings)       # outside the timed region
+    if pinned is None:
+        teams, warps, _ = autotune.tune(make, settings)   # outside the timed region
+    else:
+        teams, warps = pinned
     pk = make(teams, warps)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda")  # > 126 MB L2
@@ -363,6 +372,41 @@ def bench_fkj(steps: int, warmup: int, seed: int = 1):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     return {"ms_per_launch": ms, "gbs": FKJ_BATCH * FKJ_BYTES_PER_CONFIG / (ms * 1e-3) / 1e9, "launches": steps}
+
+
+def bench_joint_ops(steps: int, warmup: int):
+    """Model.integrate / Model.difference on the humanoid (nq 37, nv 36), B = 1,048,576 configurations.
+
+    Algorithmic bytes per configuration: integrate reads q (37) and v (36) and writes q' (37);
+    difference reads q0, q1 (2 x 37) and writes v (36): 4 * 110 = 440 B for either.
+    """
+    import torch
+    from betterrobot_b200 import synthetic as syn
+    from betterrobot_b200.configuration import difference_into, integrate_into
+    m = syn.model_from_spec(syn.humanoid_spec())
+    m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
+    B = JOINT_OPS_BATCH
+    q0 = syn.random_q(m64, B, 41, rev_range=2.5, base_translation=1.0).float().cuda()
+    q1 = syn.random_q(m64, B, 42, rev_range=2.5, base_translation=1.0).float().cuda()
+    v = torch.randn(B, m.nv, device="cuda", generator=torch.Generator("cuda").manual_seed(43)) * 0.3
+    qo = torch.empty_like(q0)
+    vo = torch.empty_like(v)
+    stream = torch.cuda.current_stream()
+    out = {}
+    for name, fn in (("integrate", lambda: integrate_into(m, q0, v, qo)),
+                     ("difference", lambda: difference_into(m, q0, q1, vo))):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_launch": ms, "gbs": B * 440 / (ms * 1e-3) / 1e9, "batch": B}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -510,8 +554,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op PyTorch arm")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
-    ap.add_argument("--only", choices=["ik", "fkj", "adjoint", "trajopt"], default=None,
+    ap.add_argument("--only", choices=["ik", "fkj", "adjoint", "trajopt", "joint_ops"], default=None,
                     help="run one section and print its raw timings (for profiling)")
+    ap.add_argument("--ik-teams", default=None,
+                    help="comma-separated lanes per problem for humanoid,dual_arm,chain7 (skips the autotuner)")
+    ap.add_argument("--ik-warps", type=int, default=4, help="warps per CTA with --ik-teams")
     args = ap.parse_args()
     warmup = max(args.warmup, 3)
     metric = "batched LM-IK solves/s reaching 1e-4 m and 1e-4 rad pose error"
@@ -545,8 +592,13 @@ def main():
         import torch
         dist_setup()
         if args.only == "ik":
-            r = bench_ik(args.steps, warmup, seed=7)
+            pinned = None
+            if args.ik_teams:
+                pinned = ([int(t) for t in args.ik_teams.split(",")], args.ik_warps)
+            r = bench_ik(args.steps, warmup, seed=7, pinned=pinned)
             r.pop("wl")
+        elif args.only == "joint_ops":
+            r = bench_joint_ops(args.steps, warmup)
         elif args.only == "fkj":
             r = bench_fkj(args.steps, warmup)
         elif args.only == "trajopt":
@@ -584,7 +636,7 @@ def main():
                 "d2h_bytes_per_step": ik["d2h"], "ms_per_step": e2e_ms},
         "roofline": {"bound": "hbm", "kernel": "fk_jac_kernel (humanoid B=65536, 12 frames, J + oMf)",
                      "achieved": fkj["gbs"], "peak": peak, "unit": "GB/s", "frac": fkj["gbs"] / peak,
-                     "traffic": None, "peak_kind": peak_kind, "ms_per_launch": fkj["ms_per_launch"]},
+                     "traffic": FKJ_TRAFFIC_BYTES, "peak_kind": peak_kind, "ms_per_launch": fkj["ms_per_launch"]},
         "ik": {"problems": ik["problems"] * world, "reached_1e-4": reached, "converged": ik["converged"],
                "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1,
                "graph_replay_ms": ik["graph_ms"], "autotuned": {"team_sizes": ik["team_sizes"],

@@ -24,11 +24,15 @@ def _check(t: torch.Tensor, n: int, name: str):
         raise DtypeMismatchError(f"{name}.dtype={t.dtype}; the sm_100a path computes in float32")
 
 
-def _run(model, op, a, b, out_dim):
+def _run(model, op, a, b, out_dim, out=None):
     batch = torch.broadcast_shapes(a.shape[:-1], b.shape[:-1])
     af = a.expand(*batch, a.shape[-1]).reshape(-1, a.shape[-1]).contiguous()
     bf = b.expand(*batch, b.shape[-1]).reshape(-1, b.shape[-1]).contiguous()
-    out = torch.empty(af.shape[0], out_dim, device=a.device, dtype=torch.float32)
+    if out is None:
+        out = torch.empty(af.shape[0], out_dim, device=a.device, dtype=torch.float32)
+    elif (out.shape[-1] != out_dim or out.numel() != af.shape[0] * out_dim or not out.is_contiguous()
+          or out.dtype != torch.float32 or out.device != a.device):
+        raise ShapeError(f"out must be a contiguous float32 ({af.shape[0]}, {out_dim}) tensor on {a.device}")
     dt = device_tree(model, a.device)
     with torch.cuda.device(a.device):
         _lib.call("br_configuration_op", dt.ptr, dt.active.data_ptr(), dt.n_active, op, af.data_ptr(), bf.data_ptr(),
@@ -48,3 +52,17 @@ def difference(model, q0: torch.Tensor, q1: torch.Tensor) -> torch.Tensor:
     _check(q0, model.nq, "q0")
     _check(q1, model.nq, "q1")
     return _run(model, OP_DIFFERENCE, q0, q1, model.nv)
+
+
+def integrate_into(model, q: torch.Tensor, v: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+    """``integrate`` writing into a preallocated ``out`` (no allocation; graph-capturable)."""
+    _check(q, model.nq, "q")
+    _check(v, model.nv, "v")
+    return _run(model, OP_INTEGRATE, q, v, model.nq, out)
+
+
+def difference_into(model, q0: torch.Tensor, q1: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+    """``difference`` writing into a preallocated ``out``."""
+    _check(q0, model.nq, "q0")
+    _check(q1, model.nq, "q1")
+    return _run(model, OP_DIFFERENCE, q0, q1, model.nv, out)

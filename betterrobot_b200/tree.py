@@ -89,6 +89,9 @@ class TreeArrays:
             raise ModelInconsistencyError("frame parent joint out of range")
         if (self.idx_q + np.array(model.nqs) > nq).any() or (self.idx_v + np.array(model.nvs) > nv).any():
             raise ModelInconsistencyError("joint q/v slices exceed nq/nv")
+        # slices are laid out cumulatively in joint order, as data_model/model.py builds idx_qs / idx_vs
+        if (np.cumsum([0, *model.nqs[:-1]]) != self.idx_q).any() or (np.cumsum([0, *model.nvs[:-1]]) != self.idx_v).any():
+            raise ModelInconsistencyError("idx_qs / idx_vs must be cumulative in joint order")
         self.frame_placement = np.zeros((self.nf, 8), np.float32)
         for i, f in enumerate(model.frames):
             fp = _np(f.joint_placement)

@@ -155,13 +155,14 @@ def test_boundary_errors():
         br.get_frame_jacobian(m, d, 0, reference="bogus")
 
 
-@pytest.mark.parametrize("name", ["humanoid", "dual_arm"])
-def test_integrate_difference_match_oracle(name):
+@pytest.mark.parametrize("name,B", [("humanoid", 300), ("dual_arm", 300), ("chain7", 45), ("humanoid", 1)])
+def test_integrate_difference_match_oracle(name, B):
+    """B = 300 / 45 leave a ragged last tile of 32 configurations; chain7 has no free-flyer."""
     from betterrobot_b200.configuration import difference, integrate
     m = syn.model_from_spec(SPECS[name])
     m64 = syn.model_from_spec(SPECS[name], dtype=torch.float64)
-    q = syn.random_q(m64, 300, 5, rev_range=2.5, base_translation=1.0)
-    v = torch.from_numpy(np.random.default_rng(6).normal(0, 0.4, size=(300, m.nv)))
+    q = syn.random_q(m64, B, 5, rev_range=2.5, base_translation=1.0)
+    v = torch.from_numpy(np.random.default_rng(6).normal(0, 0.4, size=(B, m.nv)))
     q1 = syn.noisy_start(m64, q, 0.3, 7)
     qi = integrate(m, q.float().cuda(), v.float().cuda())
     ref = K.integrate(m64, q.float().double().numpy(), v.float().double().numpy())
@@ -172,3 +173,23 @@ def test_integrate_difference_match_oracle(name):
     # round trip: q (+) (q1 (-) q) == q1
     back = integrate(m, q.float().cuda(), dv)
     np.testing.assert_allclose(back.cpu().double().numpy(), q1.float().double().numpy(), atol=1e-5, rtol=0)
+
+
+def test_integrate_difference_large_batch_round_trip():
+    """2^20 humanoid configurations (grid-stride over 32-configuration tiles): q (+) (q1 (-) q) == q1."""
+    from betterrobot_b200.configuration import difference, integrate
+    m = syn.model_from_spec(SPECS["humanoid"])
+    m64 = syn.model_from_spec(SPECS["humanoid"], dtype=torch.float64)
+    B = 1 << 20
+    q = syn.random_q(m64, B, 11, rev_range=2.5, base_translation=1.0).float().cuda()
+    q1 = syn.noisy_start(m64, q[:4096].double().cpu(), 0.3, 12).float().cuda().repeat(B // 4096, 1)
+    dv = difference(m, q, q1)
+    back = integrate(m, q, dv)
+    # quaternion slots compared up to sign; translation and revolute slots directly
+    err_t = (back[:, :3] - q1[:, :3]).abs().max()
+    dq = torch.minimum((back[:, 3:7] - q1[:, 3:7]).abs().amax(-1), (back[:, 3:7] + q1[:, 3:7]).abs().amax(-1))
+    err_r = (back[:, 7:] - q1[:, 7:]).abs().max()
+    assert float(err_t) < 2e-5 and float(dq.max()) < 2e-5 and float(err_r) < 2e-5
+    idx = np.random.default_rng(13).choice(B, 256, replace=False)
+    ref = K.difference(m64, q[idx].double().cpu().numpy(), q1[idx].double().cpu().numpy())
+    np.testing.assert_allclose(dv[idx].cpu().double().numpy(), ref, atol=2e-6, rtol=0)
