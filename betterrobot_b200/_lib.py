@@ -82,6 +82,8 @@ SIGNATURES: dict[str, tuple] = {
                                    c_void_p, c_void_p]),
     "br_configuration_op": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int32, c_int32, c_void_p, c_void_p,
                                       c_int64, c_void_p, c_void_p]),
+    "br_lie_op": (c_int32, [c_int32, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
+    "br_lie_op_sizes": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p]),
     "br_pose_loss": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_void_p,
                                c_int32, c_void_p, c_void_p, c_void_p]),
     "br_pose_loss_backward": (c_int32, [ctypes.POINTER(BrTree), c_void_p, c_void_p, c_int64, c_void_p, c_int32,

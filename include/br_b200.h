@@ -267,6 +267,40 @@ BR_API int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t n_t
 BR_API int br_configuration_op(const br_tree_t* tree, const int32_t* active_joints, int32_t n_active, int32_t op,
                                const float* a, const float* b, int64_t batch, float* out, void* stream);
 
+/* ==== batched SE3 / SO3 primitives (the LieOps seam) ====================== */
+/*
+ * Replaces the per-op LieOps protocol (src/better_robot/backends/protocol.py:27-51)
+ * as implemented by src/better_robot/lie/_torch_native_backend.py and the SE3 right
+ * Jacobians of src/better_robot/lie/tangents.py:184-207.  Element sizes (floats):
+ */
+#define BR_LIE_SE3_COMPOSE 0      /* a 7, b 7 -> 7        se3_compose     :237-246 */
+#define BR_LIE_SE3_INVERSE 1      /* a 7      -> 7        se3_inverse     :249-255 */
+#define BR_LIE_SE3_LOG 2          /* a 7      -> 6 [v,w]  se3_log         :289-310 */
+#define BR_LIE_SE3_EXP 3          /* a 6      -> 7        se3_exp         :258-286 */
+#define BR_LIE_SE3_ACT 4          /* a 7, b 3 -> 3        se3_act         :313-315 */
+#define BR_LIE_SE3_ADJOINT 5      /* a 7      -> 36 (6x6 row-major)  se3_adjoint :318-328 */
+#define BR_LIE_SE3_ADJOINT_INV 6  /* a 7      -> 36       se3_adjoint_inv :331-342 */
+#define BR_LIE_SE3_NORMALIZE 7    /* a 7      -> 7        se3_normalize   :358-361 */
+#define BR_LIE_SO3_COMPOSE 8      /* a 4, b 4 -> 4        so3_compose     :134-135 */
+#define BR_LIE_SO3_INVERSE 9      /* a 4      -> 4        so3_inverse     :138-141 */
+#define BR_LIE_SO3_LOG 10         /* a 4      -> 3        so3_log         :162-183 */
+#define BR_LIE_SO3_EXP 11         /* a 3      -> 4        so3_exp         :144-159 */
+#define BR_LIE_SO3_ACT 12         /* a 4, b 3 -> 3        so3_act         :186-199 */
+#define BR_LIE_SO3_TO_MATRIX 13   /* a 4      -> 9 (3x3 row-major)   so3_to_matrix :210-211 */
+#define BR_LIE_SO3_FROM_MATRIX 14 /* a 9      -> 4        so3_from_matrix :206-207 */
+#define BR_LIE_SO3_NORMALIZE 15   /* a 4      -> 4        so3_normalize   :202-203 */
+#define BR_LIE_SE3_JR 16          /* a 6      -> 36       tangents.right_jacobian_se3     :184-201 */
+#define BR_LIE_SE3_JR_INV 17      /* a 6      -> 36       tangents.right_jacobian_inv_se3 :204-207 */
+
+/*
+ * out[i] = op(a[i], b[i]) for i < n, float32, contiguous records.  na and nb are n or
+ * 1 (1 broadcasts that operand); b is ignored by unary ops.  Device pointers.
+ */
+BR_API int br_lie_op(int32_t op, const float* a, int64_t na, const float* b, int64_t nb, float* out, int64_t n,
+                     void* stream);
+/* Floats per element of a, b (0 for unary ops) and out for op; host only. */
+BR_API int br_lie_op_sizes(int32_t op, int32_t* a_floats, int32_t* b_floats, int32_t* out_floats);
+
 /* Library build information (for logging): returns a static string. */
 BR_API const char* br_version(void);
 

@@ -160,3 +160,52 @@ def right_jacobian_se3(xi: np.ndarray, terms: int = 9) -> np.ndarray:
 def right_jacobian_inv_se3(xi: np.ndarray) -> np.ndarray:
     """``tangents.right_jacobian_inv_se3:204-207`` (inverse of the truncated series)."""
     return np.linalg.inv(right_jacobian_se3(xi))
+
+
+def se3_act(T: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """``se3_act:313-315``: ``R p + t``."""
+    return so3_act(T[..., 3:7], p) + T[..., :3]
+
+
+def se3_adjoint(T: np.ndarray) -> np.ndarray:
+    """``se3_adjoint:318-328``: ``[[R, hat(p) R], [0, R]]``."""
+    R = quat_to_matrix(T[..., 3:7])
+    Z = np.zeros_like(R)
+    return np.concatenate([np.concatenate([R, hat(T[..., :3]) @ R], -1), np.concatenate([Z, R], -1)], -2)
+
+
+def se3_adjoint_inv(T: np.ndarray) -> np.ndarray:
+    """``se3_adjoint_inv:331-342``: ``[[R^T, -R^T hat(p)], [0, R^T]]``."""
+    RT = np.swapaxes(quat_to_matrix(T[..., 3:7]), -1, -2)
+    Z = np.zeros_like(RT)
+    return np.concatenate([np.concatenate([RT, -(RT @ hat(T[..., :3]))], -1), np.concatenate([Z, RT], -1)], -2)
+
+
+def so3_normalize(q: np.ndarray) -> np.ndarray:
+    """``so3_normalize:202-203``: ``q / max(|q|, 1e-8)``."""
+    return q / np.maximum(np.linalg.norm(q, axis=-1, keepdims=True), 1e-8)
+
+
+def so3_from_matrix(R: np.ndarray) -> np.ndarray:
+    """Shepperd's method with the reference's branch order, ``_matrix_to_quat:72-125``."""
+    m = R
+    tr = m[..., 0, 0] + m[..., 1, 1] + m[..., 2, 2]
+    s1 = np.sqrt(np.maximum(tr + 1.0, 1e-30)) * 2.0
+    s2 = np.sqrt(np.maximum(1.0 + m[..., 0, 0] - m[..., 1, 1] - m[..., 2, 2], 1e-30)) * 2.0
+    s3 = np.sqrt(np.maximum(1.0 - m[..., 0, 0] + m[..., 1, 1] - m[..., 2, 2], 1e-30)) * 2.0
+    s4 = np.sqrt(np.maximum(1.0 - m[..., 0, 0] - m[..., 1, 1] + m[..., 2, 2], 1e-30)) * 2.0
+    a = m[..., 2, 1] - m[..., 1, 2]
+    b = m[..., 0, 2] - m[..., 2, 0]
+    c = m[..., 1, 0] - m[..., 0, 1]
+    d = m[..., 0, 1] + m[..., 1, 0]
+    e = m[..., 0, 2] + m[..., 2, 0]
+    f = m[..., 1, 2] + m[..., 2, 1]
+    q1 = np.stack([a / s1, b / s1, c / s1, 0.25 * s1], -1)
+    q2 = np.stack([0.25 * s2, d / s2, e / s2, a / s2], -1)
+    q3 = np.stack([d / s3, 0.25 * s3, f / s3, b / s3], -1)
+    q4 = np.stack([e / s4, f / s4, 0.25 * s4, c / s4], -1)
+    c1 = (tr > 0)[..., None]
+    c2 = ((m[..., 0, 0] > m[..., 1, 1]) & (m[..., 0, 0] > m[..., 2, 2]))[..., None]
+    c3 = (m[..., 1, 1] > m[..., 2, 2])[..., None]
+    q = np.where(c1, q1, np.where(c2, q2, np.where(c3, q3, q4)))
+    return q / np.maximum(np.linalg.norm(q, axis=-1, keepdims=True), 1e-12)

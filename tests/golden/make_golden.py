@@ -11,6 +11,8 @@ and outputs in ``tests/golden/*.npz``:
 
 * ``lie.npz``       — ``se3_exp/log``, ``so3_exp/log`` (incl. theta -> 0 and qw < 0),
                       ``right_jacobian_inv_se3`` (the truncated-series inverse).
+* ``lie_ops.npz``   — every other LieOps method (compose, inverse, act, adjoint(_inv),
+                      normalize, to/from matrix) and ``right_jacobian_se3``.
 * ``kin_<robot>.npz`` — ``forward_kinematics`` (oMi, liMi), ``frame_pose_world``,
                       ``get_frame_jacobian`` in all three reference frames,
                       ``compute_joint_jacobians``, plus the reference model's topology
@@ -95,6 +97,47 @@ def make_lie(out):
     np.savez_compressed(out, xi=xi.numpy(), se3_exp=T.numpy(), T_in=Tq.numpy(), se3_log=tn.se3_log(Tq).numpy(),
                         so3_exp=tn.so3_exp(xi[:, 3:]).numpy(), so3_log=tn.so3_log(Tq[:, 3:]).numpy(),
                         jr_inv=right_jacobian_inv_se3(xi).numpy())
+
+
+def make_lie_ops(out):
+    """The remaining LieOps methods and ``right_jacobian_se3``, with rotations that take each
+    branch of ``_matrix_to_quat`` (trace > 0, then m00 / m11 / m22 largest) and angles near pi."""
+    from better_robot.lie import _torch_native_backend as tn
+    from better_robot.lie.tangents import right_jacobian_se3
+
+    g = torch.Generator().manual_seed(12)
+    n = 64
+    q = torch.randn(n, 4, generator=g, dtype=D)
+    q = q / q.norm(dim=-1, keepdim=True)
+    # near-pi rotations about x, y, z (qw ~ 0, both signs) and one exactly at pi
+    for i, ax in enumerate((0, 1, 2, 0, 1, 2)):
+        q[i] = 0.0
+        q[i, ax] = 1.0
+        q[i, 3] = (1e-4 if i < 3 else -1e-4)
+        q[i] = q[i] / q[i].norm()
+    q[6] = torch.tensor([0.0, 0.0, 1.0, 0.0], dtype=D)
+    q[7] = torch.tensor([0.0, 0.0, 0.0, 1.0], dtype=D)
+    t = torch.randn(n, 3, generator=g, dtype=D)
+    A = torch.cat([t, q], -1)
+    qb = torch.randn(n, 4, generator=g, dtype=D)
+    qb = qb / qb.norm(dim=-1, keepdim=True)
+    B = torch.cat([torch.randn(n, 3, generator=g, dtype=D), qb], -1)
+    P = torch.randn(n, 3, generator=g, dtype=D)
+    scale = torch.rand(n, 1, generator=g, dtype=D) * 1.5 + 0.25
+    A_unnorm = torch.cat([t, q * scale], -1)
+    xi = torch.randn(n, 6, generator=g, dtype=D)
+    xi[:, 3:] *= torch.linspace(0.0, 3.0, n, dtype=D)[:, None] / xi[:, 3:].norm(dim=-1, keepdim=True)
+    xi[0, 3:] = 0.0
+    R = tn.so3_to_matrix(q)
+    np.savez_compressed(
+        out, A=A.numpy(), B=B.numpy(), P=P.numpy(), A_unnorm=A_unnorm.numpy(), xi=xi.numpy(),
+        se3_compose=tn.se3_compose(A, B).numpy(), se3_inverse=tn.se3_inverse(A).numpy(),
+        se3_act=tn.se3_act(A, P).numpy(), se3_adjoint=tn.se3_adjoint(A).numpy(),
+        se3_adjoint_inv=tn.se3_adjoint_inv(A).numpy(), se3_normalize=tn.se3_normalize(A_unnorm).numpy(),
+        se3_log=tn.se3_log(A).numpy(), so3_log=tn.so3_log(q).numpy(),
+        so3_compose=tn.so3_compose(q, qb).numpy(), so3_inverse=tn.so3_inverse(q).numpy(),
+        so3_act=tn.so3_act(q, P).numpy(), so3_to_matrix=R.numpy(), so3_from_matrix=tn.so3_from_matrix(R).numpy(),
+        so3_normalize=tn.so3_normalize(q * scale).numpy(), jr=right_jacobian_se3(xi).numpy())
 
 
 def make_kin(name, spec, batch, seed, base_t, out):
@@ -253,6 +296,7 @@ def main():
         sys.path.insert(0, src)
     torch.set_default_dtype(D)
     make_lie(os.path.join(HERE, "lie.npz"))
+    make_lie_ops(os.path.join(HERE, "lie_ops.npz"))
     chain, hum, dual = syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()
     make_kin("chain7", chain, 16, 5, 0.0, os.path.join(HERE, "kin_chain7.npz"))
     make_kin("humanoid", hum, 8, 6, 1.0, os.path.join(HERE, "kin_humanoid.npz"))

@@ -112,3 +112,20 @@ def test_trajopt_matches_reference_solve_trajopt():
     np.testing.assert_allclose(out.X, g["X"], atol=1e-8, rtol=0)
     r, _ = ot.residual_jacobian(m, out.X, fid, g["goal"], g["start"], X0, s, want_jac=False)
     np.testing.assert_allclose(r, g["residual"], atol=1e-9, rtol=0)
+
+
+def test_lie_ops_match_reference():
+    """Every LieOps method and ``right_jacobian_se3`` (incl. rotations near pi and all Shepperd branches)."""
+    g = _load("lie_ops.npz")
+    A, B, P = g["A"], g["B"], g["P"]
+    q, qb = A[:, 3:], B[:, 3:]
+    checks = {
+        "se3_compose": lie.se3_compose(A, B), "se3_inverse": lie.se3_inverse(A), "se3_act": lie.se3_act(A, P),
+        "se3_adjoint": lie.se3_adjoint(A), "se3_adjoint_inv": lie.se3_adjoint_inv(A),
+        "se3_normalize": lie.se3_normalize(g["A_unnorm"]), "se3_log": lie.se3_log(A), "so3_log": lie.so3_log(q),
+        "so3_compose": lie.quat_mul(q, qb), "so3_inverse": lie.so3_inverse(q), "so3_act": lie.so3_act(q, P),
+        "so3_to_matrix": lie.quat_to_matrix(q), "so3_from_matrix": lie.so3_from_matrix(g["so3_to_matrix"]),
+        "so3_normalize": lie.so3_normalize(g["A_unnorm"][:, 3:]), "jr": lie.right_jacobian_se3(g["xi"]),
+    }
+    for k, v in checks.items():
+        np.testing.assert_allclose(v, g[k], atol=1e-12, rtol=0, err_msg=k)
