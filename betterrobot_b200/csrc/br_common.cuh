@@ -31,6 +31,15 @@ __device__ __forceinline__ void bulk_wait_read_all() {
 // Wait until every committed bulk group has completed (writes performed).
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
+// ---- cp.async (16-byte global -> shared copies that do not pass through registers) ----
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(s), "l"(gsrc) : "memory");
+}
+// Wait for every cp.async this thread issued (the data is then visible to this thread;
+// other threads see it after a barrier).
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Warp-cooperative copy of `n` floats from shared to global (fallback when the
 // destination block is not 16-byte aligned or its size is not a multiple of 16).
 __device__ __forceinline__ void warp_copy(float* __restrict__ g, const float* __restrict__ s, int n, int lane) {

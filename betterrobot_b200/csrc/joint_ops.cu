@@ -7,12 +7,14 @@
 //   revolute / prismatic  v = q1 - q0                    (revolute.py:51-53)
 //   free-flyer            v = log(q0^-1 * q1)            (free_flyer.py:53-57)
 //
-// Layout: a warp owns a tile of 32 consecutive configurations.  Slots of 1:1 joints
-// (nq = nv = 1) are processed by the whole warp walking the tile's rows as one
-// contiguous range (coalesced loads and stores); free-flyer slots are then processed
-// one configuration per lane, so the float64 exp / log runs on all 32 lanes at once
-// instead of on one lane of a warp that waits for it.  Memory bound: 4 * (nq + nv + nq)
-// bytes per configuration for integrate, 4 * (nq + nq + nv) for difference.
+// Layout: a warp owns a tile of 32 consecutive configurations.  Their rows of every
+// input are one contiguous slab, copied into the warp's shared memory with 16-byte
+// cp.async copies (all of a tile's copies in flight at once); free-flyer slots are then
+// computed one configuration per lane (the float64 exp / log runs on 32 lanes at once),
+// and the output slab is written with float4 stores, each lane producing 4 consecutive
+// outputs.  Memory bound: 4 * (nq + nv + nq) bytes per configuration for integrate,
+// 4 * (nq + nq + nv) for difference.  Pointers that are not 16-byte aligned take the
+// same path with 4-byte loads and stores (kVec = false).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -30,78 +32,126 @@ struct JointOpParams {
   int32_t diff;     // 0 integrate, 1 difference
 };
 
+constexpr int kJointOpsWarps = 4;
+
+// Floats of shared memory one warp stages per tile.
+__host__ __device__ inline int joint_ops_warp_floats(int nq, int nv, bool diff) {
+  return 32 * (diff ? 2 * nq + nv : nq + nv);
+}
+
 __device__ __forceinline__ DPose dpose7(const float* p) {
   return DPose{d3(p[0], p[1], p[2]), make_double4(p[3], p[4], p[5], p[6])};
 }
 
-__global__ void __launch_bounds__(256) joint_ops_kernel(const br_tree_t tree, const int32_t* __restrict__ active,
-                                                        const JointOpParams p) {
+template <bool kVec>
+__device__ __forceinline__ void slab_in(float* s, const float* __restrict__ g, int n, int lane) {
+  int done = 0;
+  if (kVec) {
+    const int n4 = n >> 2;
+    for (int i = lane; i < n4; i += 32) cp_async16(s + 4 * i, g + 4 * i);
+    done = n4 << 2;
+  }
+  for (int i = done + lane; i < n; i += 32) s[i] = g[i];
+}
+
+template <bool kVec>
+__global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br_tree_t tree,
+                                                                        const int32_t* __restrict__ active,
+                                                                        const JointOpParams p) {
+  extern __shared__ __align__(16) float slabs[];
   __shared__ int16_t vmap[BR_MAX_NQ];     // q slot -> v slot of a 1:1 joint, -1 for other slots
+  __shared__ int16_t qmap[BR_MAX_NV];     // v slot -> q slot of a 1:1 joint, -1 for other slots
   __shared__ int16_t ffq[BR_MAX_JOINTS];  // free-flyer q / v offsets
   __shared__ int16_t ffv[BR_MAX_JOINTS];
   __shared__ int nff;
   const int nq = tree.nq, nv = tree.nv;
   for (int k = threadIdx.x; k < nq; k += blockDim.x) vmap[k] = -1;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) qmap[k] = -1;
   if (threadIdx.x == 0) nff = 0;
   __syncthreads();
   for (int i = threadIdx.x; i < p.n_active; i += blockDim.x) {
     const int j = active[i];
+    const int iq = tree.idx_q[j], iv = tree.idx_v[j];
     if (tree.jtype[j] == BR_JOINT_FREE_FLYER) {
       const int s = atomicAdd(&nff, 1);
-      ffq[s] = (int16_t)tree.idx_q[j];
-      ffv[s] = (int16_t)tree.idx_v[j];
+      ffq[s] = (int16_t)iq;
+      ffv[s] = (int16_t)iv;
     } else {
-      vmap[tree.idx_q[j]] = (int16_t)tree.idx_v[j];
+      vmap[iq] = (int16_t)iv;
+      qmap[iv] = (int16_t)iq;
     }
   }
   __syncthreads();
+  const bool diff = p.diff != 0;
   const int lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
+  const int lb = diff ? nq : nv;  // floats per configuration of b
+  const int lo = diff ? nv : nq;  // floats per configuration of out
+  float* A = slabs + (size_t)(threadIdx.x >> 5) * joint_ops_warp_floats(nq, nv, diff);
+  float* Bs = A + 32 * nq;
+  float* O = Bs + 32 * lb;        // difference: free-flyer outputs, v-shaped
   const int64_t tiles = (p.batch + 31) >> 5;
   const int n_ff = nff;
   for (int64_t tile = (int64_t)blockIdx.x * warps + (threadIdx.x >> 5); tile < tiles;
        tile += (int64_t)gridDim.x * warps) {
     const int64_t b0 = tile << 5;
     const int cnt = p.batch - b0 < 32 ? (int)(p.batch - b0) : 32;
-    const int span = cnt * nq;
-    const float* a = p.a + b0 * nq;
-    if (!p.diff) {
-      const float* v = p.b + b0 * nv;
-      float* o = p.out + b0 * nq;
-      for (int e = lane; e < span; e += 32) {
-        const int c = e / nq, k = e - c * nq, kv = vmap[k];
-        if (kv >= 0) o[e] = a[e] + v[c * nv + kv];
-      }
-    } else {
-      const float* q1 = p.b + b0 * nq;
-      float* o = p.out + b0 * nv;
-      for (int e = lane; e < span; e += 32) {
-        const int c = e / nq, k = e - c * nq, kv = vmap[k];
-        if (kv >= 0) o[c * nv + kv] = q1[e] - a[e];
-      }
-    }
-    if (lane < cnt && n_ff) {
-      const int64_t bi = b0 + lane;
+    slab_in<kVec>(A, p.a + b0 * nq, cnt * nq, lane);
+    slab_in<kVec>(Bs, p.b + b0 * lb, cnt * lb, lane);
+    if (kVec) cp_async_wait_all();
+    __syncwarp();
+    if (lane < cnt) {
       for (int f = 0; f < n_ff; ++f) {
         const int iq = ffq[f], iv = ffv[f];
-        const float* qa = p.a + bi * nq + iq;
-        if (!p.diff) {
-          const float* v = p.b + bi * nv + iv;
-          float* o = p.out + bi * nq + iq;
+        float* qa = A + lane * nq + iq;
+        if (!diff) {
+          const float* v = Bs + lane * nv + iv;
           DPose n = dcompose(dpose7(qa), dse3_exp(d3(v[0], v[1], v[2]), d3(v[3], v[4], v[5])));
           n.q = dqnormalize(n.q);
-          o[0] = (float)n.t.x; o[1] = (float)n.t.y; o[2] = (float)n.t.z;
-          o[3] = (float)n.q.x; o[4] = (float)n.q.y; o[5] = (float)n.q.z; o[6] = (float)n.q.w;
+          qa[0] = (float)n.t.x; qa[1] = (float)n.t.y; qa[2] = (float)n.t.z;
+          qa[3] = (float)n.q.x; qa[4] = (float)n.q.y; qa[5] = (float)n.q.z; qa[6] = (float)n.q.w;
         } else {
-          const float* qb = p.b + bi * nq + iq;
-          float* o = p.out + bi * nv + iv;
           double3 v, w;
-          dse3_log(dcompose(dinverse(dpose7(qa)), dpose7(qb)), v, w);
+          dse3_log(dcompose(dinverse(dpose7(qa)), dpose7(Bs + lane * nq + iq)), v, w);
+          float* o = O + lane * nv + iv;
           o[0] = (float)v.x; o[1] = (float)v.y; o[2] = (float)v.z;
           o[3] = (float)w.x; o[4] = (float)w.y; o[5] = (float)w.z;
         }
       }
     }
+    __syncwarp();
+    // out[e] for the tile's slab: 1:1 slots from the staged inputs, free-flyer slots from above
+    float* go = p.out + b0 * lo;
+    const int n = cnt * lo;
+    auto val = [&](int c, int k) -> float {
+      if (!diff) {
+        const int kv = vmap[k];
+        const float x = A[c * nq + k];
+        return kv >= 0 ? x + Bs[c * nv + kv] : x;
+      }
+      const int kq = qmap[k];
+      return kq >= 0 ? Bs[c * nq + kq] - A[c * nq + kq] : O[c * nv + k];
+    };
+    int done = 0;
+    if (kVec) {
+      const int n4 = n >> 2;
+      for (int i = lane; i < n4; i += 32) {
+        int c = (4 * i) / lo, k = 4 * i - c * lo;
+        float r[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          r[u] = val(c, k);
+          if (++k == lo) { k = 0; ++c; }
+        }
+        reinterpret_cast<float4*>(go)[i] = make_float4(r[0], r[1], r[2], r[3]);
+      }
+      done = n4 << 2;
+    }
+    for (int e = done + lane; e < n; e += 32) {
+      const int c = e / lo;
+      go[e] = val(c, e - c * lo);
+    }
+    __syncwarp();  // the next tile overwrites the slabs
   }
 }
 
@@ -120,11 +170,24 @@ extern "C" int br_configuration_op(const br_tree_t* tree, const int32_t* active_
   if (!aligned4(a) || !aligned4(b) || !aligned4(out)) return BR_EALIGN;
   JointOpParams p = {a, b, out, batch, n_active, op == BR_OP_DIFFERENCE};
   const DeviceInfo& d = device_info();
-  const int threads = 256;
+  const bool vec = aligned16(a) && aligned16(b) && aligned16(out);
+  const size_t bytes = (size_t)kJointOpsWarps * joint_ops_warp_floats(tree->nq, tree->nv, p.diff) * sizeof(float);
+  if ((int64_t)bytes > d.max_smem_optin) return BR_ETOOBIG;
+  auto kern = vec ? joint_ops_kernel<true> : joint_ops_kernel<false>;
+  static size_t configured[2][16] = {};
+  size_t& have = configured[vec][d.device & 15];
+  if (bytes > have) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return (int)e;
+    have = bytes;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kJointOpsWarps, bytes);
+  if (per_sm < 1) per_sm = 1;
   const int64_t tiles = (batch + 31) / 32;
-  int64_t blocks = (tiles + threads / 32 - 1) / (threads / 32);
-  const int64_t cap = (int64_t)d.sms * 8;  // 8 CTAs of 256 threads per SM, then grid-stride
+  int64_t blocks = (tiles + kJointOpsWarps - 1) / kJointOpsWarps;
+  const int64_t cap = (int64_t)per_sm * d.sms;  // persistent: one wave, then grid-stride over tiles
   if (blocks > cap) blocks = cap;
-  joint_ops_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(*tree, active_joints, p);
+  kern<<<(unsigned)blocks, 32 * kJointOpsWarps, bytes, (cudaStream_t)stream>>>(*tree, active_joints, p);
   return (int)cudaGetLastError();
 }

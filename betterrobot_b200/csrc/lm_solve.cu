@@ -429,8 +429,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     return sqrtf(gg);
   };
 
-  // Solve (J^T J + damp I) delta = -g in float32 with a right-looking Cholesky on the packed
-  // column-major triangle (lanes over the trailing entries).  Returns false if it failed.
+  // Solve (J^T J + damp I) delta = -g in float32 by a right-looking LDL^T on the packed
+  // column-major triangle, kept unscaled: once column j is eliminated its entries are
+  // A_ij = l_ij d_j, so the trailing update A_ik -= A_ij A_kj / d_j needs no scaled copy
+  // of column j and each column costs one team sync.  d_j > 0 for every j is the same
+  // test a Cholesky factorization applies.  The two triangular solves run in registers:
+  // lane tl owns rows i = tl + T r, and each step broadcasts one value by a shuffle.
+  // Returns false if a pivot is not positive and finite.
   auto solve = [&](float damp) -> bool {
     float* Lm = work;
     const int ntri = tri(nv);
@@ -439,45 +444,75 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       Lm[e] = jtj[e] + ((ik & 255) == (ik >> 8) ? damp : 0.f);
     }
     tm.sync();
-    bool ok = true;
     int off = 0;  // first packed entry of the columns right of j
     for (int j = 0; j < nv; ++j) {
       const int cj = coff[j];
-      const float djj = Lm[cj + j];
-      if (!(djj > 0.f) || !isfinite(djj)) { ok = false; break; }
-      const float dj = sqrtf(djj);
+      const float dj = Lm[cj + j];
+      if (!(dj > 0.f) || !isfinite(dj)) return false;  // every lane read the same pivot
       const float inv = 1.f / dj;
-      tm.sync();
-      if (tl == 0) { Lm[cj + j] = dj; dinv[j] = inv; }
-      for (int i = j + 1 + tl; i < nv; i += T) Lm[cj + i] *= inv;
-      tm.sync();
+      if (tl == 0) dinv[j] = inv;
       off += nv - j;
       for (int e = off + tl; e < ntri; e += T) {
         const int ik = trik[e];
-        Lm[e] = fmaf(-Lm[cj + (ik & 255)], Lm[cj + (ik >> 8)], Lm[e]);
+        Lm[e] = fmaf(-Lm[cj + (ik & 255)] * inv, Lm[cj + (ik >> 8)], Lm[e]);
       }
       tm.sync();
     }
-    tm.sync();
-    if (!ok) return false;
-    // forward: L y = -g  (y kept in delta[]), then back: L^T dx = y
-    for (int i = tl; i < nv; i += T) delta[i] = -g[i];
-    tm.sync();
+    constexpr int R = BR_MAX_NV / T;  // rows per lane
+    float z[R], dv[R];
+    int co[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = tl + T * r;
+      z[r] = i < nv ? -g[i] : 0.f;
+      dv[r] = i < nv ? dinv[i] : 0.f;
+      co[r] = i < nv ? coff[i] : 0;
+    }
+    // L D w = -g: at step j the owner of row j holds u_j; w_j = u_j / d_j, z_i -= A_ij w_j
     for (int j = 0; j < nv; ++j) {
-      const float yj = delta[j] * dinv[j];
-      tm.sync();
-      if (tl == 0) delta[j] = yj;
-      const int cj = coff[j];
-      for (int i = j + 1 + tl; i < nv; i += T) delta[i] = fmaf(-Lm[cj + i], yj, delta[i]);
-      tm.sync();
+      const int cj = coff[j], rj = j / T;
+      float a[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = tl + T * r;
+        a[r] = (i > j && i < nv) ? Lm[cj + i] : 0.f;
+      }
+      float zj = z[0], dj = dv[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r)
+        if (r == rj) { zj = z[r]; dj = dv[r]; }
+      const float wj = tm.bcast(zj * dj, j % T);
+      if (tl == j % T) {
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          if (r == rj) z[r] = wj;
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], wj, z[r]);
     }
+    // L^T delta = w: at step j (descending) the owner holds delta_j; z_i -= (A_ji / d_i) delta_j
     for (int j = nv - 1; j >= 0; --j) {
-      const float xj = delta[j] * dinv[j];
-      tm.sync();
-      if (tl == 0) delta[j] = xj;
-      for (int i = tl; i < j; i += T) delta[i] = fmaf(-Lm[coff[i] + j], xj, delta[i]);
-      tm.sync();
+      const int rj = j / T;
+      float a[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = tl + T * r;
+        a[r] = i < j ? Lm[co[r] + j] * dv[r] : 0.f;
+      }
+      float zj = z[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r)
+        if (r == rj) zj = z[r];
+      const float xj = tm.bcast(zj, j % T);
+#pragma unroll
+      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], xj, z[r]);
     }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = tl + T * r;
+      if (i < nv) delta[i] = z[r];
+    }
+    tm.sync();
     return true;
   };
 

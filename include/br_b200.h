@@ -125,7 +125,7 @@ BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joi
 #define BR_IK_CONVERGED 0       /* status & 0xff                                   */
 #define BR_IK_MAXITER 1
 #define BR_IK_FLAG_NONFINITE 1  /* (status >> 8) bits: a non-finite cost was seen   */
-#define BR_IK_FLAG_REGULARIZED 2 /* float32 Cholesky needed extra diagonal damping */
+#define BR_IK_FLAG_REGULARIZED 2 /* float32 LDL^T needed extra diagonal damping     */
 
 /* Solver settings: LevenbergMarquardt(lam0, factor, tol) with Adaptive damping
  * bounds [lam_min, lam_max] (optim/strategies/adaptive.py:19-25), GaussNewton eps,

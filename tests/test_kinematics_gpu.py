@@ -193,3 +193,27 @@ def test_integrate_difference_large_batch_round_trip():
     idx = np.random.default_rng(13).choice(B, 256, replace=False)
     ref = K.difference(m64, q[idx].double().cpu().numpy(), q1[idx].double().cpu().numpy())
     np.testing.assert_allclose(dv[idx].cpu().double().numpy(), ref, atol=2e-6, rtol=0)
+
+
+def test_integrate_difference_unaligned_pointers_match():
+    """Inputs / outputs that start 4 bytes past a 16-byte boundary take the 4-byte load path: same results."""
+    from betterrobot_b200.configuration import difference_into, integrate_into
+    m = syn.model_from_spec(SPECS["humanoid"])
+    m64 = syn.model_from_spec(SPECS["humanoid"], dtype=torch.float64)
+    B = 1000
+    q = syn.random_q(m64, B, 21, rev_range=2.5, base_translation=1.0).float().cuda()
+    q1 = syn.noisy_start(m64, q.double().cpu(), 0.3, 22).float().cuda()
+    v = torch.randn(B, m.nv, device="cuda", generator=torch.Generator("cuda").manual_seed(23)) * 0.3
+
+    def shifted(t):
+        buf = torch.empty(t.numel() + 1, device="cuda")[1:].view(t.shape)
+        buf.copy_(t)
+        assert buf.data_ptr() % 16 != 0
+        return buf
+    ref_q, ref_v = torch.empty_like(q), torch.empty_like(v)
+    integrate_into(m, q, v, ref_q)
+    difference_into(m, q, q1, ref_v)
+    out_q, out_v = shifted(torch.zeros_like(q)), shifted(torch.zeros_like(v))
+    integrate_into(m, shifted(q), shifted(v), out_q)
+    difference_into(m, shifted(q), shifted(q1), out_v)
+    assert torch.equal(out_q, ref_q) and torch.equal(out_v, ref_v)
