@@ -54,7 +54,8 @@ struct LmParams {
 struct TeamLayout {
   int parent, jtype, idxq, idxv, support, cjoint, ckind, caxis, lower, upper;
   int fparent, fplace, tgt;
-  int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc, trik, coff,
+  int dpar, ddep, rowoff, amask, ancd;
+  int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc,
       dinv, sup, nsup;
   int total;
   __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T) {
@@ -78,8 +79,11 @@ struct TeamLayout {
     jtj = take(ntri);                          // J^T J, packed lower triangle, column-major
     work = take(6 * nv > ntri ? 6 * nv : ntri);  // one target's J columns (build) / packed L (solve)
     misc = take(8);
-    trik = take((ntri + 1) / 2);               // uint16 (row i | column k << 8) of packed entry e (column-major)
-    coff = take(nv);                           // packed index of (i, k) = coff[k] + i
+    amask = take(2 * nv);                      // uint64 strict ancestors of each DOF
+    dpar = take((nv + 3) / 4);                 // int8 parent DOF (-1 at a root)
+    ddep = take((nv + 3) / 4);                 // uint8 DOF depth
+    rowoff = take((nv + 2) / 2);               // uint16 first entry of each row, nv + 1 values
+    ancd = take((nv * nv + 3) / 4);            // uint8 ancestor of DOF c at depth a: ancd[c * nv + a]
     dinv = take(nv);                           // 1 / L_jj
     sup = take((K * nv + 3) / 4);              // uint8 support columns of each target, ascending
     nsup = take(K);
@@ -88,6 +92,10 @@ struct TeamLayout {
 };
 
 __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
+
+// DOFs one lane owns in the register triangular solves: a team of T lanes takes at most
+// lm_rows(T) * T DOFs (8 lanes: nv <= 16; 16 or 32 lanes: nv <= 64).
+__host__ __device__ constexpr int lm_rows(int T) { return T == 8 ? 2 : T == 16 ? 4 : 2; }
 
 template <int T>
 struct Team {
@@ -183,8 +191,11 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   float* delta = sm + L.delta;
   float* jtj = sm + L.jtj;
   float* work = sm + L.work;
-  unsigned short* trik = reinterpret_cast<unsigned short*>(sm + L.trik);
-  int* coff = reinterpret_cast<int*>(sm + L.coff);
+  unsigned long long* amask = reinterpret_cast<unsigned long long*>(sm + L.amask);
+  signed char* dpar = reinterpret_cast<signed char*>(sm + L.dpar);
+  unsigned char* ddep = reinterpret_cast<unsigned char*>(sm + L.ddep);
+  unsigned short* rowoff = reinterpret_cast<unsigned short*>(sm + L.rowoff);
+  unsigned char* ancd = reinterpret_cast<unsigned char*>(sm + L.ancd);
   float* dinv = sm + L.dinv;
   unsigned char* sup = reinterpret_cast<unsigned char*>(sm + L.sup);
   int* nsup = reinterpret_cast<int*>(sm + L.nsup);
@@ -224,14 +235,39 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       std8(tgt + 8 * t, DPose{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])});
     }
   }
-  // (i, k) of every packed lower-triangle entry, column-major: column k holds rows
-  // k..nv-1 and starts at k*nv - k(k-1)/2
-  for (int k = tl; k < nv; k += T) {
-    const int off = k * nv - k * (k - 1) / 2;
-    coff[k] = off - k;
-    for (int i = k; i < nv; ++i) trik[off + i - k] = (unsigned short)(i | (k << 8));
+  // ---- the DOF tree of J^T J -----------------------------------------------
+  // DOF c's parent is the previous DOF of its own joint (a free-flyer's 6 DOFs form a
+  // chain) or the last DOF of the nearest ancestor joint that has DOFs.  The residuals
+  // couple a DOF only with its ancestors (a pose target's support is a root-to-frame
+  // path; limit, rest and damping terms are diagonal), so J^T J is stored as one row per
+  // DOF over its ancestors and itself, entry (i, j) at rowoff[i] + ddep[j], and factors
+  // leaves first with no fill-in.  DOF numbering is topological (dpar[c] < c), so a
+  // DOF's ancestors have smaller indices.  One lane builds the tables once per problem.
+  if (tl == 0) {
+    int* lastd = reinterpret_cast<int*>(poseA);  // scratch: last DOF on each joint's path
+    for (int j = 0; j < nj; ++j) {
+      const int pj = parent[j];
+      const int prev = pj >= 0 ? lastd[pj] : -1;
+      const int jt = jtype[j];
+      const int nvj = jt == BR_JOINT_FREE_FLYER ? 6 : (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) ? 1 : 0;
+      for (int k = 0; k < nvj; ++k) dpar[idxv[j] + k] = (signed char)(k == 0 ? prev : idxv[j] + k - 1);
+      lastd[j] = nvj ? idxv[j] + nvj - 1 : prev;
+    }
+    int nl = 0;
+    for (int c = 0; c < nv; ++c) {
+      const int pc = dpar[c];
+      const int dc = pc < 0 ? 0 : ddep[pc] + 1;
+      ddep[c] = (unsigned char)dc;
+      amask[c] = pc < 0 ? 0ull : (amask[pc] | (1ull << pc));
+      for (int a = 0; a + 1 < dc; ++a) ancd[c * nv + a] = ancd[pc * nv + a];
+      if (pc >= 0) ancd[c * nv + dc - 1] = (unsigned char)pc;
+      rowoff[c] = (unsigned short)nl;
+      nl += dc + 1;
+    }
+    rowoff[nv] = (unsigned short)nl;
   }
   tm.sync();
+  const int nL = rowoff[nv];
   // ascending list of the tangent columns that move each target frame (its support)
   for (int t = 0; t < nt; ++t) {
     const unsigned long long sp = support[fparent[t]];
@@ -339,7 +375,6 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // Each target's pose Jacobian diag(w) Jr^-1 blockdiag(R^T, R^T) J_lwa (pose.py:68-103) is
   // built only on its support columns and accumulated into the (support x support) block.
   auto build_normal = [&](const double* q, const double* pose) -> float {
-    const int ntri = tri(nv);
     for (int c = tl; c < nv; c += T) {
       const Pose Tj = to_f(lds(pose, nj, cjoint[c]));
       const float3 a = qrot(Tj.q, f3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
@@ -354,7 +389,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
       for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
     }
-    for (int e = tl; e < ntri; e += T) jtj[e] = 0.f;
+    for (int e = tl; e < nL; e += T) jtj[e] = 0.f;
     tm.sync();
     float* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
     for (int t = 0; t < nt; ++t) {
@@ -394,7 +429,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         float acc = 0.f;
 #pragma unroll
         for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], Jc[r * nv + v], acc);
-        jtj[coff[st[v]] + st[u]] += acc;
+        jtj[rowoff[st[u]] + ddep[st[v]]] += acc;  // st ascending: st[u] descends from st[v]
       }
       const double* e = xi + 8 * t;
       const float rw[6] = {wp * (float)e[0], wp * (float)e[1], wp * (float)e[2],
@@ -420,7 +455,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           if (q[iq] > (double)upper[iq]) { dg += wl * wl; gc += wl * wl * (float)(q[iq] - (double)upper[iq]); }
         }
       }
-      jtj[coff[c] + c] += dg;
+      jtj[rowoff[c] + ddep[c]] += dg;
       g[c] = gc;
       gg += gc * gc;
     }
@@ -429,83 +464,83 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     return sqrtf(gg);
   };
 
-  // Solve (J^T J + damp I) delta = -g in float32 by a right-looking LDL^T on the packed
-  // column-major triangle, kept unscaled: once column j is eliminated its entries are
-  // A_ij = l_ij d_j, so the trailing update A_ik -= A_ij A_kj / d_j needs no scaled copy
-  // of column j and each column costs one team sync.  d_j > 0 for every j is the same
-  // test a Cholesky factorization applies.  The two triangular solves run in registers:
-  // lane tl owns rows i = tl + T r, and each step broadcasts one value by a shuffle.
-  // Returns false if a pivot is not positive and finite.
+  // Solve (J^T J + damp I) delta = -g in float32 by an LDL^T factorization that eliminates
+  // the DOF tree leaves first (Featherstone's LTL order: no fill-in).  Eliminating DOF k
+  // updates only pairs of its ancestors, A_ij -= A_ki A_kj / d_k, lanes over those pairs,
+  // one team sync per DOF; entries stay unscaled (A_ki = l_ik d_k) and the damping is
+  // added to each pivot as it is read.  d_k > 0 for every k is the test a Cholesky
+  // factorization applies.  The triangular solves run in registers (lane tl owns DOFs
+  // tl + T r), one shuffle per step.  Returns false if a pivot is not positive and finite.
   auto solve = [&](float damp) -> bool {
     float* Lm = work;
-    const int ntri = tri(nv);
-    for (int e = tl; e < ntri; e += T) {
-      const int ik = trik[e];
-      Lm[e] = jtj[e] + ((ik & 255) == (ik >> 8) ? damp : 0.f);
-    }
+    for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
     tm.sync();
-    int off = 0;  // first packed entry of the columns right of j
-    for (int j = 0; j < nv; ++j) {
-      const int cj = coff[j];
-      const float dj = Lm[cj + j];
-      if (!(dj > 0.f) || !isfinite(dj)) return false;  // every lane read the same pivot
-      const float inv = 1.f / dj;
-      if (tl == 0) dinv[j] = inv;
-      off += nv - j;
-      for (int e = off + tl; e < ntri; e += T) {
-        const int ik = trik[e];
-        Lm[e] = fmaf(-Lm[cj + (ik & 255)] * inv, Lm[cj + (ik >> 8)], Lm[e]);
+    for (int k = nv - 1; k >= 0; --k) {
+      const int dk = ddep[k], rk = rowoff[k];
+      const float piv = Lm[rk + dk] + damp;
+      if (!(piv > 0.f) || !isfinite(piv)) return false;  // every lane read the same pivot
+      const float inv = 1.f / piv;
+      if (tl == 0) dinv[k] = inv;
+      const unsigned char* anc = ancd + k * nv;
+      for (int p = tl; p < tri(dk); p += T) {                // pairs (a, b), b <= a < dk, by depth
+        int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+        if (tri(a + 1) <= p) ++a;
+        if (tri(a) > p) --a;
+        const int b = p - tri(a);
+        float* dst = Lm + rowoff[anc[a]] + b;
+        *dst = fmaf(-Lm[rk + a] * inv, Lm[rk + b], *dst);
       }
       tm.sync();
     }
-    constexpr int R = BR_MAX_NV / T;  // rows per lane
+    constexpr int R = lm_rows(T);  // DOFs per lane
     float z[R], dv[R];
-    int co[R];
+    int rd[R];  // rowoff | ddep << 16 of the lane's DOFs
+    unsigned long long am[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = tl + T * r;
-      z[r] = i < nv ? -g[i] : 0.f;
-      dv[r] = i < nv ? dinv[i] : 0.f;
-      co[r] = i < nv ? coff[i] : 0;
+      const bool in = i < nv;
+      z[r] = in ? -g[i] : 0.f;
+      dv[r] = in ? dinv[i] : 0.f;
+      rd[r] = in ? (rowoff[i] | (ddep[i] << 16)) : 0;
+      am[r] = in ? amask[i] : 0ull;
     }
-    // L D w = -g: at step j the owner of row j holds u_j; w_j = u_j / d_j, z_i -= A_ij w_j
-    for (int j = 0; j < nv; ++j) {
-      const int cj = coff[j], rj = j / T;
+    // leaves first: w_k = u_k / d_k, then u_i -= A_ki w_k for the ancestors i of k
+    for (int k = nv - 1; k >= 0; --k) {
+      const int rk = k / T, own = k % T, rowk = rowoff[k];
+      const unsigned long long mk = amask[k];
       float a[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int i = tl + T * r;
-        a[r] = (i > j && i < nv) ? Lm[cj + i] : 0.f;
+        a[r] = (i < nv && ((mk >> i) & 1ull)) ? Lm[rowk + (rd[r] >> 16)] : 0.f;
       }
-      float zj = z[0], dj = dv[0];
+      float zk = z[0], dk = dv[0];
 #pragma unroll
       for (int r = 1; r < R; ++r)
-        if (r == rj) { zj = z[r]; dj = dv[r]; }
-      const float wj = tm.bcast(zj * dj, j % T);
-      if (tl == j % T) {
+        if (r == rk) { zk = z[r]; dk = dv[r]; }
+      const float wk = tm.bcast(zk * dk, own);
+      if (tl == own) {
 #pragma unroll
         for (int r = 0; r < R; ++r)
-          if (r == rj) z[r] = wj;
+          if (r == rk) z[r] = wk;
       }
 #pragma unroll
-      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], wj, z[r]);
+      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], wk, z[r]);
     }
-    // L^T delta = w: at step j (descending) the owner holds delta_j; z_i -= (A_ji / d_i) delta_j
-    for (int j = nv - 1; j >= 0; --j) {
-      const int rj = j / T;
+    // ancestors first: delta_i is final, then w_m -= (A_mi / d_m) delta_i for the descendants m of i
+    for (int i = 0; i < nv; ++i) {
+      const int ri = i / T, di = ddep[i];
       float a[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int i = tl + T * r;
-        a[r] = i < j ? Lm[co[r] + j] * dv[r] : 0.f;
-      }
-      float zj = z[0];
+      for (int r = 0; r < R; ++r) a[r] = ((am[r] >> i) & 1ull) ? Lm[(rd[r] & 0xffff) + di] * dv[r] : 0.f;
+      float zi = z[0];
 #pragma unroll
       for (int r = 1; r < R; ++r)
-        if (r == rj) zj = z[r];
-      const float xj = tm.bcast(zj, j % T);
+        if (r == ri) zi = z[r];
+      const float xv = tm.bcast(zi, i % T);
 #pragma unroll
-      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], xj, z[r]);
+      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], xv, z[r]);
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -682,6 +717,7 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     if (st) return st;
     const int T = b.team_size[c];
     if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
+    if (b.trees[c].nv > lm_rows(T) * T) return BR_EINVAL;  // 8-lane teams take nv <= 16
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;
@@ -787,6 +823,7 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     if (st) return st;
     const int T = b.team_size[c];
     if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
+    if (b.trees[c].nv > lm_rows(T) * T) return BR_EINVAL;  // 8-lane teams take nv <= 16
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;

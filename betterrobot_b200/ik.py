@@ -158,6 +158,9 @@ class PackedIK:
         if self.K > MAX_TARGETS:
             raise ShapeError(f"at most {MAX_TARGETS} targets per problem")
         self.team = [int(t) for t in (team_sizes or [default_team_size(m) for m in models])]
+        for m, t in zip(models, self.team):
+            if t not in (8, 16, 32) or (t == 8 and int(m.nv) > 16):
+                raise ShapeError(f"team size {t} for nv={m.nv}: use 8 (nv <= 16), 16 or 32 lanes")
         self.trees = [device_tree(m, self.device) for m in models]
         self.warps_per_cta = warps_per_cta
         # per-problem layout: classes contiguous, in class order
