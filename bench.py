@@ -573,9 +573,11 @@ def main():
         steps = []
         cb = None
         cores = len(os.sched_getaffinity(0))
+        n = max(cores, 10)  # at least one problem per host core, in the mix's proportions
+        per_class = (round(0.3 * n), round(0.3 * n), n - 2 * round(0.3 * n))  # humanoid, dual_arm, chain7
         with mp.get_context("spawn").Pool(cores) as pool:
             for i in range(warmup + args.steps):
-                cb = cpu_baseline(seed=7, per_class=(4, 3, 3), cores=cores, pool=pool)
+                cb = cpu_baseline(seed=7, per_class=per_class, cores=cores, pool=pool)
                 if i >= warmup:
                     steps.append(cb)
         v = float(np.mean([s["value"] for s in steps]))

@@ -39,7 +39,8 @@ class IKSettings(ctypes.Structure):
                 ("lam_min", ctypes.c_float), ("lam_max", ctypes.c_float), ("gn_eps", ctypes.c_float),
                 ("pos_weight", ctypes.c_float), ("ori_weight", ctypes.c_float),
                 ("limit_weight", ctypes.c_float), ("rest_weight", ctypes.c_float),
-                ("max_iter", c_int32), ("optimizer", c_int32)]
+                ("max_iter", c_int32), ("optimizer", c_int32), ("kernel", c_int32),
+                ("kernel_param", ctypes.c_float)]
 
 
 class IKBatch(ctypes.Structure):

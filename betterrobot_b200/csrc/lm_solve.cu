@@ -93,6 +93,21 @@ struct TeamLayout {
 
 __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
 
+// IRLS weight w(s) of one squared residual row s (optim/kernels/{huber,cauchy,tukey}.py:
+// weight; applied as in levenberg_marquardt.py:27-44, whose sqrt(w) scales both the row
+// and its Jacobian row, so J^T J and J^T r pick up w).  Evaluated in float64.
+__device__ __forceinline__ float irls_weight(int kernel, double c, double s) {
+  switch (kernel) {
+    case BR_KERNEL_HUBER: return s <= c * c ? 1.f : (float)(c / sqrt(fmax(s, 0.0) + 1e-30));
+    case BR_KERNEL_CAUCHY: return (float)(1.0 / (1.0 + s / (c * c)));
+    case BR_KERNEL_TUKEY: {
+      const double u = fmax(1.0 - s / (c * c), 0.0);
+      return (float)(u * u);
+    }
+    default: return 1.f;
+  }
+}
+
 // DOFs one lane owns in the register triangular solves: a team of T lanes takes at most
 // lm_rows(T) * T DOFs (8 lanes: nv <= 16; 16 or 32 lanes: nv <= 64).
 __host__ __device__ constexpr int lm_rows(int T) { return T == 8 ? 2 : T == 16 ? 4 : 2; }
@@ -203,6 +218,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const br_ik_settings_t& S = P.s;
   const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
   const double wpd = wp, wod = wo, wld = wl, wrd = wr;
+  const double kc = S.kernel_param;
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
 
   // ---- load the tree table and the problem -------------------------------
@@ -421,6 +437,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
       }
       tm.sync();
+      const double* e = xi + 8 * t;
+      float kw[6];  // IRLS weight of each of the target's 6 stacked rows (1 for the l2 kernel)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        const double rr = (r < 3 ? wpd : wod) * e[r];
+        kw[r] = irls_weight(S.kernel, kc, rr * rr);
+      }
       for (int p = tl; p < tri(ns); p += T) {
         int u = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);   // row-major (u >= v) decode of p
         if (tri(u + 1) <= p) ++u;
@@ -428,12 +451,11 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         const int v = p - tri(u);
         float acc = 0.f;
 #pragma unroll
-        for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], Jc[r * nv + v], acc);
+        for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u] * kw[r], Jc[r * nv + v], acc);
         jtj[rowoff[st[u]] + ddep[st[v]]] += acc;  // st ascending: st[u] descends from st[v]
       }
-      const double* e = xi + 8 * t;
-      const float rw[6] = {wp * (float)e[0], wp * (float)e[1], wp * (float)e[2],
-                           wo * (float)e[3], wo * (float)e[4], wo * (float)e[5]};
+      const float rw[6] = {wp * (float)e[0] * kw[0], wp * (float)e[1] * kw[1], wp * (float)e[2] * kw[2],
+                           wo * (float)e[3] * kw[3], wo * (float)e[4] * kw[4], wo * (float)e[5] * kw[5]};
       for (int u = tl; u < ns; u += T) {
         float acc = 0.f;
 #pragma unroll
@@ -446,13 +468,28 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     float gg = 0.f;
     for (int c = tl; c < nv; c += T) {
       float dg = 0.f, gc = g[c];
-      if (use_rest) { dg += wr * wr; gc += wr * wr * (float)dr[c]; }
+      if (use_rest) {
+        const double rr = wrd * dr[c];
+        const float w = irls_weight(S.kernel, kc, rr * rr);
+        dg += wr * wr * w;
+        gc += wr * wr * w * (float)dr[c];
+      }
       if (use_limits) {
         const int j = cjoint[c];
         if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
           const int iq = idxq[j];
-          if (q[iq] < (double)lower[iq]) { dg += wl * wl; gc -= wl * wl * (float)((double)lower[iq] - q[iq]); }
-          if (q[iq] > (double)upper[iq]) { dg += wl * wl; gc += wl * wl * (float)(q[iq] - (double)upper[iq]); }
+          if (q[iq] < (double)lower[iq]) {
+            const double d = (double)lower[iq] - q[iq];
+            const float w = irls_weight(S.kernel, kc, wld * wld * d * d);
+            dg += wl * wl * w;
+            gc -= wl * wl * w * (float)d;
+          }
+          if (q[iq] > (double)upper[iq]) {
+            const double d = q[iq] - (double)upper[iq];
+            const float w = irls_weight(S.kernel, kc, wld * wld * d * d);
+            dg += wl * wl * w;
+            gc += wl * wl * w * (float)d;
+          }
         }
       }
       jtj[rowoff[c] + ddep[c]] += dg;
@@ -706,6 +743,8 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     return BR_EINVAL;
   if (!result->x || !result->iters || !result->status || !result->cost) return BR_EINVAL;
   if (settings->max_iter < 0) return BR_EINVAL;
+  if (settings->kernel < BR_KERNEL_L2 || settings->kernel > BR_KERNEL_TUKEY) return BR_EINVAL;
+  if (settings->kernel != BR_KERNEL_L2 && !(settings->kernel_param > 0.f)) return BR_EINVAL;
   if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
   LmParams p = {};
   p.s = *settings;
@@ -809,6 +848,8 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     return BR_EINVAL;
   if (!result->x || !result->iters || !result->status || !result->cost) return BR_EINVAL;
   if (settings->max_iter < 0) return BR_EINVAL;
+  if (settings->kernel < BR_KERNEL_L2 || settings->kernel > BR_KERNEL_TUKEY) return BR_EINVAL;
+  if (settings->kernel != BR_KERNEL_L2 && !(settings->kernel_param > 0.f)) return BR_EINVAL;
   if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
   void* scratch = nullptr;
   int st = noalloc_scratch_address(&scratch);

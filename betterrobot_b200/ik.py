@@ -64,6 +64,13 @@ class OptimizerConfig:
     lam_min: float = 1e-10
     lam_max: float = 1e8
     gn_eps: float = 1e-8
+    kernel_param: float | None = None  # None: the kernel class's default (Huber 1.0, Cauchy 1.0, Tukey 4.685)
+
+
+# OptimizerConfig.kernel -> BR_KERNEL_*, and the default parameter of each kernel class
+# (src/better_robot/optim/kernels/huber.py, cauchy.py, tukey.py)
+KERNELS = {"l2": 0, "huber": 1, "cauchy": 2, "tukey": 3}
+KERNEL_DEFAULTS = {"huber": 1.0, "cauchy": 1.0, "tukey": 4.685}
 
 
 @dataclass
@@ -104,8 +111,6 @@ def settings_from(cost_cfg: IKCostConfig, opt: OptimizerConfig) -> IKSettings:
         raise NotImplementedError(f"optimizer {opt.optimizer!r}: the sm_100a path runs 'lm' and 'gn'")
     if opt.linear_solver != "cholesky":
         raise NotImplementedError("the sm_100a path solves the normal equations by Cholesky")
-    if opt.kernel != "l2":
-        raise NotImplementedError("robust kernels are not on the sm_100a path (l2 only)")
     if opt.damping not in ("adaptive", "constant"):
         raise NotImplementedError(f"damping {opt.damping!r} is not on the sm_100a path")
     s = IKSettings()
@@ -119,6 +124,10 @@ def settings_from(cost_cfg: IKCostConfig, opt: OptimizerConfig) -> IKSettings:
     s.rest_weight = cost_cfg.rest_weight
     s.max_iter = int(opt.max_iter)
     s.optimizer = OPT_LM if opt.optimizer == "lm" else OPT_GN
+    if opt.kernel not in KERNELS:
+        raise ValueError(f"Unknown kernel {opt.kernel!r}; expected one of {sorted(KERNELS)}")
+    s.kernel = KERNELS[opt.kernel]
+    s.kernel_param = KERNEL_DEFAULTS.get(opt.kernel, 0.0) if opt.kernel_param is None else float(opt.kernel_param)
     return s
 
 

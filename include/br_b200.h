@@ -122,6 +122,10 @@ BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joi
 #define BR_LM_SCRATCH_BYTES 16  /* device scratch br_lm_solve needs (work queue)   */
 #define BR_OPT_LM 0
 #define BR_OPT_GN 1
+#define BR_KERNEL_L2 0          /* robust kernels of OptimizerConfig.kernel (tasks/ik.py:116-133) */
+#define BR_KERNEL_HUBER 1       /* w(s) = 1 if s <= d^2 else d / sqrt(s)                          */
+#define BR_KERNEL_CAUCHY 2      /* w(s) = 1 / (1 + s / c^2)                                       */
+#define BR_KERNEL_TUKEY 3       /* w(s) = max(1 - s / c^2, 0)^2                                   */
 #define BR_IK_CONVERGED 0       /* status & 0xff                                   */
 #define BR_IK_MAXITER 1
 #define BR_IK_FLAG_NONFINITE 1  /* (status >> 8) bits: a non-finite cost was seen   */
@@ -136,6 +140,8 @@ typedef struct br_ik_settings {
     float pos_weight, ori_weight, limit_weight, rest_weight;
     int32_t max_iter;
     int32_t optimizer;          /* BR_OPT_LM or BR_OPT_GN                          */
+    int32_t kernel;             /* BR_KERNEL_*: IRLS row weights (levenberg_marquardt.py:27-44) */
+    float kernel_param;         /* Huber delta / Cauchy c / Tukey c (optim/kernels/*.py)      */
 } br_ik_settings_t;
 
 /* A packed batch of independent IK problems over up to 8 robot classes. */

@@ -40,6 +40,27 @@ class IKSettings:
     gn_eps: float = 1e-8
     lam_min: float = 1e-10         # Adaptive.accept floor, adaptive.py:19
     lam_max: float = 1e8           # Adaptive.reject cap, adaptive.py:23
+    kernel: str = "l2"             # "l2" | "huber" | "cauchy" | "tukey" (tasks/ik.py:116-133)
+    kernel_param: float | None = None  # delta (huber) or c (cauchy, tukey); None = the class default
+
+
+KERNEL_DEFAULTS = {"huber": 1.0, "cauchy": 1.0, "tukey": 4.685}  # optim/kernels/{huber,cauchy,tukey}.py
+
+
+def kernel_weight(name: str, s: np.ndarray, param: float | None = None) -> np.ndarray:
+    """IRLS weight w(s) of a squared residual row ``s`` (``optim/kernels/*.py: weight``)."""
+    if name == "l2":
+        return np.ones_like(s)
+    c = KERNEL_DEFAULTS[name] if param is None else param
+    if name == "huber":                        # huber.py: min(1, delta / sqrt(s))
+        s = np.maximum(s, 0.0)
+        return np.where(s <= c * c, 1.0, c / np.sqrt(s + 1e-30))
+    if name == "cauchy":                       # cauchy.py: 1 / (1 + s / c^2)
+        return 1.0 / (1.0 + s / (c * c))
+    if name == "tukey":                        # tukey.py: max(1 - s / c^2, 0)^2
+        u = np.maximum(1.0 - s / (c * c), 0.0)
+        return u * u
+    raise ValueError(f"unknown kernel {name!r}")
 
 
 def _np(x):
@@ -140,6 +161,10 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None) -> IKOutcom
         qa = q[idx]
         _, J = residual_and_jacobian(model, qa, frame_ids, targets[idx], q_rest, s)
         ra = r[idx]
+        if s.kernel != "l2":  # IRLS: rows scaled by sqrt(w(r_i^2)) (levenberg_marquardt.py:27-44)
+            sw = np.sqrt(np.maximum(kernel_weight(s.kernel, ra * ra, s.kernel_param), 0.0))
+            ra = ra * sw
+            J = J * sw[..., None]
         JtJ = np.swapaxes(J, -1, -2) @ J
         Jtr = (np.swapaxes(J, -1, -2) @ ra[..., None])[..., 0]
         damp = lam[idx] if s.optimizer == "lm" else np.full(idx.size, s.gn_eps)

@@ -162,7 +162,7 @@ def make_kin(name, spec, batch, seed, base_t, out):
 
 
 def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, factor=10.0, pos_w=1.0, ori_w=1.0,
-                 limit_w=0.1, rest_w=0.01, optimizer="lm"):
+                 limit_w=0.1, rest_w=0.01, optimizer="lm", kernel="l2"):
     """One float64 solve through the reference's own stack (``tasks/ik.py:191-258``)."""
     from better_robot.costs.stack import CostStack
     from better_robot.kinematics.forward import forward_kinematics
@@ -190,11 +190,13 @@ def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, facto
 
     prob = LeastSquaresProblem(cost_stack=stack, state_factory=sf, x0=q0.clone(), lower=m.lower_pos_limit,
                                upper=m.upper_pos_limit, nv=m.nv, retract=lambda q, dv: m.integrate(q, dv))
+    from better_robot.tasks.ik import _make_robust_kernel
+    k = _make_robust_kernel(kernel)   # solve_ik's own factory: None for "l2"
     if optimizer == "lm":
         st = LevenbergMarquardt(lam0=lam0, factor=factor, tol=tol).minimize(
-            prob, max_iter=max_iter, linear_solver=Cholesky(), strategy=Adaptive(lam0=lam0, factor=factor))
+            prob, max_iter=max_iter, linear_solver=Cholesky(), kernel=k, strategy=Adaptive(lam0=lam0, factor=factor))
     else:
-        st = GaussNewton(tol=tol).minimize(prob, max_iter=max_iter, linear_solver=Cholesky())
+        st = GaussNewton(tol=tol).minimize(prob, max_iter=max_iter, linear_solver=Cholesky(), kernel=k)
     return st
 
 
@@ -224,7 +226,20 @@ def make_ik(case, spec, frame_names, P, seed, start, out, **kw):
                         cost=np.array(res["cost"]),
                         settings=np.array([kw.get("lam0", 0), kw.get("factor", 0), kw["tol"], kw["max_iter"],
                                            kw.get("limit_w", 0.1), kw.get("rest_w", 0.01)]),
-                        optimizer=np.array(kw.get("optimizer", "lm")))
+                        optimizer=np.array(kw.get("optimizer", "lm")), kernel=np.array(kw.get("kernel", "l2")))
+
+
+def make_ik_kernels(chain, dual, hum, lm):
+    """Robust-kernel (IRLS) solves: random starts put chain residual rows outside Huber's
+    quadratic region; Cauchy and Tukey reweight every row."""
+    make_ik("chain7_huber", chain, ["ee"], 8, 25, "random", os.path.join(HERE, "ik_chain7_huber.npz"),
+            max_iter=50, kernel="huber", **lm)
+    make_ik("chain7_gn_cauchy", chain, ["ee"], 6, 26, "noisy", os.path.join(HERE, "ik_chain7_gn_cauchy.npz"),
+            max_iter=30, tol=1e-6, optimizer="gn", kernel="cauchy")
+    make_ik("dual_arm_cauchy", dual, ["ee_l", "ee_r"], 4, 27, "noisy", os.path.join(HERE, "ik_dual_arm_cauchy.npz"),
+            max_iter=100, rest_w=1e-3, kernel="cauchy", **lm)
+    make_ik("humanoid_tukey", hum, ["track0", "track2", "track4"], 4, 28, "noisy",
+            os.path.join(HERE, "ik_humanoid_tukey.npz"), max_iter=100, rest_w=1e-3, kernel="tukey", **lm)
 
 
 def make_adjoint(spec, B, seed, out):
@@ -310,6 +325,7 @@ def main():
             max_iter=100, rest_w=1e-3, **lm)
     make_ik("humanoid", hum, ["track0", "track2", "track4"], 4, 24, "noisy",
             os.path.join(HERE, "ik_humanoid.npz"), max_iter=100, rest_w=1e-3, **lm)
+    make_ik_kernels(chain, dual, hum, lm)
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
 

@@ -47,11 +47,15 @@ def _agreement(out, ref_conv, ref_res):
 
 
 @pytest.mark.parametrize("case,robot", [("chain7_random", "chain7"), ("chain7_gn", "chain7"),
-                                        ("dual_arm", "dual_arm"), ("humanoid", "humanoid")])
+                                        ("dual_arm", "dual_arm"), ("humanoid", "humanoid"),
+                                        ("chain7_huber", "chain7"), ("chain7_gn_cauchy", "chain7"),
+                                        ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid")])
 def test_reference_solver_golden(case, robot):
+    """The reference's own float64 solves (l2 and the robust IRLS kernels) reproduced on the GPU."""
     g = np.load(os.path.join(GOLDEN, f"ik_{case}.npz"))
     m, _ = _models(robot)
     cost, opt = _cfgs(g["settings"], str(g["optimizer"]))
+    opt.kernel = str(g["kernel"]) if "kernel" in g else "l2"
     fids = [int(f) for f in g["frame_ids"]]
     out = bik.solve_ik_batched(m, fids, torch.from_numpy(g["targets"]).float().cuda(),
                                torch.from_numpy(g["q0"]).float().cuda(), cost_cfg=cost, optimizer_cfg=opt,
@@ -194,7 +198,7 @@ def test_unsupported_options_raise():
     m, _ = _models("chain7")
     T = torch.zeros(1, 1, 7, device="cuda")
     q0 = torch.zeros(1, m.nq, device="cuda")
-    for opt in (bik.OptimizerConfig(optimizer="adam"), bik.OptimizerConfig(kernel="huber"),
+    for opt in (bik.OptimizerConfig(optimizer="adam"), bik.OptimizerConfig(damping="trust_region"),
                 bik.OptimizerConfig(linear_solver="lstsq")):
         with pytest.raises(NotImplementedError):
             bik.solve_ik_batched(m, [0], T, q0, optimizer_cfg=opt)
@@ -235,3 +239,24 @@ def test_autotune_and_graph_replay_match_direct_solve():
     for c in range(2):
         assert float((pk.q_of(c) - ref.q_of(c)).abs().max()) < 1e-3
     assert (pk.status == ref.status).float().mean() >= 0.95
+
+
+@pytest.mark.parametrize("kernel", ["huber", "cauchy", "tukey"])
+def test_robust_kernels_vs_oracle(kernel):
+    """IRLS-reweighted LM on noisy humanoid starts against the oracle's float64 IRLS LM."""
+    m, m64 = _models("humanoid")
+    P = 64
+    fids = [m.frame_id(f) for f in ("track0", "track2", "track4")]
+    q_star = syn.random_q(m64, P, 80, rev_range=2.5, base_translation=0.5)
+    oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+    targets = K.frame_placements(m64, oMi, fids)
+    q0 = syn.noisy_start(m64, q_star, 0.3, 81)
+    s = oik.IKSettings(lam0=1e-3, factor=10.0, tol=1e-6, max_iter=100, rest_weight=1e-3, kernel=kernel)
+    ref = oik.solve(m64, fids, targets, q0.numpy(), s)
+    out = bik.solve_ik_batched(m, fids, torch.from_numpy(targets).float().cuda(), q0.float().cuda(),
+                               cost_cfg=bik.IKCostConfig(rest_weight=1e-3),
+                               optimizer_cfg=bik.OptimizerConfig(max_iter=100, lam0=1e-3, factor=10.0, kernel=kernel),
+                               with_residual=True)
+    ok, conv, dres = _agreement(out, ref.converged, ref.residual)
+    assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
+    assert (conv == ref.converged).mean() >= 0.85, (conv.mean(), ref.converged.mean())
