@@ -48,7 +48,7 @@ class IKBatch(ctypes.Structure):
                 ("trees", ctypes.POINTER(BrTree)), ("team_size", ctypes.POINTER(c_int32)),
                 ("items", c_void_p), ("order", c_void_p), ("n_targets", c_void_p), ("frames", c_void_p),
                 ("targets", c_void_p), ("q_offset", c_void_p), ("x0", c_void_p), ("q_rest", c_void_p),
-                ("r_offset", c_void_p)]
+                ("r_offset", c_void_p), ("target_kind", c_void_p)]
 
 
 class IKResultBuf(ctypes.Structure):

@@ -1,14 +1,10 @@
 """Autotuner for the packed persistent LM launch.
 
-Picks, for a given packed batch, the team size (lanes per problem: 8, 16 or 32)
-of every robot class and the number of warps per CTA, by timing candidate
-launches of the real batch with CUDA events.  Results are cached per batch
-signature (robot shapes, target counts, problem counts), so a serving loop pays
-the search once.
-
-Candidates: team sizes from {8, 16, 32} not smaller than the class's default
-bucket minus one step (a 36-DOF humanoid may run on 16 or 32 lanes, a 7-DOF chain
-on 8 or 16), crossed with warps per CTA in {2, 4, 8}.
+Picks, for a given packed batch, the number of warps per CTA (and the team size of
+every robot class, which is 32 lanes: the kernel is built for one problem per warp)
+by timing candidate launches of the real batch with CUDA events.  Results are cached
+per batch signature (robot shapes, target counts, problem counts), so a serving loop
+pays the search once.  Candidates: warps per CTA in {2, 4, 8}.
 """
 
 from __future__ import annotations
@@ -21,11 +17,7 @@ _CACHE: dict = {}
 
 
 def _team_choices(nv: int) -> list[int]:
-    if nv <= 8:
-        return [8, 16]
-    if nv <= 16:
-        return [8, 16, 32]
-    return [16, 32]
+    return [32]  # the kernel is built for 32-lane teams (see lm_solve.cu)
 
 
 def signature(pk) -> tuple:

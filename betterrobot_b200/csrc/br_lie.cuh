@@ -100,7 +100,7 @@ __device__ __forceinline__ float vinv_coeff(float th2) {
   }
   const float th = sqrtf(th2);
   float sh, ch;
-  sincosf(0.5f * th, &sh, &ch);
+  sincospif(th * (0.5f / 3.14159265358979f), &sh, &ch);  // sin, cos of th / 2 (th <= pi for a log)
   return 1.f / th2 - (ch / sh) / (2.f * th);
 }
 

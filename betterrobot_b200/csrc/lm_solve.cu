@@ -6,11 +6,11 @@
 // (src/better_robot/optim/optimizers/levenberg_marquardt.py:61-135); here the whole
 // loop stays on the device:
 //
-//   * a TEAM of T lanes (T = 8, 16 or 32, chosen per robot class) owns one
-//     problem; a warp takes a work item of 32/T problems of one class from an
-//     atomic queue and its teams run their LM loops independently.  A team whose
-//     problem converges leaves the loop and the warp takes the next item, so no
-//     lane keeps iterating a converged problem (work compaction by queue);
+//   * a TEAM of T = 32 lanes (one warp) owns one problem; warps take problems from
+//     an atomic queue, heaviest robot class first.  A warp whose problem converges
+//     leaves the loop and takes the next item, so no lane keeps iterating a
+//     converged problem (work compaction by queue).  The team code is written for
+//     any T in {8, 16, 32}; only T = 32 is instantiated (see lm_solve_kernel);
 //   * per iteration: forward kinematics of the trial point by pointer jumping in
 //     shared memory, the stacked residual (pose targets, joint limits, rest) and
 //     its cost by a team reduction, accept/reject, and — only after an accepted
@@ -18,8 +18,9 @@
 //     the Jacobian build: J^T J and J^T r accumulated directly from the analytic
 //     pose Jacobian Jr^-1(xi) blockdiag(R^T, R^T) J_lwa (pose.py:68-103) with columns
 //     outside a target's support skipped;
-//   * H = J^T J + lambda I factored by a right-looking Cholesky in shared memory
-//     (lanes over the trailing triangle), triangular solves by shuffles;
+//   * H = J^T J + lambda I, stored per DOF over its ancestors in the DOF tree,
+//     factored leaves first as an unscaled LDL^T (no fill-in), triangular solves
+//     in registers with one shuffle per step;
 //   * retraction q (+) dq (Model.integrate, model.py:160-174) and clamping to the
 //     joint limits (levenberg_marquardt.py:103-107).
 //
@@ -53,7 +54,7 @@ struct LmParams {
 // ---- per-team shared-memory layout (floats) --------------------------------
 struct TeamLayout {
   int parent, jtype, idxq, idxv, support, cjoint, ckind, caxis, lower, upper;
-  int fparent, fplace, tgt;
+  int fparent, fplace, tgt, tkind;
   int dpar, ddep, rowoff, amask, ancd;
   int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc,
       dinv, sup, nsup;
@@ -65,7 +66,7 @@ struct TeamLayout {
     support = take(2 * nj);
     cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
     lower = take(nq); upper = take(nq);
-    fparent = take(K); fplace = take(8 * K);
+    fparent = take(K); fplace = take(8 * K); tkind = take(K);
     // float64 regions (2 floats per double)
     x = take(2 * nq); xn = take(2 * nq); qrest = take(2 * nq);
     poseA = take(14 * nj); poseB = take(14 * nj); tw = take(16 * K); xi = take(16 * K);
@@ -108,9 +109,10 @@ __device__ __forceinline__ float irls_weight(int kernel, double c, double s) {
   }
 }
 
-// DOFs one lane owns in the register triangular solves: a team of T lanes takes at most
-// lm_rows(T) * T DOFs (8 lanes: nv <= 16; 16 or 32 lanes: nv <= 64).
-__host__ __device__ constexpr int lm_rows(int T) { return T == 8 ? 2 : T == 16 ? 4 : 2; }
+// Lanes per problem (team size) the kernel is built for, and the DOFs one lane owns in the
+// register triangular solves (lm_rows(T) * T >= BR_MAX_NV).
+constexpr int kLmTeam = 32;
+__host__ __device__ constexpr int lm_rows(int T) { return (BR_MAX_NV + T - 1) / T; }
 
 template <int T>
 struct Team {
@@ -188,6 +190,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   float* lower = sm + L.lower;
   float* upper = sm + L.upper;
   int* fparent = reinterpret_cast<int*>(sm + L.fparent);
+  int* tkind = reinterpret_cast<int*>(sm + L.tkind);
   float* fplace = sm + L.fplace;
   double* x = reinterpret_cast<double*>(sm + L.x);
   double* xn = reinterpret_cast<double*>(sm + L.xn);
@@ -219,6 +222,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
   const double wpd = wp, wod = wo, wld = wl, wrd = wr;
   const double kc = S.kernel_param;
+  const bool irls = S.kernel != BR_KERNEL_L2;
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
 
   // ---- load the tree table and the problem -------------------------------
@@ -246,6 +250,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     if (t < nt) {
       const int f = P.b.frames[(int64_t)prob * K + t];
       fparent[t] = tree.frame_parent[f];
+      tkind[t] = P.b.target_kind ? P.b.target_kind[(int64_t)prob * K + t] : BR_TARGET_POSE;
       for (int k = 0; k < 8; ++k) fplace[8 * t + k] = tree.frame_placement[8 * f + k];
       const float* tp = P.b.targets + ((int64_t)prob * K + t) * 7;
       std8(tgt + 8 * t, DPose{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])});
@@ -349,11 +354,23 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     for (int t = tl; t < nt; t += T) {
       const DPose Tee = dcompose(lds(pose, nj, fparent[t]), to_d(ld8(fplace + 8 * t)));
       std8(tw + 8 * t, Tee);
-      double3 v, w;
-      dse3_log(dcompose(dinverse(ldd(tgt + 8 * t)), Tee), v, w);     // pose.py:63-64
       double* e = xi + 8 * t;
-      e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = w.x; e[4] = w.y; e[5] = w.z;
-      acc += wpd * wpd * ddot(v, v) + wod * wod * ddot(w, w);
+      const DPose Tt = ldd(tgt + 8 * t);
+      const int kind = tkind[t];
+      if (kind == BR_TARGET_POSITION) {                              // pose.py:127-131
+        const double3 dp = dsub(Tee.t, Tt.t);
+        e[0] = dp.x; e[1] = dp.y; e[2] = dp.z; e[3] = 0.0; e[4] = 0.0; e[5] = 0.0;
+        acc += wpd * wpd * ddot(dp, dp);
+      } else if (kind == BR_TARGET_ORIENTATION) {                    // pose.py:165-173
+        const double3 w = dso3_log(dqmul(dqconj(Tt.q), Tee.q));
+        e[0] = 0.0; e[1] = 0.0; e[2] = 0.0; e[3] = w.x; e[4] = w.y; e[5] = w.z;
+        acc += wod * wod * ddot(w, w);
+      } else {
+        double3 v, w;
+        dse3_log(dcompose(dinverse(Tt), Tee), v, w);                 // pose.py:63-64
+        e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = w.x; e[4] = w.y; e[5] = w.z;
+        acc += wpd * wpd * ddot(v, v) + wod * wod * ddot(w, w);
+      }
     }
     if (use_limits) {                                                // limits.py:56-62
       for (int i = tl; i < nq; i += T) {
@@ -398,9 +415,21 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       *reinterpret_cast<float4*>(colw + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
       g[c] = 0.f;
     }
-    for (int t = tl; t < nt; t += T) {                                 // Jr^-1(xi), tangents.py:204-207
+    for (int t = tl; t < nt; t += T) {
       const double* e = xi + 8 * t;
-      const JrInv J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
+      JrInv J;
+      if (tkind[t] == BR_TARGET_POSE) {                                // SE3 Jr^-1(xi), tangents.py:204-207
+        J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
+      } else {  // orientation: SO3 Jr^-1(r) (tangents.py:122-145) as the angular block, no coupling;
+                // position: identity (its rows are replaced by J_lwa's linear rows)
+        const bool ori = tkind[t] == BR_TARGET_ORIENTATION;
+        J.w = f3((float)e[3], (float)e[4], (float)e[5]);
+        J.b0 = 1.f;
+        J.b1 = ori ? 0.5f : 0.f;
+        J.b2 = ori ? vinv_coeff(dot(J.w, J.w)) : 0.f;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) J.B[k] = 0.f;
+      }
       float* o = jri + 16 * t;
       o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
       for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
@@ -410,6 +439,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     float* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
     for (int t = 0; t < nt; ++t) {
       const int ns = nsup[t];
+      const int kind = tkind[t];
       const unsigned char* st = sup + t * nv;
       const Pose Tee = to_f(ldd(tw + 8 * t));
       const float* o = jri + 16 * t;
@@ -432,17 +462,25 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           ang = f3(0.f, 0.f, 0.f);
         }
         float3 ol, oa;
-        jr_inv_apply(J, qrot_inv(Tee.q, lin), qrot_inv(Tee.q, ang), ol, oa);   // pose.py:91-99
+        jr_inv_apply(J, qrot_inv(Tee.q, lin), qrot_inv(Tee.q, ang), ol, oa);  // pose.py:91-99
+        if (kind == BR_TARGET_POSITION) {            // top rows of J_lwa (pose.py:133-141)
+          ol = lin;
+          oa = f3(0.f, 0.f, 0.f);
+        } else if (kind == BR_TARGET_ORIENTATION) {  // Jr^-1(r) R^T J_ang (pose.py:175-195)
+          ol = f3(0.f, 0.f, 0.f);
+        }
         Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
         Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
       }
       tm.sync();
       const double* e = xi + 8 * t;
-      float kw[6];  // IRLS weight of each of the target's 6 stacked rows (1 for the l2 kernel)
+      float kw[6] = {1.f, 1.f, 1.f, 1.f, 1.f, 1.f};  // IRLS weight of each of the target's 6 rows
+      if (irls) {
 #pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        const double rr = (r < 3 ? wpd : wod) * e[r];
-        kw[r] = irls_weight(S.kernel, kc, rr * rr);
+        for (int r = 0; r < 6; ++r) {
+          const double rr = (r < 3 ? wpd : wod) * e[r];
+          kw[r] = irls_weight(S.kernel, kc, rr * rr);
+        }
       }
       for (int p = tl; p < tri(ns); p += T) {
         int u = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);   // row-major (u >= v) decode of p
@@ -450,8 +488,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         if (tri(u) > p) --u;
         const int v = p - tri(u);
         float acc = 0.f;
+        if (irls) {
 #pragma unroll
-        for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u] * kw[r], Jc[r * nv + v], acc);
+          for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u] * kw[r], Jc[r * nv + v], acc);
+        } else {
+#pragma unroll
+          for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], Jc[r * nv + v], acc);
+        }
         jtj[rowoff[st[u]] + ddep[st[v]]] += acc;  // st ascending: st[u] descends from st[v]
       }
       const float rw[6] = {wp * (float)e[0] * kw[0], wp * (float)e[1] * kw[1], wp * (float)e[2] * kw[2],
@@ -470,7 +513,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       float dg = 0.f, gc = g[c];
       if (use_rest) {
         const double rr = wrd * dr[c];
-        const float w = irls_weight(S.kernel, kc, rr * rr);
+        const float w = irls ? irls_weight(S.kernel, kc, rr * rr) : 1.f;
         dg += wr * wr * w;
         gc += wr * wr * w * (float)dr[c];
       }
@@ -662,12 +705,21 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     pose = fk(x);
     residual(x, pose);
     float* out = P.r.residual + P.b.r_offset[prob];
-    for (int t = tl; t < nt; t += T) {
+    int o = 0;  // rows of the targets: 6 per pose, 3 per position or orientation target
+    for (int t = 0; t < nt; ++t) {
       const double* e = xi + 8 * t;
-      out[6 * t + 0] = (float)(wpd * e[0]); out[6 * t + 1] = (float)(wpd * e[1]); out[6 * t + 2] = (float)(wpd * e[2]);
-      out[6 * t + 3] = (float)(wod * e[3]); out[6 * t + 4] = (float)(wod * e[4]); out[6 * t + 5] = (float)(wod * e[5]);
+      const int kind = tkind[t];
+      if (tl == 0) {
+        if (kind != BR_TARGET_ORIENTATION) {
+          out[o + 0] = (float)(wpd * e[0]); out[o + 1] = (float)(wpd * e[1]); out[o + 2] = (float)(wpd * e[2]);
+        }
+        if (kind != BR_TARGET_POSITION) {
+          const int a = kind == BR_TARGET_POSE ? o + 3 : o;
+          out[a + 0] = (float)(wod * e[3]); out[a + 1] = (float)(wod * e[4]); out[a + 2] = (float)(wod * e[5]);
+        }
+      }
+      o += kind == BR_TARGET_POSE ? 6 : 3;
     }
-    int o = 6 * nt;
     if (use_limits) {
       for (int i = tl; i < nq; i += T) {
         out[o + i] = (float)(wld * fmax((double)lower[i] - x[i], 0.0));
@@ -711,11 +763,10 @@ __global__ void lm_solve_kernel(const LmParams P) {
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= P.b.n_items) break;
     const int first = P.b.items[3 * item], count = P.b.items[3 * item + 1], cls = P.b.items[3 * item + 2];
-    switch (P.team[cls]) {
-      case 8: run_item<8>(P, cls, first, count, wsm, lane); break;
-      case 16: run_item<16>(P, cls, first, count, wsm, lane); break;
-      default: run_item<32>(P, cls, first, count, wsm, lane); break;
-    }
+    // One instantiation: 32-lane teams.  8- and 16-lane teams (several small problems per
+    // warp) were measured slower on the mixed batch: three copies of this kernel body
+    // overflow the instruction cache, and 32 lanes are the fastest per class on their own.
+    run_item<kLmTeam>(P, cls, first, count, wsm, lane);
     __syncwarp();
   }
 }
@@ -726,7 +777,7 @@ using namespace br;
 
 extern "C" int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets) {
   if (!tree || max_targets < 0) return BR_EINVAL;
-  const int T = tree->nv <= 8 ? 8 : tree->nv <= 16 ? 16 : 32;
+  const int T = kLmTeam;
   return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T).total;
 }
 
@@ -755,8 +806,7 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     const int st = validate_tree(&b.trees[c]);
     if (st) return st;
     const int T = b.team_size[c];
-    if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
-    if (b.trees[c].nv > lm_rows(T) * T) return BR_EINVAL;  // 8-lane teams take nv <= 16
+    if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;
@@ -863,8 +913,7 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     st = validate_tree(&b.trees[c]);
     if (st) return st;
     const int T = b.team_size[c];
-    if (T != 8 && T != 16 && T != 32) return BR_EINVAL;
-    if (b.trees[c].nv > lm_rows(T) * T) return BR_EINVAL;  // 8-lane teams take nv <= 16
+    if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;

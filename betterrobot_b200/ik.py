@@ -70,6 +70,7 @@ class OptimizerConfig:
 # OptimizerConfig.kernel -> BR_KERNEL_*, and the default parameter of each kernel class
 # (src/better_robot/optim/kernels/huber.py, cauchy.py, tukey.py)
 KERNELS = {"l2": 0, "huber": 1, "cauchy": 2, "tukey": 3}
+TARGET_KINDS = {"pose": 0, "position": 1, "orientation": 2}   # BR_TARGET_*
 KERNEL_DEFAULTS = {"huber": 1.0, "cauchy": 1.0, "tukey": 4.685}
 
 
@@ -137,8 +138,8 @@ def team_floats(model, max_targets: int, device) -> int:
 
 
 def default_team_size(model) -> int:
-    nv = int(model.nv)
-    return 8 if nv <= 8 else 16 if nv <= 16 else 32
+    """Lanes per problem: the kernel is built for 32-lane teams only."""
+    return 32
 
 
 class PackedIK:
@@ -153,7 +154,7 @@ class PackedIK:
 
     def __init__(self, models: Sequence, frame_ids: Sequence, n_targets: Sequence, q_rest: Sequence | None = None,
                  team_sizes: Sequence[int] | None = None, device="cuda", warps_per_cta: int = 4,
-                 with_residual: bool = False):
+                 with_residual: bool = False, target_kinds: Sequence | None = None):
         if not 1 <= len(models) <= MAX_CLASSES:
             raise ShapeError(f"1..{MAX_CLASSES} robot classes per launch, got {len(models)}")
         self.device = torch.device(device)
@@ -168,8 +169,8 @@ class PackedIK:
             raise ShapeError(f"at most {MAX_TARGETS} targets per problem")
         self.team = [int(t) for t in (team_sizes or [default_team_size(m) for m in models])]
         for m, t in zip(models, self.team):
-            if t not in (8, 16, 32) or (t == 8 and int(m.nv) > 16):
-                raise ShapeError(f"team size {t} for nv={m.nv}: use 8 (nv <= 16), 16 or 32 lanes")
+            if t != 32:
+                raise ShapeError(f"team size {t}: the kernel runs one problem per 32-lane warp")
         self.trees = [device_tree(m, self.device) for m in models]
         self.warps_per_cta = warps_per_cta
         # per-problem layout: classes contiguous, in class order
@@ -187,10 +188,23 @@ class PackedIK:
                 raise ShapeError(f"class {c}: frame id out of range")
             s0 = self.class_start[c]
             fr[s0:s0 + self.counts[c], :f.shape[1]] = f
+        kinds = np.zeros((self.P, self.K), np.int32)
+        if target_kinds is not None:
+            for c in range(self.C):
+                if target_kinds[c] is None:
+                    continue
+                k = np.asarray([TARGET_KINDS[x] if isinstance(x, str) else int(x)
+                                for x in np.asarray(target_kinds[c]).reshape(-1)], np.int32)
+                k = k.reshape(np.asarray(target_kinds[c]).shape)
+                if ((k < 0) | (k > 2)).any():
+                    raise ShapeError("target kinds are 'pose', 'position' or 'orientation'")
+                s0 = self.class_start[c]
+                kinds[s0:s0 + self.counts[c], :k.shape[-1]] = np.broadcast_to(k, (self.counts[c], k.shape[-1]))
+        rows = np.where(kinds == 0, 6, 3) * (np.arange(self.K)[None, :] < nt_all[:, None])
         dims = []
         for c, m in enumerate(models):
-            n = np.asarray(n_targets[c], np.int64)
-            dims.append(6 * n + 2 * m.nq + m.nv)
+            s0 = self.class_start[c]
+            dims.append(rows[s0:s0 + self.counts[c]].sum(-1) + 2 * m.nq + m.nv)
         rdim = np.concatenate(dims)
         self.r_offset_np = np.concatenate([[0], np.cumsum(rdim)[:-1]]).astype(np.int64)
         self.r_dim = rdim
@@ -213,6 +227,7 @@ class PackedIK:
         self.frames_t = torch.from_numpy(fr).to(dev)
         self.q_offset = torch.from_numpy(self.q_offset_np).to(dev)
         self.r_offset = torch.from_numpy(self.r_offset_np).to(dev)
+        self.kinds = torch.from_numpy(kinds).to(dev) if kinds.any() else None
         self.targets = torch.zeros(self.P, self.K, 7, device=dev)
         self.targets[..., 6] = 1.0
         self.x0 = torch.zeros(self.q_total, device=dev)
@@ -240,6 +255,7 @@ class PackedIK:
         b.targets, b.q_offset = self.targets.data_ptr(), self.q_offset.data_ptr()
         b.x0, b.q_rest = self.x0.data_ptr(), self.q_rest.data_ptr()
         b.r_offset = self.r_offset.data_ptr()
+        b.target_kind = self.kinds.data_ptr() if self.kinds is not None else None
         self._batch = b
         r = IKResultBuf()
         r.x, r.iters, r.status, r.cost = self.x.data_ptr(), self.iters.data_ptr(), self.status.data_ptr(), \
@@ -293,9 +309,16 @@ class PackedIK:
 def solve_ik_batched(model, frame_ids, targets: torch.Tensor, initial_q: torch.Tensor, *,
                      cost_cfg: IKCostConfig | None = None, optimizer_cfg: OptimizerConfig | None = None,
                      n_targets=None, with_residual: bool = False, team_size: int | None = None,
-                     warps_per_cta: int = 4) -> BatchIKResult:
+                     warps_per_cta: int = 4, target_kinds=None) -> BatchIKResult:
     """Solve ``P`` independent problems of one robot: ``targets (P, K, 7)`` for ``frame_ids``
-    (K ids shared by all problems, or ``(P, K)``), ``initial_q (P, nq)``."""
+    (K ids shared by all problems, or ``(P, K)``), ``initial_q (P, nq)``.
+
+    ``target_kinds`` (K names, or a ``(P, K)`` array): "pose" (``PoseResidual``, the
+    default), "position" (``PositionResidual``, weight ``pos_weight * pose_weight``) or
+    "orientation" (``OrientationResidual``, weight ``ori_weight * pose_weight``),
+    ``src/better_robot/residuals/pose.py:58-195``.  With ``with_residual`` the stacked
+    residual has 6 rows per pose target and 3 per position / orientation target.
+    """
     cost_cfg = cost_cfg or IKCostConfig()
     optimizer_cfg = optimizer_cfg or OptimizerConfig()
     if initial_q.dim() != 2 or initial_q.shape[-1] != model.nq:
@@ -311,13 +334,15 @@ def solve_ik_batched(model, frame_ids, targets: torch.Tensor, initial_q: torch.T
     nt = np.full(P, K, np.int32) if n_targets is None else np.asarray(n_targets, np.int32)
     qr = [cost_cfg.q_rest] if cost_cfg.q_rest is not None else None
     pk = PackedIK([model], [fr], [nt], q_rest=qr, team_sizes=[team_size or default_team_size(model)],
-                  device=initial_q.device, warps_per_cta=warps_per_cta, with_residual=with_residual)
+                  device=initial_q.device, warps_per_cta=warps_per_cta, with_residual=with_residual,
+                  target_kinds=None if target_kinds is None else [target_kinds])
     pk.set_inputs([targets], [initial_q])
     with torch.cuda.device(initial_q.device):
         pk.solve(settings_from(cost_cfg, optimizer_cfg))
     res = None
     if with_residual:
-        res = pk.residual.view(P, -1)
+        res = (pk.residual.view(P, -1) if (pk.r_dim == pk.r_dim[0]).all()
+               else list(torch.split(pk.residual, [int(d) for d in pk.r_dim])))
     return BatchIKResult(q=pk.q_of(0), iters=pk.iters, converged=(pk.status & 0xFF) == 0, status=pk.status,
                          cost=pk.cost, residual=res)
 

@@ -122,6 +122,9 @@ BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joi
 #define BR_LM_SCRATCH_BYTES 16  /* device scratch br_lm_solve needs (work queue)   */
 #define BR_OPT_LM 0
 #define BR_OPT_GN 1
+#define BR_TARGET_POSE 0        /* PoseResidual: 6 rows (residuals/pose.py:58-103)            */
+#define BR_TARGET_POSITION 1    /* PositionResidual: 3 rows (pose.py:107-141), weight pos_weight */
+#define BR_TARGET_ORIENTATION 2 /* OrientationResidual: 3 rows (pose.py:144-195), weight ori_weight */
 #define BR_KERNEL_L2 0          /* robust kernels of OptimizerConfig.kernel (tasks/ik.py:116-133) */
 #define BR_KERNEL_HUBER 1       /* w(s) = 1 if s <= d^2 else d / sqrt(s)                          */
 #define BR_KERNEL_CAUCHY 2      /* w(s) = 1 / (1 + s / c^2)                                       */
@@ -148,7 +151,7 @@ typedef struct br_ik_settings {
 typedef struct br_ik_batch {
     int32_t n_problems, max_targets, n_classes, n_items;
     const br_tree_t* trees;     /* HOST array [n_classes] (its tables live on the device) */
-    const int32_t* team_size;   /* HOST array [n_classes]: lanes per problem, 8/16/32 */
+    const int32_t* team_size;   /* HOST array [n_classes]: lanes per problem; must be 32 */
     const int32_t* items;       /* [n_items*3] work items: first slot in order[], count <= 32/team, class */
     const int32_t* order;       /* [n_problems] problem index of each slot          */
     const int32_t* n_targets;   /* [n_problems] 1..max_targets                       */
@@ -158,7 +161,8 @@ typedef struct br_ik_batch {
     const float* x0;            /* packed initial configurations                    */
     const float* q_rest;        /* packed rest configurations (RestResidual q_rest) */
     const int64_t* r_offset;    /* [n_problems] float offset of the problem's stacked residual
-                                   (6*n_targets + 2*nq + nv floats) in result.residual; may be NULL */
+                                   (target rows + 2*nq + nv floats) in result.residual; may be NULL */
+    const int32_t* target_kind; /* [n_problems*max_targets] BR_TARGET_*; NULL = every target a pose */
 } br_ik_batch_t;
 
 typedef struct br_ik_result {

@@ -67,10 +67,13 @@ def _np(x):
     return K._np(x)
 
 
-def residual_and_jacobian(model, q, frame_ids, targets, q_rest, s: IKSettings, want_jac: bool = True):
+def residual_and_jacobian(model, q, frame_ids, targets, q_rest, s: IKSettings, want_jac: bool = True, kinds=None):
     """Stacked residual ``(P, dim)`` and Jacobian ``(P, dim, nv)`` of the IK cost stack at ``q (P, nq)``.
 
-    ``targets (P, k, 7)`` are the per-problem target poses of ``frame_ids`` (length k).
+    ``targets (P, k, 7)`` are the per-problem target poses of ``frame_ids`` (length k);
+    ``kinds[i]`` is "pose" (default, ``PoseResidual`` with pos / ori weights), "position"
+    (``PositionResidual``, weight ``pos_weight``) or "orientation" (``OrientationResidual``,
+    weight ``ori_weight``), ``residuals/pose.py:58-195``.
     """
     q = _np(q)
     oMi, _ = K.forward_kinematics(model, q)
@@ -80,6 +83,21 @@ def residual_and_jacobian(model, q, frame_ids, targets, q_rest, s: IKSettings, w
         Tt = targets[:, i, :]
         fr = model.frames[f]
         Tee = lie.se3_compose(oMi[:, fr.parent_joint, :], _np(fr.joint_placement))
+        kind = "pose" if kinds is None else kinds[i]
+        if kind == "position":                                            # pose.py:127-141
+            rs.append((Tee[:, :3] - Tt[:, :3]) * s.pos_weight)
+            if want_jac:
+                Jlwa = K.frame_jacobian(model, oMi, q, f, "local_world_aligned")
+                Js.append(Jlwa[:, :3] * s.pos_weight)
+            continue
+        if kind == "orientation":                                         # pose.py:165-195
+            r = lie.so3_log(lie.quat_mul(lie.so3_inverse(Tt[:, 3:7]), Tee[:, 3:7]))
+            rs.append(r * s.ori_weight)
+            if want_jac:
+                Jlwa = K.frame_jacobian(model, oMi, q, f, "local_world_aligned")
+                RT = np.swapaxes(lie.quat_to_matrix(Tee[:, 3:7]), -1, -2)
+                Js.append(lie.right_jacobian_inv_so3(r) @ (RT @ Jlwa[:, 3:]) * s.ori_weight)
+            continue
         xi = lie.se3_log(lie.se3_compose(lie.se3_inverse(Tt), Tee))       # pose.py:63-64
         rs.append(xi * w)
         if want_jac:
@@ -139,7 +157,7 @@ class IKOutcome:
     converged: np.ndarray  # (P,)   bool
 
 
-def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None) -> IKOutcome:
+def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None, kinds=None) -> IKOutcome:
     """Run LM (or GN) on ``P`` independent problems; each follows the single-instance reference loop."""
     q = _np(q0).copy()
     P = q.shape[0]
@@ -147,7 +165,7 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None) -> IKOutcom
     q_rest = _np(model.q_neutral) if q_rest is None else _np(q_rest)
     lo = _np(model.lower_pos_limit)
     hi = _np(model.upper_pos_limit)
-    r, _ = residual_and_jacobian(model, q, frame_ids, targets, q_rest, s, want_jac=False)
+    r, _ = residual_and_jacobian(model, q, frame_ids, targets, q_rest, s, want_jac=False, kinds=kinds)
     cost = 0.5 * np.sum(r * r, -1)
     lam = np.full(P, s.lam0 if s.optimizer == "lm" else 0.0)
     active = np.ones(P, dtype=bool)
@@ -159,7 +177,7 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None) -> IKOutcom
         if idx.size == 0:
             break
         qa = q[idx]
-        _, J = residual_and_jacobian(model, qa, frame_ids, targets[idx], q_rest, s)
+        _, J = residual_and_jacobian(model, qa, frame_ids, targets[idx], q_rest, s, kinds=kinds)
         ra = r[idx]
         if s.kernel != "l2":  # IRLS: rows scaled by sqrt(w(r_i^2)) (levenberg_marquardt.py:27-44)
             sw = np.sqrt(np.maximum(kernel_weight(s.kernel, ra * ra, s.kernel_param), 0.0))
@@ -172,7 +190,7 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None) -> IKOutcom
         dv = _solve(H, -Jtr)
         qn = K.integrate(model, qa, dv)
         qn = np.minimum(np.maximum(qn, lo), hi)
-        rn, _ = residual_and_jacobian(model, qn, frame_ids, targets[idx], q_rest, s, want_jac=False)
+        rn, _ = residual_and_jacobian(model, qn, frame_ids, targets[idx], q_rest, s, want_jac=False, kinds=kinds)
         cn = 0.5 * np.sum(rn * rn, -1)
         gnorm = np.linalg.norm(Jtr, axis=-1)
         if s.optimizer == "lm":

@@ -209,3 +209,15 @@ def so3_from_matrix(R: np.ndarray) -> np.ndarray:
     c3 = (m[..., 1, 1] > m[..., 2, 2])[..., None]
     q = np.where(c1, q1, np.where(c2, q2, np.where(c3, q3, q4)))
     return q / np.maximum(np.linalg.norm(q, axis=-1, keepdims=True), 1e-12)
+
+
+def right_jacobian_inv_so3(w: np.ndarray) -> np.ndarray:
+    """``tangents.right_jacobian_inv_so3:122-145``: ``I + hat/2 + C hat^2``,
+    ``C = 1/theta^2 - (1 + cos theta) / (2 theta sin theta)`` (1/12 + theta^2/720 below theta^2 = 1e-10)."""
+    th2 = np.sum(w * w, -1)
+    th = np.sqrt(np.maximum(th2, 0.0))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        full = 1.0 / np.maximum(th2, 1e-30) - (1.0 + np.cos(th)) / np.maximum(2.0 * th * np.sin(th), 1e-30)
+    C = np.where(th2 > 1e-10, full, 1.0 / 12.0 + th2 / 720.0)
+    H = hat(w)
+    return np.eye(3) + 0.5 * H + C[..., None, None] * (H @ H)

@@ -162,7 +162,7 @@ def make_kin(name, spec, batch, seed, base_t, out):
 
 
 def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, factor=10.0, pos_w=1.0, ori_w=1.0,
-                 limit_w=0.1, rest_w=0.01, optimizer="lm", kernel="l2"):
+                 limit_w=0.1, rest_w=0.01, optimizer="lm", kernel="l2", kinds=None):
     """One float64 solve through the reference's own stack (``tasks/ik.py:191-258``)."""
     from better_robot.costs.stack import CostStack
     from better_robot.kinematics.forward import forward_kinematics
@@ -176,10 +176,18 @@ def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, facto
     from better_robot.residuals.pose import PoseResidual
     from better_robot.residuals.regularization import RestResidual
 
+    from better_robot.residuals.pose import OrientationResidual, PositionResidual
+
     stack = CostStack()
-    for name, T in zip(frame_names, targets):
-        stack.add(f"pose_{name}", PoseResidual(frame_id=m.frame_id(name), target=T, pos_weight=pos_w,
-                                               ori_weight=ori_w), weight=1.0)
+    for i, (name, T) in enumerate(zip(frame_names, targets)):
+        kind = "pose" if kinds is None else kinds[i]
+        if kind == "position":
+            res = PositionResidual(frame_id=m.frame_id(name), target=T, weight=pos_w)
+        elif kind == "orientation":
+            res = OrientationResidual(frame_id=m.frame_id(name), target=T, weight=ori_w)
+        else:
+            res = PoseResidual(frame_id=m.frame_id(name), target=T, pos_weight=pos_w, ori_weight=ori_w)
+        stack.add(f"{kind}_{name}", res, weight=1.0)
     if limit_w > 0:
         stack.add("limits", JointPositionLimit(m), weight=limit_w)
     if rest_w > 0:
@@ -226,7 +234,8 @@ def make_ik(case, spec, frame_names, P, seed, start, out, **kw):
                         cost=np.array(res["cost"]),
                         settings=np.array([kw.get("lam0", 0), kw.get("factor", 0), kw["tol"], kw["max_iter"],
                                            kw.get("limit_w", 0.1), kw.get("rest_w", 0.01)]),
-                        optimizer=np.array(kw.get("optimizer", "lm")), kernel=np.array(kw.get("kernel", "l2")))
+                        optimizer=np.array(kw.get("optimizer", "lm")), kernel=np.array(kw.get("kernel", "l2")),
+                        kinds=np.array(kw.get("kinds") or ["pose"] * len(frame_names)))
 
 
 def make_ik_kernels(chain, dual, hum, lm):
@@ -240,6 +249,17 @@ def make_ik_kernels(chain, dual, hum, lm):
             max_iter=100, rest_w=1e-3, kernel="cauchy", **lm)
     make_ik("humanoid_tukey", hum, ["track0", "track2", "track4"], 4, 28, "noisy",
             os.path.join(HERE, "ik_humanoid_tukey.npz"), max_iter=100, rest_w=1e-3, kernel="tukey", **lm)
+
+
+def make_ik_kinds(chain, dual, hum, lm):
+    """Stacks with PositionResidual / OrientationResidual targets (residuals/pose.py:107-195)."""
+    make_ik("chain7_position", chain, ["ee"], 8, 29, "noisy", os.path.join(HERE, "ik_chain7_position.npz"),
+            max_iter=50, kinds=["position"], **lm)
+    make_ik("dual_arm_mixed", dual, ["ee_l", "ee_r"], 4, 30, "noisy", os.path.join(HERE, "ik_dual_arm_mixed.npz"),
+            max_iter=100, rest_w=1e-3, kinds=["position", "orientation"], **lm)
+    make_ik("humanoid_mixed", hum, ["track0", "track2", "track4"], 4, 31, "noisy",
+            os.path.join(HERE, "ik_humanoid_mixed.npz"), max_iter=100, rest_w=1e-3,
+            kinds=["pose", "position", "orientation"], **lm)
 
 
 def make_adjoint(spec, B, seed, out):
@@ -326,6 +346,7 @@ def main():
     make_ik("humanoid", hum, ["track0", "track2", "track4"], 4, 24, "noisy",
             os.path.join(HERE, "ik_humanoid.npz"), max_iter=100, rest_w=1e-3, **lm)
     make_ik_kernels(chain, dual, hum, lm)
+    make_ik_kinds(chain, dual, hum, lm)
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
 

@@ -49,7 +49,9 @@ def _agreement(out, ref_conv, ref_res):
 @pytest.mark.parametrize("case,robot", [("chain7_random", "chain7"), ("chain7_gn", "chain7"),
                                         ("dual_arm", "dual_arm"), ("humanoid", "humanoid"),
                                         ("chain7_huber", "chain7"), ("chain7_gn_cauchy", "chain7"),
-                                        ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid")])
+                                        ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid"),
+                                        ("chain7_position", "chain7"), ("dual_arm_mixed", "dual_arm"),
+                                        ("humanoid_mixed", "humanoid")])
 def test_reference_solver_golden(case, robot):
     """The reference's own float64 solves (l2 and the robust IRLS kernels) reproduced on the GPU."""
     g = np.load(os.path.join(GOLDEN, f"ik_{case}.npz"))
@@ -57,9 +59,10 @@ def test_reference_solver_golden(case, robot):
     cost, opt = _cfgs(g["settings"], str(g["optimizer"]))
     opt.kernel = str(g["kernel"]) if "kernel" in g else "l2"
     fids = [int(f) for f in g["frame_ids"]]
+    kinds = [str(k) for k in g["kinds"]] if "kinds" in g else None
     out = bik.solve_ik_batched(m, fids, torch.from_numpy(g["targets"]).float().cuda(),
                                torch.from_numpy(g["q0"]).float().cuda(), cost_cfg=cost, optimizer_cfg=opt,
-                               with_residual=True)
+                               with_residual=True, target_kinds=kinds)
     ok, conv, dres = _agreement(out, g["converged"], g["residual"])
     # every converged reference solve must converge here to the same residual
     both = g["converged"].astype(bool)
@@ -257,6 +260,31 @@ def test_robust_kernels_vs_oracle(kernel):
                                cost_cfg=bik.IKCostConfig(rest_weight=1e-3),
                                optimizer_cfg=bik.OptimizerConfig(max_iter=100, lam0=1e-3, factor=10.0, kernel=kernel),
                                with_residual=True)
+    ok, conv, dres = _agreement(out, ref.converged, ref.residual)
+    assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
+    assert (conv == ref.converged).mean() >= 0.85, (conv.mean(), ref.converged.mean())
+
+
+@pytest.mark.parametrize("robot,frames,kinds", [
+    ("chain7", ["ee"], ["position"]),
+    ("dual_arm", ["ee_l", "ee_r"], ["position", "orientation"]),
+    ("humanoid", ["track0", "track2", "track4"], ["pose", "position", "orientation"])])
+def test_position_orientation_targets_vs_oracle(robot, frames, kinds):
+    """PositionResidual / OrientationResidual targets (pose.py:107-195) against the float64 oracle."""
+    m, m64 = _models(robot)
+    P = 64
+    fids = [m.frame_id(f) for f in frames]
+    q_star = syn.random_q(m64, P, 90, rev_range=2.5, base_translation=0.5)
+    oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+    targets = K.frame_placements(m64, oMi, fids)
+    q0 = syn.noisy_start(m64, q_star, 0.3, 91)
+    s = oik.IKSettings(lam0=1e-3, factor=10.0, tol=1e-6, max_iter=100, rest_weight=1e-3)
+    ref = oik.solve(m64, fids, targets, q0.numpy(), s, kinds=kinds)
+    out = bik.solve_ik_batched(m, fids, torch.from_numpy(targets).float().cuda(), q0.float().cuda(),
+                               cost_cfg=bik.IKCostConfig(rest_weight=1e-3),
+                               optimizer_cfg=bik.OptimizerConfig(max_iter=100, lam0=1e-3, factor=10.0),
+                               with_residual=True, target_kinds=kinds)
+    assert out.residual.shape == ref.residual.shape
     ok, conv, dres = _agreement(out, ref.converged, ref.residual)
     assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
     assert (conv == ref.converged).mean() >= 0.85, (conv.mean(), ref.converged.mean())

@@ -62,7 +62,9 @@ def test_lie_matches_reference():
 @pytest.mark.parametrize("case,robot", [("chain7_random", "chain7"), ("chain7_gn", "chain7"),
                                         ("dual_arm", "dual_arm"), ("humanoid", "humanoid"),
                                         ("chain7_huber", "chain7"), ("chain7_gn_cauchy", "chain7"),
-                                        ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid")])
+                                        ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid"),
+                                        ("chain7_position", "chain7"), ("dual_arm_mixed", "dual_arm"),
+                                        ("humanoid_mixed", "humanoid")])
 def test_lm_gn_match_reference_solver(case, robot):
     g = _load(f"ik_{case}.npz")
     m = syn.model_from_spec(SPECS[robot], dtype=torch.float64)
@@ -70,7 +72,8 @@ def test_lm_gn_match_reference_solver(case, robot):
     s = ik.IKSettings(lam0=st[0], factor=st[1], tol=st[2], max_iter=int(st[3]), limit_weight=st[4],
                       rest_weight=st[5], optimizer=str(g["optimizer"]),
                       kernel=str(g["kernel"]) if "kernel" in g else "l2")
-    out = ik.solve(m, [int(f) for f in g["frame_ids"]], g["targets"], g["q0"], s)
+    kinds = [str(k) for k in g["kinds"]] if "kinds" in g else None
+    out = ik.solve(m, [int(f) for f in g["frame_ids"]], g["targets"], g["q0"], s, kinds=kinds)
     np.testing.assert_array_equal(out.iters, g["iters"])
     np.testing.assert_array_equal(out.converged, g["converged"])
     np.testing.assert_allclose(out.q, g["q_final"], atol=1e-9, rtol=0)
