@@ -172,7 +172,9 @@ __device__ __forceinline__ Pose to_f(const DPose& P) {
 }
 
 // ---- one problem, solved by one team ---------------------------------------
-template <int T>
+// kGeneral = false compiles the plain stack (pose targets, l2 kernel) with the target-kind
+// and IRLS branches folded away; the host launches it whenever a batch needs nothing else.
+template <int T, bool kGeneral>
 __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
   const int K = P.b.max_targets;
@@ -222,7 +224,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
   const double wpd = wp, wod = wo, wld = wl, wrd = wr;
   const double kc = S.kernel_param;
-  const bool irls = S.kernel != BR_KERNEL_L2;
+  const bool irls = kGeneral && S.kernel != BR_KERNEL_L2;
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
 
   // ---- load the tree table and the problem -------------------------------
@@ -250,7 +252,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     if (t < nt) {
       const int f = P.b.frames[(int64_t)prob * K + t];
       fparent[t] = tree.frame_parent[f];
-      tkind[t] = P.b.target_kind ? P.b.target_kind[(int64_t)prob * K + t] : BR_TARGET_POSE;
+      tkind[t] = (kGeneral && P.b.target_kind) ? P.b.target_kind[(int64_t)prob * K + t] : BR_TARGET_POSE;
       for (int k = 0; k < 8; ++k) fplace[8 * t + k] = tree.frame_placement[8 * f + k];
       const float* tp = P.b.targets + ((int64_t)prob * K + t) * 7;
       std8(tgt + 8 * t, DPose{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])});
@@ -356,7 +358,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       std8(tw + 8 * t, Tee);
       double* e = xi + 8 * t;
       const DPose Tt = ldd(tgt + 8 * t);
-      const int kind = tkind[t];
+      const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
       if (kind == BR_TARGET_POSITION) {                              // pose.py:127-131
         const double3 dp = dsub(Tee.t, Tt.t);
         e[0] = dp.x; e[1] = dp.y; e[2] = dp.z; e[3] = 0.0; e[4] = 0.0; e[5] = 0.0;
@@ -418,7 +420,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     for (int t = tl; t < nt; t += T) {
       const double* e = xi + 8 * t;
       JrInv J;
-      if (tkind[t] == BR_TARGET_POSE) {                                // SE3 Jr^-1(xi), tangents.py:204-207
+      if (!kGeneral || tkind[t] == BR_TARGET_POSE) {                   // SE3 Jr^-1(xi), tangents.py:204-207
         J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
       } else {  // orientation: SO3 Jr^-1(r) (tangents.py:122-145) as the angular block, no coupling;
                 // position: identity (its rows are replaced by J_lwa's linear rows)
@@ -439,7 +441,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     float* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
     for (int t = 0; t < nt; ++t) {
       const int ns = nsup[t];
-      const int kind = tkind[t];
+      const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
       const unsigned char* st = sup + t * nv;
       const Pose Tee = to_f(ldd(tw + 8 * t));
       const float* o = jri + 16 * t;
@@ -708,7 +710,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     int o = 0;  // rows of the targets: 6 per pose, 3 per position or orientation target
     for (int t = 0; t < nt; ++t) {
       const double* e = xi + 8 * t;
-      const int kind = tkind[t];
+      const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
       if (tl == 0) {
         if (kind != BR_TARGET_ORIENTATION) {
           out[o + 0] = (float)(wpd * e[0]); out[o + 1] = (float)(wpd * e[1]); out[o + 2] = (float)(wpd * e[2]);
@@ -738,7 +740,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   tm.sync();
 }
 
-template <int T>
+template <int T, bool kGeneral>
 __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, int count, float* wsm, int lane) {
   const int team = lane / T;
   Team<T> tm;
@@ -748,10 +750,11 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
   const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T);
   if (team < count) {
     const int prob = P.b.order[first + team];
-    solve_problem<T>(P, tree, prob, wsm + team * L.total, tm);
+    solve_problem<T, kGeneral>(P, tree, prob, wsm + team * L.total, tm);
   }
 }
 
+template <bool kGeneral>
 __global__ void lm_solve_kernel(const LmParams P) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -766,7 +769,7 @@ __global__ void lm_solve_kernel(const LmParams P) {
     // One instantiation: 32-lane teams.  8- and 16-lane teams (several small problems per
     // warp) were measured slower on the mixed batch: three copies of this kernel body
     // overflow the instruction cache, and 32 lanes are the fastest per class on their own.
-    run_item<kLmTeam>(P, cls, first, count, wsm, lane);
+    run_item<kLmTeam, kGeneral>(P, cls, first, count, wsm, lane);
     __syncwarp();
   }
 }
@@ -822,14 +825,17 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     bytes = (size_t)wpc * warp_floats * sizeof(float);
   }
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  static int configured[16] = {0};
-  if ((int)bytes > configured[dev.device & 15]) {
-    cudaError_t e = cudaFuncSetAttribute(lm_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  const bool general = b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2;
+  auto kern = general ? lm_solve_kernel<true> : lm_solve_kernel<false>;
+  static int configured[2][16] = {};
+  int& have = configured[general][dev.device & 15];
+  if ((int)bytes > have) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return (int)e;
-    configured[dev.device & 15] = (int)bytes;
+    have = (int)bytes;
   }
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lm_solve_kernel, wpc * kWarp, bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpc * kWarp, bytes);
   if (per_sm < 1) per_sm = 1;
   const int64_t need = (b.n_items + wpc - 1) / wpc;
   const int64_t cap = (int64_t)per_sm * dev.sms;
@@ -837,7 +843,7 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
   cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int32_t), s);
   if (e != cudaSuccess) return (int)e;
-  lm_solve_kernel<<<grid, wpc * kWarp, bytes, s>>>(p);
+  kern<<<grid, wpc * kWarp, bytes, s>>>(p);
   return (int)cudaGetLastError();
 }
 
@@ -929,10 +935,12 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     bytes = (size_t)wpc * warp_floats * sizeof(float);
   }
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  cudaError_t e = cudaFuncSetAttribute(lm_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  auto kern = (b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2) ? lm_solve_kernel<true>
+                                                                            : lm_solve_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return (int)e;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lm_solve_kernel, wpc * kWarp, bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpc * kWarp, bytes);
   if (per_sm < 1) per_sm = 1;
   const int64_t want = (b.n_items + wpc - 1) / wpc;
   const int64_t cap = (int64_t)per_sm * dev.sms;
@@ -940,6 +948,6 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
   cudaStream_t s = (cudaStream_t)stream;
   e = cudaMemsetAsync(scratch, 0, (size_t)need, s);  // the queue counter must start at zero
   if (e != cudaSuccess) return (int)e;
-  lm_solve_kernel<<<grid, wpc * kWarp, bytes, s>>>(p);
+  kern<<<grid, wpc * kWarp, bytes, s>>>(p);
   return (int)cudaGetLastError();
 }
