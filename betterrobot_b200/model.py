@@ -25,6 +25,9 @@ REVOLUTE_KINDS = ("revolute_rx", "revolute_ry", "revolute_rz", "revolute_unalign
 PRISMATIC_KINDS = ("prismatic_px", "prismatic_py", "prismatic_pz", "prismatic_unaligned")
 FIXED_KINDS = ("universe", "fixed")
 FREE_FLYER_KIND = "free_flyer"
+# multi-slot kinds: (nq, nv) and neutral configuration (joint_models/*.py)
+MULTI_KINDS = {"spherical": (4, 3, (0.0, 0.0, 0.0, 1.0)), "planar": (4, 3, (0.0, 0.0, 1.0, 0.0)),
+               "revolute_unbounded": (2, 1, (1.0, 0.0)), "translation": (3, 3, (0.0, 0.0, 0.0))}
 
 _AXES = {
     "revolute_rx": (1.0, 0.0, 0.0), "revolute_ry": (0.0, 1.0, 0.0), "revolute_rz": (0.0, 0.0, 1.0),
@@ -46,6 +49,8 @@ class JointModel:
     def neutral(self) -> torch.Tensor:
         if self.kind == FREE_FLYER_KIND:
             return torch.tensor(IDENTITY_SE3)
+        if self.kind in MULTI_KINDS:
+            return torch.tensor(MULTI_KINDS[self.kind][2])
         return torch.zeros(self.nq)
 
 
@@ -55,6 +60,12 @@ def joint_model(kind: str, axis: Sequence[float] | None = None) -> JointModel:
         return JointModel(kind, 0, 0, None)
     if kind == FREE_FLYER_KIND:
         return JointModel(kind, 7, 6, None)
+    if kind in MULTI_KINDS:
+        nq, nv, _ = MULTI_KINDS[kind]
+        ax = None
+        if kind == "revolute_unbounded":  # axis defaults to z (revolute.py:195-198)
+            ax = torch.tensor([float(a) for a in (axis if axis is not None else (0.0, 0.0, 1.0))])
+        return JointModel(kind, nq, nv, ax)
     if kind in REVOLUTE_KINDS or kind in PRISMATIC_KINDS:
         if kind.endswith("unaligned"):
             if axis is None:
@@ -193,6 +204,11 @@ def build_model(name: str, joints: Sequence[dict], frames: Sequence[dict] = (),
         if jm.kind == FREE_FLYER_KIND:
             lower.extend([-inf] * 7)
             upper.extend([inf] * 7)
+        elif jm.kind in MULTI_KINDS:  # the limits build_model gives these kinds (io/build_model.py:382-408)
+            lo, hi = {"spherical": ([-1.0] * 4, [1.0] * 4), "planar": ([-inf, -inf, -1.0, -1.0], [inf, inf, 1.0, 1.0]),
+                      "revolute_unbounded": ([-inf] * 2, [inf] * 2), "translation": ([-inf] * 3, [inf] * 3)}[jm.kind]
+            lower.extend(lo)
+            upper.extend(hi)
         elif jm.nq == 1:
             lo = rec.get("lower")
             hi = rec.get("upper")

@@ -62,6 +62,26 @@ def dual_arm_spec(seed: int = 2, n: int = 7) -> dict:
     return {"name": "dual_arm", "joints": joints, "frames": frames}
 
 
+def mixed_spec(seed: int = 3) -> dict:
+    """A mobile manipulator using every multi-slot joint kind: fixed root, planar base,
+    3-DOF translation lift, revolute-z, spherical shoulder, revolute-y, unbounded wrist
+    (axis x); frames ``ee`` (wrist) and ``mid`` (shoulder)."""
+    rng = np.random.default_rng(seed)
+    kinds = [("planar", "mobile"), ("translation", "lift"), ("revolute_rz", "link1"), ("spherical", "link2"),
+             ("revolute_ry", "link3"), ("revolute_unbounded", "link4")]
+    joints = [{"name": "root_joint", "kind": "fixed", "parent": 0, "body": "base"}]
+    for i, (kind, body) in enumerate(kinds):
+        rec = {"name": f"j_{body}", "kind": kind, "parent": i + 1, "origin": _rand_pose(rng), "body": body}
+        if kind.startswith("revolute_r"):
+            rec.update(lower=-LIMIT, upper=LIMIT)
+        if kind == "revolute_unbounded":
+            rec["axis"] = (1.0, 0.0, 0.0)
+        joints.append(rec)
+    frames = [{"name": "ee", "parent": len(joints), "placement": _rand_pose(rng)},
+              {"name": "mid", "parent": 5, "placement": _rand_pose(rng)}]
+    return {"name": "mixed", "joints": joints, "frames": frames}
+
+
 HUMANOID_BRANCHES = (("lleg", 6), ("rleg", 6), ("larm", 7), ("rarm", 7), ("torso", 4))
 
 
@@ -112,6 +132,18 @@ def random_q(model: Model, batch: int, seed: int, rev_range: float = LIMIT,
             q[:, iq:iq + 3] = rng.uniform(-base_translation, base_translation, size=(batch, 3))
             quat = rng.normal(size=(batch, 4))
             q[:, iq + 3:iq + 7] = quat / np.linalg.norm(quat, axis=1, keepdims=True)
+        elif jm.kind == "spherical":
+            quat = rng.normal(size=(batch, 4))
+            q[:, iq:iq + 4] = quat / np.linalg.norm(quat, axis=1, keepdims=True)
+        elif jm.kind == "planar":
+            th = rng.uniform(-np.pi, np.pi, size=batch)
+            q[:, iq:iq + 2] = rng.uniform(-0.5, 0.5, size=(batch, 2))
+            q[:, iq + 2], q[:, iq + 3] = np.cos(th), np.sin(th)
+        elif jm.kind == "revolute_unbounded":
+            th = rng.uniform(-np.pi, np.pi, size=batch)
+            q[:, iq], q[:, iq + 1] = np.cos(th), np.sin(th)
+        elif jm.kind == "translation":
+            q[:, iq:iq + 3] = rng.uniform(-0.3, 0.3, size=(batch, 3))
         elif jm.nq == 1:
             q[:, iq] = rng.uniform(-rev_range, rev_range, size=batch)
     return torch.from_numpy(q)
@@ -146,6 +178,19 @@ def noisy_start(model: Model, q_star: torch.Tensor, sigma: float, seed: int) -> 
             s = np.where(th > 1e-12, np.sin(0.5 * th) / np.maximum(th, 1e-12), 0.5)
             dq = np.concatenate([s * w, np.cos(0.5 * th)], axis=1)
             q[:, iq + 3:iq + 7] = _quat_mul_np(q[:, iq + 3:iq + 7], dq)
+        elif jm.kind == "spherical":
+            w = rng.normal(0.0, sigma, size=(q.shape[0], 3))
+            th = np.linalg.norm(w, axis=1, keepdims=True)
+            s = np.where(th > 1e-12, np.sin(0.5 * th) / np.maximum(th, 1e-12), 0.5)
+            q[:, iq:iq + 4] = _quat_mul_np(q[:, iq:iq + 4], np.concatenate([s * w, np.cos(0.5 * th)], axis=1))
+        elif jm.kind in ("planar", "revolute_unbounded"):
+            k = iq + (2 if jm.kind == "planar" else 0)
+            th = np.arctan2(q[:, k + 1], q[:, k]) + rng.normal(0.0, sigma, size=q.shape[0])
+            q[:, k], q[:, k + 1] = np.cos(th), np.sin(th)
+            if jm.kind == "planar":
+                q[:, iq:iq + 2] += rng.normal(0.0, sigma / 3.0, size=(q.shape[0], 2))
+        elif jm.kind == "translation":
+            q[:, iq:iq + 3] += rng.normal(0.0, sigma / 3.0, size=(q.shape[0], 3))
         elif jm.nq == 1:
             q[:, iq] = np.clip(q[:, iq] + rng.normal(0.0, sigma, size=q.shape[0]), lo[iq], hi[iq])
     return torch.from_numpy(q)

@@ -1,8 +1,9 @@
 """Forward kinematics and Jacobians in float64 numpy — oracle only.
 
 Restates ``src/better_robot/kinematics/forward.py`` and
-``src/better_robot/kinematics/jacobian.py`` for the joint kinds the configs use
-(universe/fixed, revolute about any axis, prismatic, free-flyer).
+``src/better_robot/kinematics/jacobian.py`` for the joint kinds of
+``src/better_robot/data_model/joint_models/``: universe/fixed, revolute about any axis,
+revolute_unbounded, prismatic, free-flyer, spherical, planar, translation.
 """
 
 from __future__ import annotations
@@ -35,6 +36,21 @@ def joint_transform(jm, qj: np.ndarray) -> np.ndarray:
     """
     kind = jm.kind
     batch = qj.shape[:-1]
+    if kind == "revolute_unbounded":                  # revolute.py:206-211: angle = atan2(sin, cos)
+        a = axis_of(jm)
+        half = np.arctan2(qj[..., 1], qj[..., 0]) / 2.0
+        q = np.concatenate([np.sin(half)[..., None] * a, np.cos(half)[..., None]], -1)
+        return np.concatenate([np.zeros(batch + (3,)), q], -1)
+    if kind == "spherical":                           # spherical.py:22-32: rotation normalize(q)
+        return np.concatenate([np.zeros(batch + (3,)), lie.so3_normalize(qj)], -1)
+    if kind == "planar":                              # planar.py:20-41: half-angle from cos, sign of sin
+        c, s = qj[..., 2], qj[..., 3]
+        hc = np.sqrt(np.maximum((1.0 + c) / 2.0, 0.0))
+        hs = np.sqrt(np.maximum((1.0 - c) / 2.0, 0.0)) * np.sign(s)
+        z = np.zeros_like(c)
+        return np.stack([qj[..., 0], qj[..., 1], z, z, z, hs, hc], -1)
+    if kind == "translation":                         # translation.py:19-23
+        return np.concatenate([qj[..., :3], np.zeros(batch + (3,)), np.ones(batch + (1,))], -1)
     if kind.startswith("revolute"):
         a = axis_of(jm)
         half = qj[..., 0] / 2.0
@@ -87,8 +103,14 @@ def _joint_world_columns(model, oMi: np.ndarray, q: np.ndarray, j: int) -> np.nd
     T = oMi[..., j, :]
     p = T[..., :3]
     R = lie.quat_to_matrix(T[..., 3:7])
-    if jm.kind.startswith("revolute"):
+    if jm.kind.startswith("revolute"):               # incl. revolute_unbounded (revolute.py:213-216)
         S = np.zeros((6, 1)); S[3:, 0] = axis_of(jm)
+    elif jm.kind == "spherical":                     # spherical.py:34-41
+        S = np.zeros((6, 3)); S[3:, :] = np.eye(3)
+    elif jm.kind == "planar":                        # planar.py:43-50
+        S = np.zeros((6, 3)); S[0, 0] = 1.0; S[1, 1] = 1.0; S[5, 2] = 1.0
+    elif jm.kind == "translation":                   # translation.py:25-32
+        S = np.zeros((6, 3)); S[:3, :] = np.eye(3)
     elif jm.kind.startswith("prismatic"):
         S = np.zeros((6, 1)); S[:3, 0] = axis_of(jm)
     elif jm.kind == "free_flyer":
@@ -155,6 +177,14 @@ def integrate(model, q, v) -> np.ndarray:
         vj = v[..., iv:iv + jm.nv]
         if jm.kind == "free_flyer":
             parts.append(lie.se3_normalize(lie.se3_compose(qj, lie.se3_exp(vj))))
+        elif jm.kind == "spherical":                 # spherical.py:52-56
+            parts.append(lie.so3_normalize(lie.quat_mul(qj, lie.so3_exp(vj))))
+        elif jm.kind == "revolute_unbounded":        # revolute.py:223-231
+            th = np.arctan2(qj[..., 1], qj[..., 0]) + vj[..., 0]
+            parts.append(np.stack([np.cos(th), np.sin(th)], -1))
+        elif jm.kind == "planar":                    # planar.py:61-68
+            th = np.arctan2(qj[..., 3], qj[..., 2]) + vj[..., 2]
+            parts.append(np.stack([qj[..., 0] + vj[..., 0], qj[..., 1] + vj[..., 1], np.cos(th), np.sin(th)], -1))
         else:
             parts.append(qj + vj)
     return np.concatenate(parts, -1) if parts else q.copy()
@@ -173,6 +203,13 @@ def difference(model, q0, q1) -> np.ndarray:
         b = q1[..., iq:iq + jm.nq]
         if jm.kind == "free_flyer":
             parts.append(lie.se3_log(lie.se3_compose(lie.se3_inverse(a), b)))
+        elif jm.kind == "spherical":                 # spherical.py:58-62
+            parts.append(lie.so3_log(lie.so3_normalize(lie.quat_mul(lie.so3_inverse(a), b))))
+        elif jm.kind == "revolute_unbounded":        # revolute.py:233-237
+            parts.append((np.arctan2(b[..., 1], b[..., 0]) - np.arctan2(a[..., 1], a[..., 0]))[..., None])
+        elif jm.kind == "planar":                    # planar.py:70-76
+            parts.append(np.stack([b[..., 0] - a[..., 0], b[..., 1] - a[..., 1],
+                                   np.arctan2(b[..., 3], b[..., 2]) - np.arctan2(a[..., 3], a[..., 2])], -1))
         else:
             parts.append(b - a)
     return np.concatenate(parts, -1)

@@ -57,9 +57,20 @@ def reference_model(spec):
                 b.add_free_flyer_root(rec["name"], child=rec["body"], origin=origin)
             continue  # fixed root: build_model inserts "root_joint" itself
         parent_body = bodies[rec["parent"]]
+        kw = dict(parent=parent_body, child=rec["body"], origin=origin)
         if rec["kind"] == "revolute_rz":
-            b.add_revolute_z(rec["name"], parent=parent_body, child=rec["body"], origin=origin,
-                             lower=rec["lower"], upper=rec["upper"])
+            b.add_revolute_z(rec["name"], lower=rec["lower"], upper=rec["upper"], **kw)
+        elif rec["kind"] == "revolute_ry":
+            b.add_revolute_y(rec["name"], lower=rec["lower"], upper=rec["upper"], **kw)
+        elif rec["kind"] == "revolute_unbounded":
+            b.add_revolute(rec["name"], axis=torch.tensor(rec["axis"], dtype=D), unbounded=True, **kw)
+        elif rec["kind"] == "spherical":
+            b.add_spherical(rec["name"], **kw)
+        elif rec["kind"] == "planar":
+            b.add_planar(rec["name"], **kw)
+        elif rec["kind"] == "translation":
+            from better_robot.data_model.joint_models.translation import JointTranslation
+            b.add_joint(rec["name"], kind=JointTranslation(), **kw)
         else:
             raise NotImplementedError(rec["kind"])
     for fr in spec["frames"]:
@@ -155,7 +166,12 @@ def make_kin(name, spec, batch, seed, base_t, out):
         Js[ref] = torch.stack([get_frame_jacobian(m, data, f, reference=ref) for f in sel], -3).numpy()
     data2 = forward_kinematics(m, q)
     compute_joint_jacobians(m, data2)
+    # Model.integrate / Model.difference (data_model/model.py:160-190) on the same configurations
+    v = torch.from_numpy(np.random.default_rng(seed + 50).normal(0.0, 0.4, size=(batch, m.nv)))
+    q1 = syn.noisy_start(mine, q, 0.3, seed + 51)
     np.savez_compressed(out, q=q.numpy(), oMi=data.joint_pose_world.numpy(), liMi=data.joint_pose_local.numpy(),
+                        v=v.numpy(), q1=q1.numpy(), integrate=m.integrate(q, v).numpy(),
+                        difference=m.difference(q, q1).numpy(),
                         oMf=data.frame_pose_world.numpy(), frame_ids=np.array(sel),
                         J_world=Js["world"], J_lwa=Js["local_world_aligned"], J_local=Js["local"],
                         joint_jacobians=data2.joint_jacobians.numpy(), **topology_arrays(m))
@@ -336,6 +352,7 @@ def main():
     make_kin("chain7", chain, 16, 5, 0.0, os.path.join(HERE, "kin_chain7.npz"))
     make_kin("humanoid", hum, 8, 6, 1.0, os.path.join(HERE, "kin_humanoid.npz"))
     make_kin("dual_arm", dual, 8, 7, 0.0, os.path.join(HERE, "kin_dual_arm.npz"))
+    make_kin("mixed", syn.mixed_spec(), 16, 8, 0.0, os.path.join(HERE, "kin_mixed.npz"))
     lm = dict(lam0=1e-3, factor=10.0, tol=1e-6)
     make_ik("chain7_random", chain, ["ee"], 8, 21, "random", os.path.join(HERE, "ik_chain7_random.npz"),
             max_iter=50, **lm)
@@ -347,6 +364,8 @@ def main():
             os.path.join(HERE, "ik_humanoid.npz"), max_iter=100, rest_w=1e-3, **lm)
     make_ik_kernels(chain, dual, hum, lm)
     make_ik_kinds(chain, dual, hum, lm)
+    make_ik("mixed", syn.mixed_spec(), ["ee", "mid"], 6, 32, "noisy", os.path.join(HERE, "ik_mixed.npz"),
+            max_iter=100, rest_w=1e-3, **lm)
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
 

@@ -11,7 +11,8 @@ from oracle import ik, kinematics as K, lie
 
 from conftest import GOLDEN
 
-SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec()}
+SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec(),
+         "mixed": syn.mixed_spec()}
 
 
 def _load(name):
@@ -48,6 +49,8 @@ def test_fk_frames_jacobians_match_reference(robot):
         J = np.stack([K.frame_jacobian(m, oMi, g["q"], int(f), ref) for f in g["frame_ids"]], -3)
         np.testing.assert_allclose(J, g[key], atol=1e-12, rtol=0)
     np.testing.assert_allclose(K.compute_joint_jacobians(m, oMi, g["q"]), g["joint_jacobians"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(K.integrate(m, g["q"], g["v"]), g["integrate"], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(K.difference(m, g["q"], g["q1"]), g["difference"], atol=1e-12, rtol=0)
 
 
 def test_lie_matches_reference():
@@ -64,7 +67,7 @@ def test_lie_matches_reference():
                                         ("chain7_huber", "chain7"), ("chain7_gn_cauchy", "chain7"),
                                         ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid"),
                                         ("chain7_position", "chain7"), ("dual_arm_mixed", "dual_arm"),
-                                        ("humanoid_mixed", "humanoid")])
+                                        ("humanoid_mixed", "humanoid"), ("mixed", "mixed")])
 def test_lm_gn_match_reference_solver(case, robot):
     g = _load(f"ik_{case}.npz")
     m = syn.model_from_spec(SPECS[robot], dtype=torch.float64)
