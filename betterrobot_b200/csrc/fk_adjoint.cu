@@ -291,12 +291,19 @@ static int fill_loss(const br_tree_t* tree, LossParams& p, const int32_t* frame_
 
 using namespace br;
 
+// Joint kinds whose raw-q chain rule the backward implements (revolute, prismatic, free-flyer).
+static bool adjoint_kinds_ok(const br_tree_t* t) {
+  const int ok = (1 << BR_JOINT_FIXED) | (1 << BR_JOINT_REVOLUTE) | (1 << BR_JOINT_PRISMATIC) | (1 << BR_JOINT_FREE_FLYER);
+  return t && t->kinds != 0 && (t->kinds & ~ok) == 0;
+}
+
 extern "C" int br_pose_loss(const br_tree_t* tree, const float* q, int64_t batch, const int32_t* frame_ids,
                             int32_t n_frames, const float* targets, const float* weights,
                             int32_t weights_per_config, float* loss, float* joint_pose_world, void* stream) {
   LossParams p = {};
   int st = fill_loss(tree, p, frame_ids, n_frames);
   if (st) return st;
+  if (!adjoint_kinds_ok(tree)) return BR_EINVAL;
   if (batch < 0 || (batch > 0 && (!q || !targets || !weights || !loss))) return BR_EINVAL;
   p.q = q; p.targets = targets; p.weights = weights; p.loss = loss; p.oMi_out = joint_pose_world;
   p.batch = batch; p.weights_per_config = weights_per_config != 0;
@@ -310,6 +317,7 @@ extern "C" int br_pose_loss_backward(const br_tree_t* tree, const float* q, cons
   LossParams p = {};
   int st = fill_loss(tree, p, frame_ids, n_frames);
   if (st) return st;
+  if (!adjoint_kinds_ok(tree)) return BR_EINVAL;
   if (batch < 0 || (batch > 0 && (!q || !targets || !weights || !grad_loss || !grad_q))) return BR_EINVAL;
   p.q = q; p.oMi_in = joint_pose_world; p.targets = targets; p.weights = weights;
   p.grad_loss = grad_loss; p.grad_q = grad_q; p.batch = batch; p.weights_per_config = weights_per_config != 0;

@@ -1,16 +1,20 @@
 // joint_ops.cu — batched configuration-space retraction and difference.
 //
 // integrate:  q' = q (+) v   (Model.integrate, src/better_robot/data_model/model.py:160-174):
-//   revolute / prismatic  q' = q + v                     (revolute.py:46-48)
+//   revolute / prismatic / translation  q' = q + v       (revolute.py:46-48, translation.py:40-41)
 //   free-flyer            q' = normalize(q * exp(v))     (free_flyer.py:47-51)
+//   spherical             q' = normalize(q * exp(v))     (spherical.py:52-56)
+//   planar, unbounded     theta' = atan2(sin, cos) + v   (planar.py:61-68, revolute.py:223-231)
 // difference: v = q1 (-) q0  (Model.difference, model.py:176-190):
-//   revolute / prismatic  v = q1 - q0                    (revolute.py:51-53)
+//   revolute / prismatic / translation  v = q1 - q0      (revolute.py:51-53)
 //   free-flyer            v = log(q0^-1 * q1)            (free_flyer.py:53-57)
+//   spherical             v = log(normalize(q0^-1 q1))   (spherical.py:58-62)
+//   planar, unbounded     atan2(q1) - atan2(q0)          (planar.py:70-76, revolute.py:233-237)
 //
 // Layout: a warp owns a tile of 32 consecutive configurations.  Their rows of every
 // input are one contiguous slab, copied into the warp's shared memory with 16-byte
-// cp.async copies (all of a tile's copies in flight at once); free-flyer slots are then
-// computed one configuration per lane (the float64 exp / log runs on 32 lanes at once),
+// cp.async copies (all of a tile's copies in flight at once); the slots of the other kinds
+// (free-flyer, spherical, planar, unbounded) are then computed one configuration per lane (the float64 exp / log runs on 32 lanes at once),
 // and the output slab is written with float4 stores, each lane producing 4 consecutive
 // outputs.  Memory bound: 4 * (nq + nv + nq) bytes per configuration for integrate,
 // 4 * (nq + nq + nv) for difference.  Pointers that are not 16-byte aligned take the
@@ -19,6 +23,7 @@
 #include <stdint.h>
 
 #include "br_common.cuh"
+#include "br_fk.cuh"
 #include "br_lie.cuh"
 
 namespace br {
@@ -61,8 +66,9 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
   extern __shared__ __align__(16) float slabs[];
   __shared__ int16_t vmap[BR_MAX_NQ];     // q slot -> v slot of a 1:1 joint, -1 for other slots
   __shared__ int16_t qmap[BR_MAX_NV];     // v slot -> q slot of a 1:1 joint, -1 for other slots
-  __shared__ int16_t ffq[BR_MAX_JOINTS];  // free-flyer q / v offsets
-  __shared__ int16_t ffv[BR_MAX_JOINTS];
+  __shared__ int16_t ffq[BR_MAX_JOINTS];  // q / v offsets and kind of the joints handled per lane
+  __shared__ int16_t ffv[BR_MAX_JOINTS];   // (free-flyer, spherical, planar, unbounded revolute)
+  __shared__ int8_t ffk[BR_MAX_JOINTS];
   __shared__ int nff;
   const int nq = tree.nq, nv = tree.nv;
   for (int k = threadIdx.x; k < nq; k += blockDim.x) vmap[k] = -1;
@@ -72,13 +78,17 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
   for (int i = threadIdx.x; i < p.n_active; i += blockDim.x) {
     const int j = active[i];
     const int iq = tree.idx_q[j], iv = tree.idx_v[j];
-    if (tree.jtype[j] == BR_JOINT_FREE_FLYER) {
+    const int jt = tree.jtype[j];
+    if (joint_is_vector(jt)) {
+      for (int k = 0; k < joint_nv(jt); ++k) {
+        vmap[iq + k] = (int16_t)(iv + k);
+        qmap[iv + k] = (int16_t)(iq + k);
+      }
+    } else {
       const int s = atomicAdd(&nff, 1);
       ffq[s] = (int16_t)iq;
       ffv[s] = (int16_t)iv;
-    } else {
-      vmap[iq] = (int16_t)iv;
-      qmap[iv] = (int16_t)iq;
+      ffk[s] = (int8_t)jt;
     }
   }
   __syncthreads();
@@ -102,20 +112,51 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
     __syncwarp();
     if (lane < cnt) {
       for (int f = 0; f < n_ff; ++f) {
-        const int iq = ffq[f], iv = ffv[f];
+        const int iq = ffq[f], iv = ffv[f], jt = ffk[f];
         float* qa = A + lane * nq + iq;
         if (!diff) {
           const float* v = Bs + lane * nv + iv;
-          DPose n = dcompose(dpose7(qa), dse3_exp(d3(v[0], v[1], v[2]), d3(v[3], v[4], v[5])));
-          n.q = dqnormalize(n.q);
-          qa[0] = (float)n.t.x; qa[1] = (float)n.t.y; qa[2] = (float)n.t.z;
-          qa[3] = (float)n.q.x; qa[4] = (float)n.q.y; qa[5] = (float)n.q.z; qa[6] = (float)n.q.w;
+          if (jt == BR_JOINT_FREE_FLYER) {
+            DPose n = dcompose(dpose7(qa), dse3_exp(d3(v[0], v[1], v[2]), d3(v[3], v[4], v[5])));
+            n.q = dqnormalize(n.q);
+            qa[0] = (float)n.t.x; qa[1] = (float)n.t.y; qa[2] = (float)n.t.z;
+            qa[3] = (float)n.q.x; qa[4] = (float)n.q.y; qa[5] = (float)n.q.z; qa[6] = (float)n.q.w;
+          } else if (jt == BR_JOINT_SPHERICAL) {  // normalize(q * exp(v)), spherical.py:52-56
+            const double4 n = dqnormalize(dqmul(make_double4(qa[0], qa[1], qa[2], qa[3]),
+                                                dse3_exp(d3(0.0, 0.0, 0.0), d3(v[0], v[1], v[2])).q));
+            qa[0] = (float)n.x; qa[1] = (float)n.y; qa[2] = (float)n.z; qa[3] = (float)n.w;
+          } else {                                // planar.py:61-68, revolute.py:223-231
+            const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
+            double s, c;
+            sincos(atan2((double)qa[k + 1], (double)qa[k]) + (double)v[k], &s, &c);
+            if (jt == BR_JOINT_PLANAR) {
+              qa[0] = qa[0] + v[0];
+              qa[1] = qa[1] + v[1];
+            }
+            qa[k] = (float)c;
+            qa[k + 1] = (float)s;
+          }
         } else {
-          double3 v, w;
-          dse3_log(dcompose(dinverse(dpose7(qa)), dpose7(Bs + lane * nq + iq)), v, w);
+          const float* qb = Bs + lane * nq + iq;
           float* o = O + lane * nv + iv;
-          o[0] = (float)v.x; o[1] = (float)v.y; o[2] = (float)v.z;
-          o[3] = (float)w.x; o[4] = (float)w.y; o[5] = (float)w.z;
+          if (jt == BR_JOINT_FREE_FLYER) {
+            double3 v, w;
+            dse3_log(dcompose(dinverse(dpose7(qa)), dpose7(qb)), v, w);
+            o[0] = (float)v.x; o[1] = (float)v.y; o[2] = (float)v.z;
+            o[3] = (float)w.x; o[4] = (float)w.y; o[5] = (float)w.z;
+          } else if (jt == BR_JOINT_SPHERICAL) {  // log(normalize(q0^-1 q1)), spherical.py:58-62
+            const double3 w = dso3_log(dqnormalize(dqmul(dqconj(make_double4(qa[0], qa[1], qa[2], qa[3])),
+                                                         make_double4(qb[0], qb[1], qb[2], qb[3]))));
+            o[0] = (float)w.x; o[1] = (float)w.y; o[2] = (float)w.z;
+          } else {                                // planar.py:70-76, revolute.py:233-237
+            const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
+            const double dth = atan2((double)qb[k + 1], (double)qb[k]) - atan2((double)qa[k + 1], (double)qa[k]);
+            if (jt == BR_JOINT_PLANAR) {
+              o[0] = qb[0] - qa[0];
+              o[1] = qb[1] - qa[1];
+            }
+            o[k] = (float)dth;
+          }
         }
       }
     }

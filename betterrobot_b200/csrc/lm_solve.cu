@@ -35,6 +35,7 @@
 
 #include "../../include/br_b200.h"
 #include "br_common.cuh"
+#include "br_fk.cuh"
 #include "br_lie.cuh"
 
 namespace br {
@@ -272,7 +273,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       const int pj = parent[j];
       const int prev = pj >= 0 ? lastd[pj] : -1;
       const int jt = jtype[j];
-      const int nvj = jt == BR_JOINT_FREE_FLYER ? 6 : (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) ? 1 : 0;
+      const int nvj = joint_nv(jt);
       for (int k = 0; k < nvj; ++k) dpar[idxv[j] + k] = (signed char)(k == 0 ? prev : idxv[j] + k - 1);
       lastd[j] = nvj ? idxv[j] + nvj - 1 : prev;
     }
@@ -311,19 +312,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // float64 FK of configuration q (shared) -> world poses (returned buffer), pointer jumping.
   auto fk = [&](const double* q) -> double* {
     for (int j = tl; j < nj; j += T) {
-      const DPose Pj = to_d(ld8(place + 8 * j));
-      DPose Lj = Pj;
-      const int jt = jtype[j];
-      const double* qv = q + idxq[j];
-      if (jt == BR_JOINT_REVOLUTE) {                                  // revolute.py:18-21
-        double s, c;
-        sincos(0.5 * qv[0], &s, &c);
-        Lj.q = dqmul(Pj.q, make_double4(s * axis[4 * j], s * axis[4 * j + 1], s * axis[4 * j + 2], c));
-      } else if (jt == BR_JOINT_PRISMATIC) {
-        Lj.t = dadd(Pj.t, dqrot(Pj.q, d3(qv[0] * axis[4 * j], qv[0] * axis[4 * j + 1], qv[0] * axis[4 * j + 2])));
-      } else if (jt == BR_JOINT_FREE_FLYER) {                         // free_flyer.py:31-36
-        Lj = dcompose(Pj, DPose{d3(qv[0], qv[1], qv[2]), dqnormalize(make_double4(qv[3], qv[4], qv[5], qv[6]))});
-      }
+      const DPose Lj = dlocal_transform(jtype[j], to_d(ld8(place + 8 * j)), axis + 4 * j, q + idxq[j]);
       sts(poseA, nj, j, Lj);
       ancA[j] = parent[j];
     }
@@ -384,10 +373,29 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       for (int j = tl; j < nj; j += T) {
         const int jt = jtype[j];
         const int iq = idxq[j], iv = idxv[j];
-        if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
-          const double dd = q[iq] - qrest[iq];
-          dr[iv] = dd;
-          acc += wrd * wrd * dd * dd;
+        if (joint_is_vector(jt)) {
+          for (int k = 0; k < joint_nv(jt); ++k) {
+            const double dd = q[iq + k] - qrest[iq + k];
+            dr[iv + k] = dd;
+            acc += wrd * wrd * dd * dd;
+          }
+        } else if (jt == BR_JOINT_SPHERICAL) {                       // spherical.py:58-62
+          const double3 w = dso3_log(dqnormalize(dqmul(
+              dqconj(make_double4(qrest[iq], qrest[iq + 1], qrest[iq + 2], qrest[iq + 3])),
+              make_double4(q[iq], q[iq + 1], q[iq + 2], q[iq + 3]))));
+          dr[iv] = w.x; dr[iv + 1] = w.y; dr[iv + 2] = w.z;
+          acc += wrd * wrd * ddot(w, w);
+        } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {  // planar.py:70-76, revolute.py:233-237
+          const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
+          const double dth = atan2(q[iq + k + 1], q[iq + k]) - atan2(qrest[iq + k + 1], qrest[iq + k]);
+          if (jt == BR_JOINT_PLANAR) {
+            const double dx = q[iq] - qrest[iq], dy = q[iq + 1] - qrest[iq + 1];
+            dr[iv] = dx; dr[iv + 1] = dy; dr[iv + 2] = dth;
+            acc += wrd * wrd * (dx * dx + dy * dy + dth * dth);
+          } else {
+            dr[iv] = dth;
+            acc += wrd * wrd * dth * dth;
+          }
         } else if (jt == BR_JOINT_FREE_FLYER) {                      // free_flyer.py:53-57
           const DPose a{d3(qrest[iq], qrest[iq + 1], qrest[iq + 2]),
                         make_double4(qrest[iq + 3], qrest[iq + 4], qrest[iq + 5], qrest[iq + 6])};
@@ -521,8 +529,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       }
       if (use_limits) {
         const int j = cjoint[c];
-        if (jtype[j] == BR_JOINT_REVOLUTE || jtype[j] == BR_JOINT_PRISMATIC) {
-          const int iq = idxq[j];
+        if (joint_is_vector(jtype[j])) {  // nq == nv: +-w on active rows; other kinds give zero rows (limits.py:42-54)
+          const int iq = idxq[j] + (c - idxv[j]);
           if (q[iq] < (double)lower[iq]) {
             const double d = (double)lower[iq] - q[iq];
             const float w = irls_weight(S.kernel, kc, wld * wld * d * d);
@@ -638,8 +646,24 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     for (int j = tl; j < nj; j += T) {
       const int jt = jtype[j];
       const int iq = idxq[j], iv = idxv[j];
-      if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
-        xn[iq] = fmin(fmax(x[iq] + (double)delta[iv], (double)lower[iq]), (double)upper[iq]);
+      auto clampq = [&](int k, double v) { xn[iq + k] = fmin(fmax(v, (double)lower[iq + k]), (double)upper[iq + k]); };
+      if (joint_is_vector(jt)) {
+        for (int k = 0; k < joint_nv(jt); ++k) clampq(k, x[iq + k] + (double)delta[iv + k]);
+      } else if (jt == BR_JOINT_SPHERICAL) {                         // spherical.py:52-56
+        const double4 n = dqnormalize(dqmul(make_double4(x[iq], x[iq + 1], x[iq + 2], x[iq + 3]),
+                                            dse3_exp(d3(0.0, 0.0, 0.0), d3(delta[iv], delta[iv + 1], delta[iv + 2])).q));
+        clampq(0, n.x); clampq(1, n.y); clampq(2, n.z); clampq(3, n.w);
+      } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {  // planar.py:61-68, revolute.py:223-231
+        const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
+        const double th = atan2(x[iq + k + 1], x[iq + k]) + (double)delta[iv + k];
+        double s, c;
+        sincos(th, &s, &c);
+        if (jt == BR_JOINT_PLANAR) {
+          clampq(0, x[iq] + (double)delta[iv]);
+          clampq(1, x[iq + 1] + (double)delta[iv + 1]);
+        }
+        clampq(k, c);
+        clampq(k + 1, s);
       } else if (jt == BR_JOINT_FREE_FLYER) {                        // free_flyer.py:47-51
         const DPose a{d3(x[iq], x[iq + 1], x[iq + 2]), make_double4(x[iq + 3], x[iq + 4], x[iq + 5], x[iq + 6])};
         DPose n = dcompose(a, dse3_exp(d3(delta[iv], delta[iv + 1], delta[iv + 2]),
@@ -722,13 +746,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       }
       o += kind == BR_TARGET_POSE ? 6 : 3;
     }
-    if (use_limits) {
+    if (use_limits) {  // the limit and rest rows keep their place when their weight is 0
       for (int i = tl; i < nq; i += T) {
         out[o + i] = (float)(wld * fmax((double)lower[i] - x[i], 0.0));
         out[o + nq + i] = (float)(wld * fmax(x[i] - (double)upper[i], 0.0));
       }
-      o += 2 * nq;
     }
+    o += 2 * nq;
     if (use_rest)
       for (int c = tl; c < nv; c += T) out[o + c] = (float)(wrd * dr[c]);
   }

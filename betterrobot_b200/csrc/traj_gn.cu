@@ -172,15 +172,9 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     const double* q = xs + t * nv;
     for (int j = lane; j < nj; j += kWarp) {
       const Pose Pj = load_pose8(place + 8 * j);
-      DPose Lj{d3(Pj.t.x, Pj.t.y, Pj.t.z), make_double4(Pj.q.x, Pj.q.y, Pj.q.z, Pj.q.w)};
-      if (jtype[j] == BR_JOINT_REVOLUTE) {
-        double s, co;
-        sincos(0.5 * q[idxq[j]], &s, &co);
-        Lj.q = dqmul(Lj.q, make_double4(s * axis[4 * j], s * axis[4 * j + 1], s * axis[4 * j + 2], co));
-      } else if (jtype[j] == BR_JOINT_PRISMATIC) {
-        const double d = q[idxq[j]];
-        Lj.t = dadd(Lj.t, dqrot(Lj.q, d3(d * axis[4 * j], d * axis[4 * j + 1], d * axis[4 * j + 2])));
-      }
+      const DPose Lj = dlocal_transform(jtype[j], DPose{d3(Pj.t.x, Pj.t.y, Pj.t.z),
+                                                        make_double4(Pj.q.x, Pj.q.y, Pj.q.z, Pj.q.w)},
+                                        axis + 4 * j, q + idxq[j]);
       std8d(pA + 8 * j, Lj);
       ancA[j] = parent[j];
     }
@@ -499,6 +493,11 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
   if (!settings || n_traj < 0 || knots < 3) return BR_EINVAL;
   if (knots > BR_MAX_TRAJ_KNOTS || tree->nv > BR_MAX_TRAJ_NV) return BR_ETOOBIG;
   if (tree->nq != tree->nv) return BR_EINVAL;  // fixed-base trees: difference(q0, q1) = q1 - q0
+  {
+    const int ok = (1 << BR_JOINT_FIXED) | (1 << BR_JOINT_REVOLUTE) | (1 << BR_JOINT_PRISMATIC) |
+                   (1 << BR_JOINT_TRANSLATION);
+    if (tree->kinds == 0 || (tree->kinds & ~ok)) return BR_EINVAL;  // q + v kinds only
+  }
   if (frame_id < 0 || frame_id >= tree->nframes) return BR_EINVAL;
   if (n_traj == 0) return BR_OK;
   if (!x0 || !goal || !x || !iters || !status || !cost) return BR_EINVAL;

@@ -241,7 +241,8 @@ class PackedIK:
         self.iters = torch.empty(self.P, dtype=torch.int32, device=dev)
         self.status = torch.empty(self.P, dtype=torch.int32, device=dev)
         self.cost = torch.empty(self.P, device=dev)
-        self.residual = torch.empty(int(rdim.sum()), device=dev) if with_residual else None
+        # fixed layout per problem: target rows, 2 nq limit rows, nv rest rows (zero when unused)
+        self.residual = torch.zeros(int(rdim.sum()), device=dev) if with_residual else None
         self.scratch = torch.zeros(SCRATCH_BYTES // 4, dtype=torch.int32, device=dev)
         # ctypes structs (kept alive on the object)
         self._trees = (BrTree * self.C)(*[t.struct for t in self.trees])
@@ -341,8 +342,18 @@ def solve_ik_batched(model, frame_ids, targets: torch.Tensor, initial_q: torch.T
         pk.solve(settings_from(cost_cfg, optimizer_cfg))
     res = None
     if with_residual:
-        res = (pk.residual.view(P, -1) if (pk.r_dim == pk.r_dim[0]).all()
-               else list(torch.split(pk.residual, [int(d) for d in pk.r_dim])))
+        # the reference's CostStack has a limit / rest block only when its weight is > 0
+        # (tasks/ik.py:200-205): drop the unused blocks of the fixed device layout
+        def stack_rows(r: torch.Tensor) -> torch.Tensor:
+            nt_rows = r.shape[-1] - 2 * model.nq - model.nv
+            parts = [r[..., :nt_rows]]
+            if cost_cfg.limit_weight > 0.0:
+                parts.append(r[..., nt_rows:nt_rows + 2 * model.nq])
+            if cost_cfg.rest_weight > 0.0:
+                parts.append(r[..., nt_rows + 2 * model.nq:])
+            return torch.cat(parts, -1) if len(parts) > 1 else parts[0]
+        res = (stack_rows(pk.residual.view(P, -1)) if (pk.r_dim == pk.r_dim[0]).all()
+               else [stack_rows(r) for r in torch.split(pk.residual, [int(d) for d in pk.r_dim])])
     return BatchIKResult(q=pk.q_of(0), iters=pk.iters, converged=(pk.status & 0xFF) == 0, status=pk.status,
                          cost=pk.cost, residual=res)
 

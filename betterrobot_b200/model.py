@@ -92,6 +92,8 @@ def joint_axis(jm) -> tuple[float, float, float]:
     if kind in _AXES:
         return _AXES[kind]
     ax = getattr(jm, "axis", None)
+    if ax is None and kind == "revolute_unbounded":
+        return (0.0, 0.0, 1.0)
     if ax is None:
         return (0.0, 0.0, 0.0)
     ax = ax.detach().cpu().double().reshape(-1).tolist()

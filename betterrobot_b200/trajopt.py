@@ -17,7 +17,7 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib
-from .exceptions import ShapeError
+from .exceptions import UnsupportedJointError, ShapeError
 from .tree import device_tree
 
 
@@ -63,6 +63,11 @@ def solve_trajopt_batched(model, frame_id: int, goal: torch.Tensor, initial_q_tr
                           start: torch.Tensor | None = None, q_ref: torch.Tensor | None = None,
                           cfg: TrajOptConfig | None = None, want_goal_grad: bool = True) -> BatchTrajResult:
     """``initial_q_traj (N, T, nq)``, ``goal (N, 7)`` (and ``start (N, 7)``) float32 CUDA tensors."""
+    bad = [jm.kind for jm in model.joint_models
+           if not (jm.kind in ("universe", "fixed", "translation") or jm.kind.startswith("prismatic")
+                   or (jm.kind.startswith("revolute") and jm.kind != "revolute_unbounded"))]
+    if bad:
+        raise UnsupportedJointError(f"trajopt: the knot stack needs q + v joints; got {sorted(set(bad))}")
     cfg = cfg or TrajOptConfig()
     if initial_q_traj.dim() != 3 or initial_q_traj.shape[-1] != model.nq:
         raise ShapeError(f"initial_q_traj must be (N, T, {model.nq}), got {tuple(initial_q_traj.shape)}")

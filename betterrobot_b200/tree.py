@@ -19,6 +19,14 @@ from .exceptions import ModelInconsistencyError, UnsupportedJointError
 from .model import FIXED_KINDS, FREE_FLYER_KIND, PRISMATIC_KINDS, REVOLUTE_KINDS, joint_axis
 
 JOINT_FIXED, JOINT_REVOLUTE, JOINT_PRISMATIC, JOINT_FREE_FLYER = 0, 1, 2, 3
+JOINT_SPHERICAL, JOINT_PLANAR, JOINT_REVOLUTE_UNBOUNDED, JOINT_TRANSLATION = 4, 5, 6, 7
+# tangent columns of the multi-slot kinds in the joint frame: (col_kind 0 = rotation about,
+# 1 = translation along, axis) — the motion subspaces of joint_models/{spherical,planar,translation}.py
+_MULTI_COLUMNS = {
+    "spherical": (JOINT_SPHERICAL, [(0, 0), (0, 1), (0, 2)]),
+    "planar": (JOINT_PLANAR, [(1, 0), (1, 1), (0, 2)]),
+    "translation": (JOINT_TRANSLATION, [(1, 0), (1, 1), (1, 2)]),
+}
 MAX_JOINTS, MAX_NV, MAX_NQ = 64, 64, 128
 
 
@@ -66,6 +74,19 @@ class TreeArrays:
                 self.col_joint[iv] = j
                 self.col_kind[iv] = 0 if rev else 1
                 self.col_axis[iv, :3] = a
+            elif kind == "revolute_unbounded":
+                self.jtype[j] = JOINT_REVOLUTE_UNBOUNDED
+                a = joint_axis(jm)
+                self.axis[j, :3] = a
+                self.col_joint[iv] = j
+                self.col_kind[iv] = 0
+                self.col_axis[iv, :3] = a
+            elif kind in _MULTI_COLUMNS:
+                self.jtype[j], cols = _MULTI_COLUMNS[kind]
+                for k, (ck, ax) in enumerate(cols):
+                    self.col_joint[iv + k] = j
+                    self.col_kind[iv + k] = ck
+                    self.col_axis[iv + k, ax] = 1.0
             elif kind == FREE_FLYER_KIND:
                 self.jtype[j] = JOINT_FREE_FLYER
                 for k in range(6):
@@ -132,6 +153,7 @@ class DeviceTree:
         a = self.arrays
         st = BrTree()
         st.njoints, st.nq, st.nv, st.nframes, st.rounds = a.nj, a.nq, a.nv, a.nf, a.rounds
+        st.kinds = int(np.bitwise_or.reduce(np.left_shift(1, a.jtype.astype(np.int64))))
         for name, _ in a.sections():
             setattr(st, name, base + offs[name])
         self.struct = st

@@ -46,6 +46,11 @@ extern "C" {
 #define BR_JOINT_REVOLUTE 1     /* revolute_rx/ry/rz/unaligned: rotation about axis */
 #define BR_JOINT_PRISMATIC 2    /* prismatic_px/py/pz/unaligned: translation along axis */
 #define BR_JOINT_FREE_FLYER 3   /* nq = 7 [t, quat], nv = 6, transform = normalize(q) */
+#define BR_JOINT_SPHERICAL 4    /* nq = 4 quat, nv = 3: rotation normalize(q) (spherical.py:22-32) */
+#define BR_JOINT_PLANAR 5       /* nq = 4 [x, y, cos, sin], nv = 3 (planar.py:20-41)          */
+#define BR_JOINT_REVOLUTE_UNBOUNDED 6 /* nq = 2 [cos, sin], nv = 1: rotation by atan2 about axis
+                                         (revolute.py:192-243)                                */
+#define BR_JOINT_TRANSLATION 7  /* nq = nv = 3: translation by q (translation.py:19-23)       */
 
 /* ---- Jacobian reference frames (kinematics/__init__.py:24-37) --------- */
 #define BR_REF_WORLD 0
@@ -62,7 +67,10 @@ extern "C" {
 typedef struct br_tree {
     int32_t njoints, nq, nv, nframes;
     int32_t rounds;           /* ceil(log2(max joint depth)): pointer-jumping rounds */
-    int32_t reserved[3];
+    int32_t kinds;            /* bit k set if some joint has kind BR_JOINT_k; entry points
+                                 that support only some kinds (the FK adjoint, trajectory
+                                 optimisation) reject a tree whose mask names others or is 0 */
+    int32_t reserved[2];
     const int32_t* parent;          /* [njoints]   -1 for the universe            */
     const int32_t* jtype;           /* [njoints]   BR_JOINT_*                      */
     const int32_t* idx_q;           /* [njoints]                                   */
@@ -161,7 +169,8 @@ typedef struct br_ik_batch {
     const float* x0;            /* packed initial configurations                    */
     const float* q_rest;        /* packed rest configurations (RestResidual q_rest) */
     const int64_t* r_offset;    /* [n_problems] float offset of the problem's stacked residual
-                                   (target rows + 2*nq + nv floats) in result.residual; may be NULL */
+                                   (target rows, 2*nq limit rows, nv rest rows) in result.residual;
+                                   rows of a term whose weight is 0 are not written; may be NULL */
     const int32_t* target_kind; /* [n_problems*max_targets] BR_TARGET_*; NULL = every target a pose */
 } br_ik_batch_t;
 

@@ -115,3 +115,15 @@ def test_grad_output_scaling():
     q2 = q.detach().clone().requires_grad_(True)
     (g1,) = torch.autograd.grad(pose_loss(m, q2, fids, T, w).sum(), q2)
     torch.testing.assert_close(g, g1 * go[:, None], rtol=1e-6, atol=1e-6)
+
+
+def test_unsupported_joint_kinds_raise():
+    """The backward's raw-q chain rule covers revolute, prismatic and free-flyer joints only."""
+    from betterrobot_b200.exceptions import UnsupportedJointError
+    from betterrobot_b200 import trajopt as btr
+    m = syn.model_from_spec(syn.mixed_spec())
+    q = torch.zeros(2, m.nq, device="cuda")
+    with pytest.raises(UnsupportedJointError):
+        pose_loss(m, q, [0], torch.zeros(2, 1, 7, device="cuda"), torch.ones(1, device="cuda"))
+    with pytest.raises(UnsupportedJointError):
+        btr.solve_trajopt_batched(m, 0, torch.zeros(1, 7, device="cuda"), torch.zeros(1, 4, m.nq, device="cuda"))

@@ -64,8 +64,9 @@ def test_tree_arrays(spec):
 def test_unsupported_joint_kind_rejected():
     from betterrobot_b200.exceptions import UnsupportedJointError
     from betterrobot_b200.model import joint_model
-    with pytest.raises(UnsupportedJointError):
-        joint_model("spherical")
+    for kind in ("helical", "mimic", "composite"):  # not buildable by the reference's build_model either
+        with pytest.raises(UnsupportedJointError):
+            joint_model(kind)
 
 
 def test_cpu_tensor_rejected_without_fallback():

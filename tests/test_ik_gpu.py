@@ -24,7 +24,8 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 RES_TOL = 1e-4
-SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec()}
+SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec(),
+         "mixed": syn.mixed_spec()}
 
 
 def _models(name):
@@ -51,7 +52,7 @@ def _agreement(out, ref_conv, ref_res):
                                         ("chain7_huber", "chain7"), ("chain7_gn_cauchy", "chain7"),
                                         ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid"),
                                         ("chain7_position", "chain7"), ("dual_arm_mixed", "dual_arm"),
-                                        ("humanoid_mixed", "humanoid")])
+                                        ("humanoid_mixed", "humanoid"), ("mixed", "mixed")])
 def test_reference_solver_golden(case, robot):
     """The reference's own float64 solves (l2 and the robust IRLS kernels) reproduced on the GPU."""
     g = np.load(os.path.join(GOLDEN, f"ik_{case}.npz"))
@@ -99,6 +100,9 @@ def test_config0_chain_random_starts_vs_oracle():
 @pytest.mark.parametrize("robot,frames,rest,P,agree_min", [
     ("chain7", ["ee"], 1e-3, 64, 0.9), ("dual_arm", ["ee_l", "ee_r"], 1e-3, 64, 0.9),
     ("humanoid", ["track0", "track1", "track2", "track3"], 1e-3, 64, 0.9),
+    # mixed robot: planar base + translation lift are redundant; with a rest term the float64
+    # LM converges on 9% of these problems in 100 iterations, without it on 73% (median 33)
+    ("mixed", ["ee", "mid"], 0.0, 64, 0.9),
     ("humanoid", ["track0", "track4"], 0.01, 128, 0.85)])
 def test_noisy_start_vs_oracle(robot, frames, rest, P, agree_min):
     """Config-3 style problems: targets from FK(q*), q0 = q* + N(0, 0.3), 100 iterations.
@@ -124,7 +128,10 @@ def test_noisy_start_vs_oracle(robot, frames, rest, P, agree_min):
                                optimizer_cfg=bik.OptimizerConfig(max_iter=100, lam0=1e-3, factor=10.0),
                                with_residual=True)
     ok, conv, dres = _agreement(out, ref.converged, ref.residual)
-    assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
+    # final residuals are compared where the float64 solve converged: elsewhere they record
+    # where each run stopped at the iteration limit
+    done = ref.converged.astype(bool)
+    assert (dres[done] <= RES_TOL).mean() >= 0.95, (np.sort(dres[done])[-8:], done.mean())
     assert (conv == ref.converged).mean() >= agree_min, (conv.mean(), ref.converged.mean())
     assert abs(conv.mean() - ref.converged.mean()) <= 0.08, (conv.mean(), ref.converged.mean())
 

@@ -23,7 +23,8 @@ pytestmark = pytest.mark.gpu
 POS_TOL = 1e-5
 ROT_TOL = 1e-5
 JAC_TOL = 1e-4
-SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec()}
+SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec(),
+         "mixed": syn.mixed_spec()}  # mixed: planar base, translation, spherical and unbounded joints
 
 
 def assert_poses(got, ref):
@@ -79,6 +80,11 @@ def test_golden_fixture_through_cuda(name):
         assert_jac(J1, g[key][:, 0])
     br.compute_joint_jacobians(m, data)
     assert_jac(data.joint_jacobians, g["joint_jacobians"])
+    from betterrobot_b200.configuration import difference, integrate
+    np.testing.assert_allclose(integrate(m, q, torch.from_numpy(g["v"]).float().cuda()).cpu().double().numpy(),
+                               g["integrate"], atol=2e-6, rtol=0)
+    np.testing.assert_allclose(difference(m, q, torch.from_numpy(g["q1"]).float().cuda()).cpu().double().numpy(),
+                               g["difference"], atol=2e-6, rtol=0)
 
 
 @pytest.mark.parametrize("reference", ["world", "local_world_aligned", "local"])
@@ -155,7 +161,8 @@ def test_boundary_errors():
         br.get_frame_jacobian(m, d, 0, reference="bogus")
 
 
-@pytest.mark.parametrize("name,B", [("humanoid", 300), ("dual_arm", 300), ("chain7", 45), ("humanoid", 1)])
+@pytest.mark.parametrize("name,B", [("humanoid", 300), ("dual_arm", 300), ("chain7", 45), ("humanoid", 1),
+                                    ("mixed", 300)])
 def test_integrate_difference_match_oracle(name, B):
     """B = 300 / 45 leave a ragged last tile of 32 configurations; chain7 has no free-flyer."""
     from betterrobot_b200.configuration import difference, integrate
