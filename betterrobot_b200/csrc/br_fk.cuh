@@ -94,11 +94,13 @@ __device__ __forceinline__ Pose local_transform(int jt, const Pose& P, const flo
   return L;
 }
 
-// float64 liMi_j for the LM / trajectory kernels (same cases as local_transform).
+// float64 liMi_j for the LM / trajectory kernels (same cases as local_transform).  With
+// kAllKinds = false only fixed, revolute, prismatic and free-flyer joints are compiled in.
+template <bool kAllKinds = true>
 __device__ __forceinline__ DPose dlocal_transform(int jt, const DPose& P, const float* __restrict__ axis4,
                                                   const double* __restrict__ qv) {
   DPose L = P;
-  if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
+  if (jt == BR_JOINT_REVOLUTE || (kAllKinds && jt == BR_JOINT_REVOLUTE_UNBOUNDED)) {
     const double th = jt == BR_JOINT_REVOLUTE ? qv[0] : atan2(qv[1], qv[0]);
     double s, c;
     sincos(0.5 * th, &s, &c);
@@ -107,15 +109,19 @@ __device__ __forceinline__ DPose dlocal_transform(int jt, const DPose& P, const 
     L.t = dadd(P.t, dqrot(P.q, d3(qv[0] * axis4[0], qv[0] * axis4[1], qv[0] * axis4[2])));
   } else if (jt == BR_JOINT_FREE_FLYER) {
     L = dcompose(P, DPose{d3(qv[0], qv[1], qv[2]), dqnormalize(make_double4(qv[3], qv[4], qv[5], qv[6]))});
-  } else if (jt == BR_JOINT_SPHERICAL) {
+  } else if (kAllKinds && jt == BR_JOINT_SPHERICAL) {
     L.q = dqmul(P.q, dqnormalize(make_double4(qv[0], qv[1], qv[2], qv[3])));
-  } else if (jt == BR_JOINT_PLANAR) {
+  } else if (kAllKinds && jt == BR_JOINT_PLANAR) {
     L.t = dadd(P.t, dqrot(P.q, d3(qv[0], qv[1], 0.0)));
     L.q = dqmul(P.q, dplanar_quat(qv[2], qv[3]));
-  } else if (jt == BR_JOINT_TRANSLATION) {
+  } else if (kAllKinds && jt == BR_JOINT_TRANSLATION) {
     L.t = dadd(P.t, dqrot(P.q, d3(qv[0], qv[1], qv[2])));
   }
   return L;
 }
+
+// Joint kinds the plain LM variant is compiled for (bit BR_JOINT_k).
+constexpr int kBasicKinds = (1 << BR_JOINT_FIXED) | (1 << BR_JOINT_REVOLUTE) | (1 << BR_JOINT_PRISMATIC) |
+                            (1 << BR_JOINT_FREE_FLYER);
 
 }  // namespace br

@@ -173,8 +173,9 @@ __device__ __forceinline__ Pose to_f(const DPose& P) {
 }
 
 // ---- one problem, solved by one team ---------------------------------------
-// kGeneral = false compiles the plain stack (pose targets, l2 kernel) with the target-kind
-// and IRLS branches folded away; the host launches it whenever a batch needs nothing else.
+// kGeneral = false compiles the plain stack (pose targets, l2 kernel, fixed / revolute /
+// prismatic / free-flyer joints) with the other branches folded away; the host launches it
+// whenever a batch needs nothing else.
 template <int T, bool kGeneral>
 __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
@@ -312,7 +313,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // float64 FK of configuration q (shared) -> world poses (returned buffer), pointer jumping.
   auto fk = [&](const double* q) -> double* {
     for (int j = tl; j < nj; j += T) {
-      const DPose Lj = dlocal_transform(jtype[j], to_d(ld8(place + 8 * j)), axis + 4 * j, q + idxq[j]);
+      const DPose Lj = dlocal_transform<kGeneral>(jtype[j], to_d(ld8(place + 8 * j)), axis + 4 * j, q + idxq[j]);
       sts(poseA, nj, j, Lj);
       ancA[j] = parent[j];
     }
@@ -373,19 +374,19 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       for (int j = tl; j < nj; j += T) {
         const int jt = jtype[j];
         const int iq = idxq[j], iv = idxv[j];
-        if (joint_is_vector(jt)) {
-          for (int k = 0; k < joint_nv(jt); ++k) {
+        if (kGeneral ? joint_is_vector(jt) : (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC)) {
+          for (int k = 0; k < (kGeneral ? joint_nv(jt) : 1); ++k) {
             const double dd = q[iq + k] - qrest[iq + k];
             dr[iv + k] = dd;
             acc += wrd * wrd * dd * dd;
           }
-        } else if (jt == BR_JOINT_SPHERICAL) {                       // spherical.py:58-62
+        } else if (kGeneral && jt == BR_JOINT_SPHERICAL) {           // spherical.py:58-62
           const double3 w = dso3_log(dqnormalize(dqmul(
               dqconj(make_double4(qrest[iq], qrest[iq + 1], qrest[iq + 2], qrest[iq + 3])),
               make_double4(q[iq], q[iq + 1], q[iq + 2], q[iq + 3]))));
           dr[iv] = w.x; dr[iv + 1] = w.y; dr[iv + 2] = w.z;
           acc += wrd * wrd * ddot(w, w);
-        } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {  // planar.py:70-76, revolute.py:233-237
+        } else if (kGeneral && (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED)) {  // planar.py:70-76, revolute.py:233-237
           const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
           const double dth = atan2(q[iq + k + 1], q[iq + k]) - atan2(qrest[iq + k + 1], qrest[iq + k]);
           if (jt == BR_JOINT_PLANAR) {
@@ -647,13 +648,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       const int jt = jtype[j];
       const int iq = idxq[j], iv = idxv[j];
       auto clampq = [&](int k, double v) { xn[iq + k] = fmin(fmax(v, (double)lower[iq + k]), (double)upper[iq + k]); };
-      if (joint_is_vector(jt)) {
-        for (int k = 0; k < joint_nv(jt); ++k) clampq(k, x[iq + k] + (double)delta[iv + k]);
-      } else if (jt == BR_JOINT_SPHERICAL) {                         // spherical.py:52-56
+      if (kGeneral ? joint_is_vector(jt) : (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC)) {
+        for (int k = 0; k < (kGeneral ? joint_nv(jt) : 1); ++k) clampq(k, x[iq + k] + (double)delta[iv + k]);
+      } else if (kGeneral && jt == BR_JOINT_SPHERICAL) {             // spherical.py:52-56
         const double4 n = dqnormalize(dqmul(make_double4(x[iq], x[iq + 1], x[iq + 2], x[iq + 3]),
                                             dse3_exp(d3(0.0, 0.0, 0.0), d3(delta[iv], delta[iv + 1], delta[iv + 2])).q));
         clampq(0, n.x); clampq(1, n.y); clampq(2, n.z); clampq(3, n.w);
-      } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {  // planar.py:61-68, revolute.py:223-231
+      } else if (kGeneral && (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED)) {  // planar.py:61-68, revolute.py:223-231
         const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
         const double th = atan2(x[iq + k + 1], x[iq + k]) + (double)delta[iv + k];
         double s, c;
@@ -849,7 +850,8 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     bytes = (size_t)wpc * warp_floats * sizeof(float);
   }
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  const bool general = b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2;
+  bool general = b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2;
+  for (int c = 0; c < b.n_classes; ++c) general |= (b.trees[c].kinds & ~kBasicKinds) != 0 || b.trees[c].kinds == 0;
   auto kern = general ? lm_solve_kernel<true> : lm_solve_kernel<false>;
   static int configured[2][16] = {};
   int& have = configured[general][dev.device & 15];
@@ -959,8 +961,9 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     bytes = (size_t)wpc * warp_floats * sizeof(float);
   }
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  auto kern = (b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2) ? lm_solve_kernel<true>
-                                                                            : lm_solve_kernel<false>;
+  bool general = b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2;
+  for (int c = 0; c < b.n_classes; ++c) general |= (b.trees[c].kinds & ~kBasicKinds) != 0 || b.trees[c].kinds == 0;
+  auto kern = general ? lm_solve_kernel<true> : lm_solve_kernel<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return (int)e;
   int per_sm = 0;
