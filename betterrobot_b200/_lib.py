@@ -26,7 +26,7 @@ class BrTree(ctypes.Structure):
     """Mirror of ``br_tree_t``."""
 
     _fields_ = [("njoints", c_int32), ("nq", c_int32), ("nv", c_int32), ("nframes", c_int32),
-                ("rounds", c_int32), ("kinds", c_int32), ("reserved", c_int32 * 2),
+                ("rounds", c_int32), ("kinds", c_int32), ("dof_entries", c_int32), ("dof_depth", c_int32),
                 ("parent", c_void_p), ("jtype", c_void_p), ("idx_q", c_void_p), ("idx_v", c_void_p),
                 ("axis", c_void_p), ("placement", c_void_p), ("support", c_void_p),
                 ("frame_parent", c_void_p), ("frame_placement", c_void_p),

@@ -59,8 +59,11 @@ struct TeamLayout {
   int dpar, ddep, rowoff, amask, ancd;
   int x, xn, qrest, poseA, poseB, ancA, ancB, tw, xi, jri, colw, d, g, delta, jtj, work, misc,
       dinv, sup, nsup;
+  int n_ent, anc_stride;  // capacity of the J^T J / factor storage; row length of ancd
   int total;
-  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T) {
+  // ent / dep: the tree's DOF entry count and depth bound (br_tree_t.dof_entries /
+  // dof_depth), 0 for the dense bounds.
+  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T, int ent = 0, int dep = 0) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += round4(n); return r; };
     parent = take(nj); jtype = take(nj); idxq = take(nj); idxv = take(nj);
@@ -78,14 +81,16 @@ struct TeamLayout {
     jri = take(16 * K); colw = take(8 * nv);
     g = take(nv); delta = take(nv);
     const int ntri = nv * (nv + 1) / 2;
-    jtj = take(ntri);                          // J^T J, packed lower triangle, column-major
-    work = take(6 * nv > ntri ? 6 * nv : ntri);  // one target's J columns (build) / packed L (solve)
+    n_ent = (ent > 0 && ent < ntri) ? ent : ntri;
+    anc_stride = (dep > 0 && dep < nv) ? dep : (nv > 0 ? nv : 1);
+    jtj = take(n_ent);                         // J^T J, one row per DOF over its ancestors
+    work = take(6 * nv > n_ent ? 6 * nv : n_ent);  // one target's J columns (build) / the factor (solve)
     misc = take(8);
     amask = take(2 * nv);                      // uint64 strict ancestors of each DOF
     dpar = take((nv + 3) / 4);                 // int8 parent DOF (-1 at a root)
     ddep = take((nv + 3) / 4);                 // uint8 DOF depth
     rowoff = take((nv + 2) / 2);               // uint16 first entry of each row, nv + 1 values
-    ancd = take((nv * nv + 3) / 4);            // uint8 ancestor of DOF c at depth a: ancd[c * nv + a]
+    ancd = take((nv * anc_stride + 3) / 4);    // uint8 ancestor of DOF c at depth a: ancd[c * anc_stride + a]
     dinv = take(nv);                           // 1 / L_jj
     sup = take((K * nv + 3) / 4);              // uint8 support columns of each target, ascending
     nsup = take(K);
@@ -180,7 +185,7 @@ template <int T, bool kGeneral>
 __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
   const int K = P.b.max_targets;
-  const TeamLayout L(nj, nq, nv, K, T);
+  const TeamLayout L(nj, nq, nv, K, T, tree.dof_entries, tree.dof_depth);
   int* parent = reinterpret_cast<int*>(sm + L.parent);
   int* jtype = reinterpret_cast<int*>(sm + L.jtype);
   int* idxq = reinterpret_cast<int*>(sm + L.idxq);
@@ -219,6 +224,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   unsigned short* rowoff = reinterpret_cast<unsigned short*>(sm + L.rowoff);
   unsigned char* ancd = reinterpret_cast<unsigned char*>(sm + L.ancd);
   float* dinv = sm + L.dinv;
+  int* misc = reinterpret_cast<int*>(sm + L.misc);  // [0]: the tree's size fields are too small
   unsigned char* sup = reinterpret_cast<unsigned char*>(sm + L.sup);
   int* nsup = reinterpret_cast<int*>(sm + L.nsup);
   const int tl = tm.tl;
@@ -279,19 +285,36 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       lastd[j] = nvj ? idxv[j] + nvj - 1 : prev;
     }
     int nl = 0;
+    bool bad = false;
+    const int As = L.anc_stride;
     for (int c = 0; c < nv; ++c) {
       const int pc = dpar[c];
       const int dc = pc < 0 ? 0 : ddep[pc] + 1;
       ddep[c] = (unsigned char)dc;
       amask[c] = pc < 0 ? 0ull : (amask[pc] | (1ull << pc));
-      for (int a = 0; a + 1 < dc; ++a) ancd[c * nv + a] = ancd[pc * nv + a];
-      if (pc >= 0) ancd[c * nv + dc - 1] = (unsigned char)pc;
+      if (dc > As) {
+        bad = true;  // deeper than the tree's dof_depth claims: the ancestor table would overflow
+      } else {
+        for (int a = 0; a + 1 < dc; ++a) ancd[c * As + a] = ancd[pc * As + a];
+        if (pc >= 0) ancd[c * As + dc - 1] = (unsigned char)pc;
+      }
       rowoff[c] = (unsigned short)nl;
       nl += dc + 1;
     }
     rowoff[nv] = (unsigned short)nl;
+    misc[0] = (bad || nl > L.n_ent) ? 1 : 0;
   }
   tm.sync();
+  if (misc[0]) {  // dof_entries / dof_depth of the tree are smaller than its DOF tree: refuse
+    for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = P.b.x0[qoff + i];
+    if (tl == 0) {
+      P.r.iters[prob] = 0;
+      P.r.status[prob] = BR_IK_MAXITER | (BR_IK_FLAG_BADTREE << 8);
+      P.r.cost[prob] = __int_as_float(0x7fc00000);  // NaN
+    }
+    tm.sync();
+    return;
+  }
   const int nL = rowoff[nv];
   // ascending list of the tangent columns that move each target frame (its support)
   for (int t = 0; t < nt; ++t) {
@@ -572,7 +595,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       if (!(piv > 0.f) || !isfinite(piv)) return false;  // every lane read the same pivot
       const float inv = 1.f / piv;
       if (tl == 0) dinv[k] = inv;
-      const unsigned char* anc = ancd + k * nv;
+      const unsigned char* anc = ancd + k * L.anc_stride;
       for (int p = tl; p < tri(dk); p += T) {                // pairs (a, b), b <= a < dk, by depth
         int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
         if (tri(a + 1) <= p) ++a;
@@ -772,7 +795,7 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
   tm.tl = lane % T;
   tm.mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (team * T));
   const br_tree_t& tree = P.trees[cls];
-  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T);
+  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T, tree.dof_entries, tree.dof_depth);
   if (team < count) {
     const int prob = P.b.order[first + team];
     solve_problem<T, kGeneral>(P, tree, prob, wsm + team * L.total, tm);
@@ -806,7 +829,7 @@ using namespace br;
 extern "C" int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets) {
   if (!tree || max_targets < 0) return BR_EINVAL;
   const int T = kLmTeam;
-  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T).total;
+  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T, tree->dof_entries, tree->dof_depth).total;
 }
 
 extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
@@ -837,7 +860,8 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
     p.trees[c] = b.trees[c];
     p.team[c] = T;
-    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;
+    const br_tree_t& tc = b.trees[c];
+    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;
@@ -948,7 +972,8 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
     p.trees[c] = b.trees[c];
     p.team[c] = T;
-    const int f = (32 / T) * TeamLayout(b.trees[c].njoints, b.trees[c].nq, b.trees[c].nv, b.max_targets, T).total;
+    const br_tree_t& tc = b.trees[c];
+    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;

@@ -118,6 +118,21 @@ class TreeArrays:
             fp = _np(f.joint_placement)
             self.frame_placement[i, :3] = fp[:3]
             self.frame_placement[i, 4:8] = fp[3:7]
+        # DOF tree (a joint's DOFs chained, the first under the last DOF of the nearest
+        # ancestor joint with DOFs): J^T J entries per DOF = depth + 1
+        lastd = np.full(nj, -1, np.int64)
+        ddep = np.zeros(nv, np.int64)
+        for j in range(nj):
+            p = parents[j]
+            prev = lastd[p] if p >= 0 else -1
+            nvj = int(model.nvs[j])
+            for k in range(nvj):
+                c = int(self.idx_v[j]) + k
+                pc = prev if k == 0 else c - 1
+                ddep[c] = 0 if pc < 0 else ddep[pc] + 1
+            lastd[j] = int(self.idx_v[j]) + nvj - 1 if nvj else prev
+        self.dof_entries = int((ddep + 1).sum())
+        self.dof_depth = int(ddep.max()) + 1 if nv else 1
         self.lower = _np(model.lower_pos_limit).astype(np.float32)
         self.upper = _np(model.upper_pos_limit).astype(np.float32)
 
@@ -154,6 +169,7 @@ class DeviceTree:
         st = BrTree()
         st.njoints, st.nq, st.nv, st.nframes, st.rounds = a.nj, a.nq, a.nv, a.nf, a.rounds
         st.kinds = int(np.bitwise_or.reduce(np.left_shift(1, a.jtype.astype(np.int64))))
+        st.dof_entries, st.dof_depth = a.dof_entries, a.dof_depth
         for name, _ in a.sections():
             setattr(st, name, base + offs[name])
         self.struct = st

@@ -70,7 +70,9 @@ typedef struct br_tree {
     int32_t kinds;            /* bit k set if some joint has kind BR_JOINT_k; entry points
                                  that support only some kinds (the FK adjoint, trajectory
                                  optimisation) reject a tree whose mask names others or is 0 */
-    int32_t reserved[2];
+    int32_t dof_entries;      /* sum over tangent columns of (depth in the DOF tree + 1): the
+                                 LM's J^T J storage; 0 = not given (dense nv (nv + 1) / 2) */
+    int32_t dof_depth;        /* 1 + deepest DOF-tree depth; 0 = not given (nv)            */
     const int32_t* parent;          /* [njoints]   -1 for the universe            */
     const int32_t* jtype;           /* [njoints]   BR_JOINT_*                      */
     const int32_t* idx_q;           /* [njoints]                                   */
@@ -141,6 +143,7 @@ BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joi
 #define BR_IK_MAXITER 1
 #define BR_IK_FLAG_NONFINITE 1  /* (status >> 8) bits: a non-finite cost was seen   */
 #define BR_IK_FLAG_REGULARIZED 2 /* float32 LDL^T needed extra diagonal damping     */
+#define BR_IK_FLAG_BADTREE 4    /* tree's dof_entries / dof_depth below its DOF tree: not solved */
 
 /* Solver settings: LevenbergMarquardt(lam0, factor, tol) with Adaptive damping
  * bounds [lam_min, lam_max] (optim/strategies/adaptive.py:19-25), GaussNewton eps,
