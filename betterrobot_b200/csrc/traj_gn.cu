@@ -58,7 +58,7 @@ struct TrajParams {
 
 struct TrajLayout {
   // doubles
-  int x, xn, xref, g, delta, D, E1, E2, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
+  int x, xn, xref, g, delta, D, E1, E2, dinvt, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
   int total_doubles;
   // ints / floats (in units of doubles)
   int parent, jtype, idxq, cjoint, ckind, axis, place, caxis, anc, lower, upper, misc;
@@ -67,7 +67,7 @@ struct TrajLayout {
     int o = 0;
     auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };  // 16-byte aligned
     x = take(T * nv); xn = take(T * nv); xref = take(T * nv); g = take(T * nv); delta = take(T * nv);
-    D = take(T * nv * nv); E1 = take(T * nv * nv); E2 = take(T * nv * nv);
+    D = take(T * nv * nv); E1 = take(T * nv * nv); E2 = take(T * nv * nv); dinvt = take(T * nv);
     Jg = take(6 * nv); Js = take(6 * nv); rg = take(8); rs = take(8); jtjg = take(nv * nv); jtjs = take(nv * nv);
     pA = take(8 * nj); pB = take(8 * nj);
     total_doubles = o;
@@ -103,6 +103,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   double* D = sm + L.D;
   double* E1 = sm + L.E1;
   double* E2 = sm + L.E2;
+  double* dinvt = sm + L.dinvt;  // 1 / L_tt[k][k] of every diagonal block
   double* Jg = sm + L.Jg;
   double* Js = sm + L.Js;
   double* rg = sm + L.rg;
@@ -350,9 +351,10 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         const double dkk = Dt[k * nv + k];
         if (!(dkk > 0.0)) return false;
         const double s = sqrt(dkk);
+        const double inv = 1.0 / s;                                // every lane: no broadcast needed
         __syncwarp();
-        if (lane > k && lane < nv) Dt[lane * nv + k] /= s;
-        if (lane == k) Dt[k * nv + k] = s;
+        if (lane > k && lane < nv) Dt[lane * nv + k] *= inv;
+        if (lane == k) { Dt[k * nv + k] = s; dinvt[t * nv + k] = inv; }
         __syncwarp();
         for (int e = lane; e < b2; e += kWarp) {
           const int i = e / nv, j = e - i * nv;
@@ -367,52 +369,52 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       if (lane >= 16 && lane - 16 < nv && t + 2 < T) { X = E2 + t * b2; row = lane - 16; }
       if (X) {
         double* xr = X + row * nv;
+        const double* di = dinvt + t * nv;
         for (int j = 0; j < nv; ++j) {
           double v = xr[j];
           for (int k = 0; k < j; ++k) v -= xr[k] * Dt[j * nv + k];
-          xr[j] = v / Dt[j * nv + j];
+          xr[j] = v * di[j];
         }
       }
       __syncwarp();
     }
-    // forward: L y = -g (y in delta)
+    // forward: L y = -g (y in delta).  Lane i < nv owns row i of each knot; the 7x7
+    // diagonal solve broadcasts one finished entry per step by shuffle.
+    const double* Ld = D;
     for (int t = 0; t < T; ++t) {
+      double v = 0.0;
       if (lane < nv) {
-        double v = -g[t * nv + lane];
+        v = -g[t * nv + lane];
         if (t >= 1) for (int k = 0; k < nv; ++k) v -= E1[(t - 1) * b2 + lane * nv + k] * delta[(t - 1) * nv + k];
         if (t >= 2) for (int k = 0; k < nv; ++k) v -= E2[(t - 2) * b2 + lane * nv + k] * delta[(t - 2) * nv + k];
-        delta[t * nv + lane] = v;
       }
-      __syncwarp();
-      if (lane == 0) {
-        const double* Lt = D + t * b2;
-        double* y = delta + t * nv;
-        for (int j = 0; j < nv; ++j) {
-          double v = y[j];
-          for (int k = 0; k < j; ++k) v -= Lt[j * nv + k] * y[k];
-          y[j] = v / Lt[j * nv + j];
-        }
+      const double* Lt = Ld + t * b2;
+      const double* di = dinvt + t * nv;
+      for (int j = 0; j < nv; ++j) {
+        const double yj = __shfl_sync(0xffffffffu, v, j) * di[j];
+        if (lane == j) v = yj;
+        else if (lane > j && lane < nv) v -= Lt[lane * nv + j] * yj;
       }
+      if (lane < nv) delta[t * nv + lane] = v;
       __syncwarp();
     }
     // backward: L^T dx = y
     for (int t = T - 1; t >= 0; --t) {
+      double v = 0.0;
       if (lane < nv) {
-        double v = delta[t * nv + lane];
+        v = delta[t * nv + lane];
         if (t + 1 < T) for (int k = 0; k < nv; ++k) v -= E1[t * b2 + k * nv + lane] * delta[(t + 1) * nv + k];
         if (t + 2 < T) for (int k = 0; k < nv; ++k) v -= E2[t * b2 + k * nv + lane] * delta[(t + 2) * nv + k];
-        delta[t * nv + lane] = v;
+      }
+      const double* Lt = Ld + t * b2;
+      const double* di = dinvt + t * nv;
+      for (int j = nv - 1; j >= 0; --j) {
+        const double xj = __shfl_sync(0xffffffffu, v, j) * di[j];
+        if (lane == j) v = xj;
+        else if (lane < j) v -= Lt[j * nv + lane] * xj;
       }
       __syncwarp();
-      if (lane == 0) {
-        const double* Lt = D + t * b2;
-        double* y = delta + t * nv;
-        for (int j = nv - 1; j >= 0; --j) {
-          double v = y[j];
-          for (int k = j + 1; k < nv; ++k) v -= Lt[k * nv + j] * y[k];
-          y[j] = v / Lt[j * nv + j];
-        }
-      }
+      if (lane < nv) delta[t * nv + lane] = v;
       __syncwarp();
     }
     return true;
