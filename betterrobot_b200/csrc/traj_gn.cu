@@ -10,14 +10,20 @@
 //   accel : (q_{s+2} - 2 q_{s+1} + q_s)/dt^2 (AccelerationResidual, residuals/smoothness.py:98-161)
 //   limits: JointPositionLimit at every knot (residuals/limits.py:56-86)
 //   ref   : q_t - q_ref_t                   (ReferenceTrajectoryResidual, residuals/regularization.py:133-152)
-// each with a CostStack item weight.  Its J^T J is block PENTA-diagonal in 7x7
-// blocks (the acceleration row couples three knots), with the acceleration part a
-// scalar band times I: this kernel assembles only the bands — H_tt, H_{t+1,t},
-// H_{t+2,t} — and factors them with a bandwidth-2 block Cholesky
-//   L_tt     = chol(H_tt - L_{t,t-1} L_{t,t-1}^T - L_{t,t-2} L_{t,t-2}^T)
-//   L_{t+1,t} = (H_{t+1,t} - L_{t+1,t-1} L_{t,t-1}^T) L_tt^-T
-//   L_{t+2,t} = H_{t+2,t} L_tt^-T
-// followed by block forward / backward substitution: O(T nv^3) instead of O((T nv)^3).
+// each with a CostStack item weight.  In its J^T J + damp I every term except the
+// two pose terms acts on one DOF at a time: the acceleration rows couple knots
+// t, t+1, t+2 of the same DOF, limits / reference / damping are diagonal.  So H is
+// nv independent scalar PENTA-diagonal T x T matrices (one per DOF) plus the dense
+// nv x nv pose blocks at knots 0 and T-1.  The kernel solves it in nested-dissection
+// order: the interior knots 1..T-2 of each DOF first — lane i runs the banded
+// LDL^T of DOF i and three solves (right-hand side and the two columns that tie the
+// interior to knots 0 and T-1) — leaving a 2nv x 2nv Schur complement on the
+// boundary knots,
+//   S = H_bb - H_bI P^-1 H_Ib,   P = blockdiag_i(P_i) the per-DOF interior bands,
+// which the warp factors with a dense Cholesky; the interior step follows by one
+// update.  This is the exact Cholesky of a symmetric permutation of H (no
+// approximation): O(T nv) sequential work per iteration instead of the O(T nv^3) of
+// a block-banded factorization or the O((T nv)^3) of the dense one.
 //
 // Precision: the normal matrix has condition ~1e8 (acceleration stiffness
 // (w/dt^2)^2 against a 1e-6 regularisation).  A float32 factorization fails there,
@@ -58,7 +64,7 @@ struct TrajParams {
 
 struct TrajLayout {
   // doubles
-  int x, xn, xref, g, delta, D, E1, E2, dinvt, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
+  int x, xn, xref, g, delta, bl1, bl2, bdi, vy, vu, vw, Sb, sdi, rb, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
   int total_doubles;
   // ints / floats (in units of doubles)
   int parent, jtype, idxq, cjoint, ckind, axis, place, caxis, anc, lower, upper, misc;
@@ -67,7 +73,11 @@ struct TrajLayout {
     int o = 0;
     auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };  // 16-byte aligned
     x = take(T * nv); xn = take(T * nv); xref = take(T * nv); g = take(T * nv); delta = take(T * nv);
-    D = take(T * nv * nv); E1 = take(T * nv * nv); E2 = take(T * nv * nv); dinvt = take(T * nv);
+    // per-DOF interior bands (index p * nv + i, p = knot - 1): L[p][p-1], L[p][p-2], 1 / D[p];
+    // solutions of P_i y = r, P_i u = h0, P_i w = hT
+    bl1 = take(T * nv); bl2 = take(T * nv); bdi = take(T * nv);
+    vy = take(T * nv); vu = take(T * nv); vw = take(T * nv);
+    Sb = take(4 * nv * nv); sdi = take(2 * nv); rb = take(2 * nv);   // boundary Schur complement
     Jg = take(6 * nv); Js = take(6 * nv); rg = take(8); rs = take(8); jtjg = take(nv * nv); jtjs = take(nv * nv);
     pA = take(8 * nj); pB = take(8 * nj);
     total_doubles = o;
@@ -100,10 +110,15 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   double* xref = sm + L.xref;
   double* g = sm + L.g;
   double* delta = sm + L.delta;
-  double* D = sm + L.D;
-  double* E1 = sm + L.E1;
-  double* E2 = sm + L.E2;
-  double* dinvt = sm + L.dinvt;  // 1 / L_tt[k][k] of every diagonal block
+  double* bl1 = sm + L.bl1;
+  double* bl2 = sm + L.bl2;
+  double* bdi = sm + L.bdi;
+  double* vy = sm + L.vy;
+  double* vu = sm + L.vu;
+  double* vw = sm + L.vw;
+  double* Sb = sm + L.Sb;
+  double* sdi = sm + L.sdi;
+  double* rb = sm + L.rb;
   double* Jg = sm + L.Jg;
   double* Js = sm + L.Js;
   double* rg = sm + L.rg;
@@ -300,123 +315,145 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     __syncwarp();
     return sqrt(gg);
   };
-  // assemble the bands of J^T J + damp I at x
-  auto assemble = [&](double damp) {
-    for (int e = lane; e < T * nv * nv; e += kWarp) {
-      const int t = e / (nv * nv), ij = e - t * nv * nv, i = ij / nv, j = ij - i * nv;
-      double d = 0.0, e1 = 0.0, e2 = 0.0;
-      if (i == j) {
-        // diagonal: acceleration coefficient squares at knot t
-        double a = 0.0;
-        if (t <= T - 3) a += 1.0;
-        if (t - 1 >= 0 && t - 1 <= T - 3) a += 4.0;
-        if (t - 2 >= 0) a += 1.0;
-        const double xv = x[t * nv + i];
-        d = c2 * a + wr * wr + damp;
-        if (xv < (double)lower[i]) d += wl * wl;
-        if (xv > (double)upper[i]) d += wl * wl;
-        double b = 0.0;                       // block (t+1, t)
-        if (t <= T - 3) b += -2.0;
-        if (t - 1 >= 0 && t <= T - 2) b += -2.0;
-        e1 = (t <= T - 2) ? c2 * b : 0.0;
-        e2 = (t <= T - 3) ? c2 : 0.0;        // block (t+2, t)
+  // bands of J^T J + damp I at x (DOF i): diagonal at knot t, H[(t+1,i),(t,i)], and
+  // H[(t+2,i),(t,i)] = c2 for t <= T-3.  Acceleration row s has coefficients (1, -2, 1)
+  // on knots (s, s+1, s+2), s = 0..T-3.
+  auto hdiag = [&](int t, int i, double damp) -> double {
+    double a = 0.0;
+    if (t <= T - 3) a += 1.0;
+    if (t - 1 >= 0 && t - 1 <= T - 3) a += 4.0;
+    if (t - 2 >= 0) a += 1.0;
+    const double xv = x[t * nv + i];
+    double d = c2 * a + wr * wr + damp;
+    if (xv < (double)lower[i]) d += wl * wl;
+    if (xv > (double)upper[i]) d += wl * wl;
+    return d;
+  };
+  auto hoff1 = [&](int t) -> double {
+    double b = 0.0;
+    if (t <= T - 3) b += -2.0;
+    if (t - 1 >= 0 && t <= T - 2) b += -2.0;
+    return c2 * b;
+  };
+  // solve (J^T J + damp I) delta = -g; false when a pivot is not positive
+  auto newton_solve = [&](double damp) -> bool {
+    const int m = T - 2, nb = 2 * nv;
+    bool good = true;
+    if (lane < nv) {
+      const int i = lane;
+      // banded LDL^T of the interior of DOF i: L[p][p-2] = c2 / D[p-2],
+      // L[p][p-1] = (H[p][p-1] - c2 L[p-1][p-2]) / D[p-1], D[p] = H[p][p] - L[p][p-1]^2 D[p-1] - L[p][p-2] c2
+      double d1 = 0.0, di1 = 0.0, di2 = 0.0, l1p = 0.0;
+      for (int p = 0; p < m; ++p) {
+        const int t = p + 1;
+        const double l2 = (p >= 2) ? c2 * di2 : 0.0;
+        const double l1 = (p >= 1) ? (hoff1(t - 1) - c2 * l1p) * di1 : 0.0;
+        const double dp = hdiag(t, i, damp) - l1 * l1 * d1 - l2 * c2;
+        if (!(dp > 0.0)) { good = false; break; }
+        const double dip = 1.0 / dp;
+        bl1[p * nv + i] = l1; bl2[p * nv + i] = l2; bdi[p * nv + i] = dip;
+        di2 = di1; di1 = dip; d1 = dp; l1p = l1;
       }
-      if (has_goal && t == T - 1) d += jtjg[ij];
-      if (has_start && t == 0) d += jtjs[ij];
-      D[e] = d;
-      E1[e] = e1;
-      E2[e] = e2;
-    }
-    __syncwarp();
-  };
-  // C -= A B^T (nv x nv blocks)
-  auto sub_abt = [&](double* C, const double* A, const double* B) {
-    for (int e = lane; e < nv * nv; e += kWarp) {
-      const int i = e / nv, j = e - i * nv;
-      double acc = C[e];
-      for (int k = 0; k < nv; ++k) acc -= A[i * nv + k] * B[j * nv + k];
-      C[e] = acc;
-    }
-    __syncwarp();
-  };
-  // bandwidth-2 block Cholesky in place; solve L L^T delta = -g
-  auto factor_solve = [&]() -> bool {
-    const int b2 = nv * nv;
-    for (int t = 0; t < T; ++t) {
-      double* Dt = D + t * b2;
-      if (t >= 1) sub_abt(Dt, E1 + (t - 1) * b2, E1 + (t - 1) * b2);
-      if (t >= 2) sub_abt(Dt, E2 + (t - 2) * b2, E2 + (t - 2) * b2);
-      if (t >= 1 && t + 1 < T) sub_abt(E1 + t * b2, E2 + (t - 1) * b2, E1 + (t - 1) * b2);
-      for (int k = 0; k < nv; ++k) {                               // chol(D_t)
-        const double dkk = Dt[k * nv + k];
-        if (!(dkk > 0.0)) return false;
-        const double s = sqrt(dkk);
-        const double inv = 1.0 / s;                                // every lane: no broadcast needed
-        __syncwarp();
-        if (lane > k && lane < nv) Dt[lane * nv + k] *= inv;
-        if (lane == k) { Dt[k * nv + k] = s; dinvt[t * nv + k] = inv; }
-        __syncwarp();
-        for (int e = lane; e < b2; e += kWarp) {
-          const int i = e / nv, j = e - i * nv;
-          if (j > k && i >= j) Dt[e] -= Dt[i * nv + k] * Dt[j * nv + k];
+      if (good) {
+        // forward L z = (r, h0, hT), r = -g on the interior; h0 / hT: the columns of knots 0 / T-1
+        double y1 = 0, y2 = 0, u1 = 0, u2 = 0, w1 = 0, w2 = 0;
+        for (int p = 0; p < m; ++p) {
+          const int t = p + 1;
+          const double l1 = bl1[p * nv + i], l2 = bl2[p * nv + i];
+          const double h0 = (t == 1) ? hoff1(0) : (t == 2 ? c2 : 0.0);
+          const double hT = (t == T - 2) ? hoff1(T - 2) : (t == T - 3 ? c2 : 0.0);
+          const double y = -g[t * nv + i] - l1 * y1 - l2 * y2;
+          const double u = h0 - l1 * u1 - l2 * u2;
+          const double w = hT - l1 * w1 - l2 * w2;
+          vy[p * nv + i] = y; vu[p * nv + i] = u; vw[p * nv + i] = w;
+          y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
         }
-        __syncwarp();
-      }
-      // off-diagonal blocks: X <- X L_tt^-T, lanes 0..nv-1 rows of E1_t, lanes 16.. rows of E2_t
-      double* X = nullptr;
-      int row = -1;
-      if (lane < nv && t + 1 < T) { X = E1 + t * b2; row = lane; }
-      if (lane >= 16 && lane - 16 < nv && t + 2 < T) { X = E2 + t * b2; row = lane - 16; }
-      if (X) {
-        double* xr = X + row * nv;
-        const double* di = dinvt + t * nv;
-        for (int j = 0; j < nv; ++j) {
-          double v = xr[j];
-          for (int k = 0; k < j; ++k) v -= xr[k] * Dt[j * nv + k];
-          xr[j] = v * di[j];
+        // backward D L^T v = z
+        y1 = y2 = u1 = u2 = w1 = w2 = 0;
+        for (int p = m - 1; p >= 0; --p) {
+          const double di = bdi[p * nv + i];
+          const double l1n = (p + 1 < m) ? bl1[(p + 1) * nv + i] : 0.0;   // L[p+1][p]
+          const double l2n = (p + 2 < m) ? bl2[(p + 2) * nv + i] : 0.0;   // L[p+2][p]
+          const double y = vy[p * nv + i] * di - l1n * y1 - l2n * y2;
+          const double u = vu[p * nv + i] * di - l1n * u1 - l2n * u2;
+          const double w = vw[p * nv + i] * di - l1n * w1 - l2n * w2;
+          vy[p * nv + i] = y; vu[p * nv + i] = u; vw[p * nv + i] = w;
+          y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
         }
       }
+    }
+    if (!__all_sync(0xffffffffu, good)) return false;
+    // boundary block H_bb: b = i for (knot 0, DOF i), nv + i for (knot T-1, DOF i)
+    for (int e = lane; e < nb * nb; e += kWarp) {
+      const int r = e / nb, cc = e - r * nb;
+      const int kr = r / nv, kc = cc / nv, ir = r - kr * nv, ic = cc - kc * nv;
+      double h = 0.0;
+      if (kr == kc) {
+        if (kr == 0 && has_start) h = jtjs[ir * nv + ic];
+        if (kr == 1 && has_goal) h = jtjg[ir * nv + ic];
+        if (ir == ic) h += hdiag(kr ? T - 1 : 0, ir, damp);
+      } else if (ir == ic && T == 3) {
+        h = c2;                                                    // row 0 couples knots 0 and 2
+      }
+      Sb[e] = h;
+    }
+    __syncwarp();
+    if (lane < nv) {
+      // S = H_bb - H_bI P^-1 H_Ib and rb = -g_b - H_bI y: h0 is nonzero at interior p = 0, 1,
+      // hT at p = m-1, m-2
+      const int i = lane;
+      const double a0 = hoff1(0), a1 = (m >= 2) ? c2 : 0.0;           // h0[0], h0[1]
+      const double b0 = hoff1(T - 2), b1 = (m >= 2) ? c2 : 0.0;       // hT[m-1], hT[m-2]
+      auto at = [&](const double* v, int p) { return v[p * nv + i]; };
+      const double h0u = a0 * at(vu, 0) + (m >= 2 ? a1 * at(vu, 1) : 0.0);
+      const double h0w = a0 * at(vw, 0) + (m >= 2 ? a1 * at(vw, 1) : 0.0);
+      const double hTw = b0 * at(vw, m - 1) + (m >= 2 ? b1 * at(vw, m - 2) : 0.0);
+      const double h0y = a0 * at(vy, 0) + (m >= 2 ? a1 * at(vy, 1) : 0.0);
+      const double hTy = b0 * at(vy, m - 1) + (m >= 2 ? b1 * at(vy, m - 2) : 0.0);
+      Sb[i * nb + i] -= h0u;
+      Sb[i * nb + nv + i] -= h0w;
+      Sb[(nv + i) * nb + i] -= h0w;
+      Sb[(nv + i) * nb + nv + i] -= hTw;
+      rb[i] = -g[i] - h0y;
+      rb[nv + i] = -g[(T - 1) * nv + i] - hTy;
+    }
+    __syncwarp();
+    for (int k = 0; k < nb; ++k) {                                  // chol(S), lower, in place
+      const double dkk = Sb[k * nb + k];
+      if (!(dkk > 0.0)) return false;
+      const double sk = sqrt(dkk);
+      const double inv = 1.0 / sk;
+      __syncwarp();
+      if (lane > k && lane < nb) Sb[lane * nb + k] *= inv;
+      if (lane == k) { Sb[k * nb + k] = sk; sdi[k] = inv; }
+      __syncwarp();
+      for (int e = lane; e < nb * nb; e += kWarp) {
+        const int r = e / nb, cc = e - r * nb;
+        if (cc > k && r >= cc) Sb[e] -= Sb[r * nb + k] * Sb[cc * nb + k];
+      }
       __syncwarp();
     }
-    // forward: L y = -g (y in delta).  Lane i < nv owns row i of each knot; the 7x7
-    // diagonal solve broadcasts one finished entry per step by shuffle.
-    const double* Ld = D;
-    for (int t = 0; t < T; ++t) {
-      double v = 0.0;
-      if (lane < nv) {
-        v = -g[t * nv + lane];
-        if (t >= 1) for (int k = 0; k < nv; ++k) v -= E1[(t - 1) * b2 + lane * nv + k] * delta[(t - 1) * nv + k];
-        if (t >= 2) for (int k = 0; k < nv; ++k) v -= E2[(t - 2) * b2 + lane * nv + k] * delta[(t - 2) * nv + k];
-      }
-      const double* Lt = Ld + t * b2;
-      const double* di = dinvt + t * nv;
-      for (int j = 0; j < nv; ++j) {
-        const double yj = __shfl_sync(0xffffffffu, v, j) * di[j];
-        if (lane == j) v = yj;
-        else if (lane > j && lane < nv) v -= Lt[lane * nv + j] * yj;
-      }
-      if (lane < nv) delta[t * nv + lane] = v;
-      __syncwarp();
+    // z = S^-1 rb: lane b owns entry b; one finished entry broadcast per step
+    double v = (lane < nb) ? rb[lane] : 0.0;
+    for (int j = 0; j < nb; ++j) {
+      const double zj = __shfl_sync(0xffffffffu, v, j) * sdi[j];
+      if (lane == j) v = zj;
+      else if (lane > j && lane < nb) v -= Sb[lane * nb + j] * zj;
     }
-    // backward: L^T dx = y
-    for (int t = T - 1; t >= 0; --t) {
-      double v = 0.0;
-      if (lane < nv) {
-        v = delta[t * nv + lane];
-        if (t + 1 < T) for (int k = 0; k < nv; ++k) v -= E1[t * b2 + k * nv + lane] * delta[(t + 1) * nv + k];
-        if (t + 2 < T) for (int k = 0; k < nv; ++k) v -= E2[t * b2 + k * nv + lane] * delta[(t + 2) * nv + k];
-      }
-      const double* Lt = Ld + t * b2;
-      const double* di = dinvt + t * nv;
-      for (int j = nv - 1; j >= 0; --j) {
-        const double xj = __shfl_sync(0xffffffffu, v, j) * di[j];
-        if (lane == j) v = xj;
-        else if (lane < j) v -= Lt[j * nv + lane] * xj;
-      }
-      __syncwarp();
-      if (lane < nv) delta[t * nv + lane] = v;
-      __syncwarp();
+    for (int j = nb - 1; j >= 0; --j) {
+      const double zj = __shfl_sync(0xffffffffu, v, j) * sdi[j];
+      if (lane == j) v = zj;
+      else if (lane < j) v -= Sb[j * nb + lane] * zj;
     }
+    if (lane < nv) delta[lane] = v;
+    else if (lane < nb) delta[(T - 1) * nv + lane - nv] = v;
+    __syncwarp();
+    // interior: y - u z(knot 0) - w z(knot T-1)
+    for (int e = lane; e < m * nv; e += kWarp) {
+      const int i = e % nv;
+      delta[nv + e] = vy[e] - vu[e] * delta[i] - vw[e] * delta[(T - 1) * nv + i];
+    }
+    __syncwarp();
     return true;
   };
 
@@ -429,14 +466,12 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   int status = BR_IK_MAXITER, flags = 0, it = 0;
   for (; it < S.max_iter; ++it) {
     if (need) { gnorm = build(); need = false; }
-    assemble(lm ? lam : (double)S.gn_eps);
-    if (!factor_solve()) {
+    if (!newton_solve(lm ? lam : (double)S.gn_eps)) {
       flags |= BR_IK_FLAG_REGULARIZED;
       bool ok = false;
       double extra = 1e-9;
       for (int k = 0; k < 8 && !ok; ++k, extra *= 10.0) {
-        assemble((lm ? lam : (double)S.gn_eps) + extra);
-        ok = factor_solve();
+        ok = newton_solve((lm ? lam : (double)S.gn_eps) + extra);
       }
       if (!ok) {
         for (int e = lane; e < n; e += kWarp) delta[e] = 0.0;
