@@ -31,7 +31,7 @@ class BrTree(ctypes.Structure):
                 ("axis", c_void_p), ("placement", c_void_p), ("support", c_void_p),
                 ("frame_parent", c_void_p), ("frame_placement", c_void_p),
                 ("col_joint", c_void_p), ("col_kind", c_void_p), ("col_axis", c_void_p),
-                ("lower", c_void_p), ("upper", c_void_p)]
+                ("lower", c_void_p), ("upper", c_void_p), ("dof_sched", c_void_p)]
 
 
 class IKSettings(ctypes.Structure):
@@ -76,6 +76,7 @@ SIGNATURES: dict[str, tuple] = {
     "br_lm_solve": (c_int32, [ctypes.POINTER(IKBatch), ctypes.POINTER(IKSettings), ctypes.POINTER(IKResultBuf),
                               c_int32, c_void_p, c_int64, c_void_p]),
     "br_lm_team_floats": (c_int64, [ctypes.POINTER(BrTree), c_int32]),
+    "br_dof_schedule": (c_int64, [c_void_p, c_int32, c_void_p, c_int64]),
     "br_lm_solve_noalloc": (c_int32, [ctypes.POINTER(IKBatch), ctypes.POINTER(IKSettings),
                                       ctypes.POINTER(IKResultBuf), c_int32, c_void_p]),
     "br_trajopt_solve": (c_int32, [ctypes.POINTER(BrTree), c_int32, c_int64, c_int32, c_void_p, c_void_p, c_void_p,

@@ -84,7 +84,8 @@ struct TeamLayout {
     n_ent = (ent > 0 && ent < ntri) ? ent : ntri;
     anc_stride = (dep > 0 && dep < nv) ? dep : (nv > 0 ? nv : 1);
     jtj = take(n_ent);                         // J^T J, one row per DOF over its ancestors
-    work = take(6 * nv > n_ent ? 6 * nv : n_ent);  // one target's J columns (build) / the factor (solve)
+    // one target's J columns (build) / the factor and its right-hand-side slots (solve)
+    work = take(6 * nv > n_ent + nv ? 6 * nv : n_ent + nv);
     misc = take(8);
     amask = take(2 * nv);                      // uint64 strict ancestors of each DOF
     dpar = take((nv + 3) / 4);                 // int8 parent DOF (-1 at a root)
@@ -182,7 +183,8 @@ __device__ __forceinline__ Pose to_f(const DPose& P) {
 // prismatic / free-flyer joints) with the other branches folded away; the host launches it
 // whenever a batch needs nothing else.
 template <int T, bool kGeneral>
-__device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm) {
+__device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm,
+                              const uint32_t*& sched_ok) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
   const int K = P.b.max_targets;
   const TeamLayout L(nj, nq, nv, K, T, tree.dof_entries, tree.dof_depth);
@@ -224,7 +226,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   unsigned short* rowoff = reinterpret_cast<unsigned short*>(sm + L.rowoff);
   unsigned char* ancd = reinterpret_cast<unsigned char*>(sm + L.ancd);
   float* dinv = sm + L.dinv;
-  int* misc = reinterpret_cast<int*>(sm + L.misc);  // [0]: the tree's size fields are too small
+  int* misc = reinterpret_cast<int*>(sm + L.misc);  // [0]: the tree's tables are inconsistent; [1]: 1 + max DOF depth
   unsigned char* sup = reinterpret_cast<unsigned char*>(sm + L.sup);
   int* nsup = reinterpret_cast<int*>(sm + L.nsup);
   const int tl = tm.tl;
@@ -234,6 +236,27 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const double kc = S.kernel_param;
   const bool irls = kGeneral && S.kernel != BR_KERNEL_L2;
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
+  // packed lower-triangle pairs p -> (a, b), b <= a, p = tri(a) + b: the lane's first
+  // kPairRegs pair indices (p = tl + T r) decoded once, the rest decoded on the fly
+  constexpr int kPairRegs = 4;
+  auto decode_pair = [](int p) {
+    int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+    if (tri(a + 1) <= p) ++a;
+    if (tri(a) > p) --a;
+    return a | ((p - tri(a)) << 8);
+  };
+  int pdec[kPairRegs];
+#pragma unroll
+  for (int r = 0; r < kPairRegs; ++r) pdec[r] = decode_pair(tl + T * r);
+  auto for_pairs = [&](int np, auto&& f) {
+#pragma unroll
+    for (int r = 0; r < kPairRegs; ++r)
+      if (tl + T * r < np) f(pdec[r] & 0xff, pdec[r] >> 8);
+    for (int p = tl + T * kPairRegs; p < np; p += T) {
+      const int ab = decode_pair(p);
+      f(ab & 0xff, ab >> 8);
+    }
+  };
 
   // ---- load the tree table and the problem -------------------------------
   for (int j = tl; j < nj; j += T) {
@@ -284,13 +307,14 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       for (int k = 0; k < nvj; ++k) dpar[idxv[j] + k] = (signed char)(k == 0 ? prev : idxv[j] + k - 1);
       lastd[j] = nvj ? idxv[j] + nvj - 1 : prev;
     }
-    int nl = 0;
+    int nl = 0, dlev = 0;
     bool bad = false;
     const int As = L.anc_stride;
     for (int c = 0; c < nv; ++c) {
       const int pc = dpar[c];
       const int dc = pc < 0 ? 0 : ddep[pc] + 1;
       ddep[c] = (unsigned char)dc;
+      dlev = dc + 1 > dlev ? dc + 1 : dlev;
       amask[c] = pc < 0 ? 0ull : (amask[pc] | (1ull << pc));
       if (dc > As) {
         bad = true;  // deeper than the tree's dof_depth claims: the ancestor table would overflow
@@ -303,8 +327,43 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     }
     rowoff[nv] = (unsigned short)nl;
     misc[0] = (bad || nl > L.n_ent) ? 1 : 0;
+    misc[1] = dlev;
   }
   tm.sync();
+  // level schedule (br_tree_t.dof_sched): every offset it holds must address this
+  // problem's factor storage; checked once per team and schedule
+  const uint32_t* sched = tree.dof_sched;
+  if (sched && sched != sched_ok && !misc[0]) {
+    const int nL0 = rowoff[nv], lim = nL0 + nv;
+    const int nlev = (int)sched[0], ntask = (int)sched[1], nextra = (int)sched[2];
+    bool bad = nlev < 0 || nlev > nv || ntask < 0 || nextra < 0 || (int)sched[3] != misc[1];
+    if (!bad) {
+      for (int l = tl; l <= nlev; l += T) {
+        const int s0 = (int)sched[4 + l];
+        bad |= (l == 0 && s0 != 0) || (l == nlev && s0 != ntask) || s0 < 0 || s0 > ntask ||
+               (l > 0 && s0 < (int)sched[3 + l]);
+      }
+      const int toff = (5 + nlev + 3) & ~3;
+      const uint4* tk = reinterpret_cast<const uint4*>(sched + toff);
+      const uint2* ex = reinterpret_cast<const uint2*>(sched + toff + 4 * ntask);
+      for (int p = tl; p < ntask; p += T) {
+        const uint4 t4 = tk[p];
+        bad |= (int)(t4.x & 0xffff) >= lim || (int)(t4.y & 0xffff) >= lim || (int)(t4.y >> 16) >= lim ||
+               (int)(t4.z & 0xffff) >= nL0 || (int)(t4.z >> 16) + (int)(t4.x >> 16) > nextra;
+      }
+      for (int e = tl; e < nextra; e += T) {
+        const uint2 e2 = ex[e];
+        bad |= (int)(e2.x & 0xffff) >= lim || (int)(e2.x >> 16) >= lim || (int)e2.y >= nL0;
+      }
+    }
+    bad = __any_sync(tm.mask, bad);
+    if (bad) {
+      if (tl == 0) misc[0] = 1;
+    } else {
+      sched_ok = sched;
+    }
+    tm.sync();
+  }
   if (misc[0]) {  // dof_entries / dof_depth of the tree are smaller than its DOF tree: refuse
     for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = P.b.x0[qoff + i];
     if (tl == 0) {
@@ -517,10 +576,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         }
       }
       for (int p = tl; p < tri(ns); p += T) {
-        int u = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);   // row-major (u >= v) decode of p
-        if (tri(u + 1) <= p) ++u;
-        if (tri(u) > p) --u;
-        const int v = p - tri(u);
+        const int uv = decode_pair(p);                        // row-major (u >= v) decode of p
+        const int u = uv & 0xff, v = uv >> 8;
         float acc = 0.f;
         if (irls) {
 #pragma unroll
@@ -585,7 +642,76 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // added to each pivot as it is read.  d_k > 0 for every k is the test a Cholesky
   // factorization applies.  The triangular solves run in registers (lane tl owns DOFs
   // tl + T r), one shuffle per step.  Returns false if a pivot is not positive and finite.
+  // Level-scheduled factorization: the DOFs of one height in the DOF tree are
+  // eliminated together (tasks of the schedule, one lane each), the right-hand side
+  // -g is updated in the same tasks (forward substitution), then back substitution
+  // runs root first by depth: delta_i = (z_i - sum_a Lm[i][a] delta_anc(i, a)) / D_i.
+  auto solve_levels = [&](float damp) -> bool {
+    float* Lm = work;
+    float* z = work + nL;
+    for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
+    for (int i = tl; i < nv; i += T) z[i] = -g[i];
+    tm.sync();
+    const int nlev = (int)sched[0];
+    const int toff = (5 + nlev + 3) & ~3;
+    const uint4* tasks = reinterpret_cast<const uint4*>(sched + toff);
+    const uint2* extra = reinterpret_cast<const uint2*>(sched + toff + 4 * (int)sched[1]);
+    for (int l = 0; l < nlev; ++l) {
+      const int t1 = (int)__ldg(sched + 5 + l);
+      int p = (int)__ldg(sched + 4 + l) + tl;
+      uint4 nx = p < t1 ? __ldg(tasks + p) : make_uint4(0u, 0u, 0u, 0u);
+      for (; p < t1; p += T) {
+        const uint4 tk = nx;                                   // the next pass's task is in flight
+        if (p + T < t1) nx = __ldg(tasks + p + T);
+        const int dst = tk.x & 0xffff;
+        float acc = fmaf(-Lm[tk.y & 0xffff] * __frcp_rn(Lm[tk.z & 0xffff] + damp), Lm[tk.y >> 16], Lm[dst]);
+        for (int e = (int)(tk.z >> 16), e1 = e + (int)(tk.x >> 16); e < e1; ++e) {
+          const uint2 ex = __ldg(extra + e);
+          acc = fmaf(-Lm[ex.x & 0xffff] * __frcp_rn(Lm[ex.y] + damp), Lm[ex.x >> 16], acc);
+        }
+        Lm[dst] = acc;
+      }
+      tm.sync();
+    }
+    bool bad = false;  // pivots are final once their level is done
+    for (int i = tl; i < nv; i += T) {
+      const float piv = Lm[rowoff[i] + ddep[i]] + damp;
+      bad |= !(piv > 0.f) || !isfinite(piv);
+      dinv[i] = __frcp_rn(piv);
+    }
+    if (__any_sync(tm.mask, bad)) return false;
+    tm.sync();
+    // back substitution by depth, root first: a lane keeps its DOFs' right-hand sides in
+    // registers; once the DOFs of depth dl are final, every deeper DOF subtracts the
+    // term of its one ancestor at depth dl (no two lanes write the same DOF)
+    constexpr int R = lm_rows(T);
+    float zr[R], dvr[R];
+    int dr[R], ror[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = tl + T * r;
+      const bool in = i < nv;
+      zr[r] = in ? z[i] : 0.f;
+      dvr[r] = in ? dinv[i] : 0.f;
+      dr[r] = in ? ddep[i] : -1;
+      ror[r] = in ? rowoff[i] : 0;
+    }
+    const int ndl = misc[1];
+    for (int dl = 0; dl < ndl; ++dl) {
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (dr[r] == dl) delta[tl + T * r] = zr[r] * dvr[r];
+      tm.sync();
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (dr[r] > dl) zr[r] = fmaf(-Lm[ror[r] + dl], delta[ancd[(tl + T * r) * L.anc_stride + dl]], zr[r]);
+    }
+    tm.sync();
+    return true;
+  };
+
   auto solve = [&](float damp) -> bool {
+    if (sched) return solve_levels(damp);
     float* Lm = work;
     for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
     tm.sync();
@@ -593,17 +719,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       const int dk = ddep[k], rk = rowoff[k];
       const float piv = Lm[rk + dk] + damp;
       if (!(piv > 0.f) || !isfinite(piv)) return false;  // every lane read the same pivot
-      const float inv = 1.f / piv;
+      const float inv = __frcp_rn(piv);                      // == 1.f / piv
       if (tl == 0) dinv[k] = inv;
       const unsigned char* anc = ancd + k * L.anc_stride;
-      for (int p = tl; p < tri(dk); p += T) {                // pairs (a, b), b <= a < dk, by depth
-        int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
-        if (tri(a + 1) <= p) ++a;
-        if (tri(a) > p) --a;
-        const int b = p - tri(a);
+      for_pairs(tri(dk), [&](int a, int b) {                 // pairs (a, b), b <= a < dk, by depth
         float* dst = Lm + rowoff[anc[a]] + b;
         *dst = fmaf(-Lm[rk + a] * inv, Lm[rk + b], *dst);
-      }
+      });
       tm.sync();
     }
     constexpr int R = lm_rows(T);  // DOFs per lane
@@ -789,7 +911,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
 }
 
 template <int T, bool kGeneral>
-__device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, int count, float* wsm, int lane) {
+__device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, int count, float* wsm, int lane,
+                                         const uint32_t*& sched_ok) {
   const int team = lane / T;
   Team<T> tm;
   tm.tl = lane % T;
@@ -798,7 +921,7 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
   const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T, tree.dof_entries, tree.dof_depth);
   if (team < count) {
     const int prob = P.b.order[first + team];
-    solve_problem<T, kGeneral>(P, tree, prob, wsm + team * L.total, tm);
+    solve_problem<T, kGeneral>(P, tree, prob, wsm + team * L.total, tm, sched_ok);
   }
 }
 
@@ -808,6 +931,7 @@ __global__ void lm_solve_kernel(const LmParams P) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   float* wsm = smem + (size_t)warp * P.warp_floats;
+  const uint32_t* sched_ok = nullptr;  // the level schedule this team has checked
   for (;;) {
     int item = 0;
     if (lane == 0) item = atomicAdd(P.queue, 1);
@@ -817,7 +941,7 @@ __global__ void lm_solve_kernel(const LmParams P) {
     // One instantiation: 32-lane teams.  8- and 16-lane teams (several small problems per
     // warp) were measured slower on the mixed batch: three copies of this kernel body
     // overflow the instruction cache, and 32 lanes are the fastest per class on their own.
-    run_item<kLmTeam, kGeneral>(P, cls, first, count, wsm, lane);
+    run_item<kLmTeam, kGeneral>(P, cls, first, count, wsm, lane, sched_ok);
     __syncwarp();
   }
 }

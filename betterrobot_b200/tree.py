@@ -122,6 +122,7 @@ class TreeArrays:
         # ancestor joint with DOFs): J^T J entries per DOF = depth + 1
         lastd = np.full(nj, -1, np.int64)
         ddep = np.zeros(nv, np.int64)
+        self.dof_parent = np.full(nv, -1, np.int32)
         for j in range(nj):
             p = parents[j]
             prev = lastd[p] if p >= 0 else -1
@@ -129,6 +130,7 @@ class TreeArrays:
             for k in range(nvj):
                 c = int(self.idx_v[j]) + k
                 pc = prev if k == 0 else c - 1
+                self.dof_parent[c] = pc
                 ddep[c] = 0 if pc < 0 else ddep[pc] + 1
             lastd[j] = int(self.idx_v[j]) + nvj - 1 if nvj else prev
         self.dof_entries = int((ddep + 1).sum())
@@ -143,10 +145,24 @@ class TreeArrays:
                 ("col_joint", self.col_joint), ("col_kind", self.col_kind), ("col_axis", self.col_axis),
                 ("lower", self.lower), ("upper", self.upper)]
 
-    def blob(self) -> tuple[np.ndarray, dict]:
+    def dof_schedule(self) -> np.ndarray:
+        """The LM's level schedule over the DOF tree (``br_dof_schedule``, host code of the library)."""
+        from . import _lib
+        lib = _lib.load()
+        dp = np.ascontiguousarray(self.dof_parent)
+        n = lib.br_dof_schedule(dp.ctypes.data, self.nv, None, 0)
+        if n < 0:
+            raise ModelInconsistencyError(f"br_dof_schedule failed ({n})")
+        out = np.zeros(max(int(n), 4), np.uint32)
+        n2 = lib.br_dof_schedule(dp.ctypes.data, self.nv, out.ctypes.data, out.size)
+        if n2 != n:
+            raise ModelInconsistencyError(f"br_dof_schedule failed ({n2})")
+        return out
+
+    def blob(self, extra=()) -> tuple[np.ndarray, dict]:
         """One byte buffer with 16-byte aligned sections, and their offsets."""
         offs, parts, o = {}, [], 0
-        for name, arr in self.sections():
+        for name, arr in [*self.sections(), *extra]:
             b = np.ascontiguousarray(arr).tobytes()
             offs[name] = o
             pad = (-len(b)) % 16
@@ -162,7 +178,8 @@ class DeviceTree:
     def __init__(self, model, device: torch.device):
         self.model = model
         self.arrays = TreeArrays(model)
-        buf, offs = self.arrays.blob()
+        sched = self.arrays.dof_schedule() if self.arrays.nv else None
+        buf, offs = self.arrays.blob([("dof_sched", sched)] if sched is not None else [])
         self.buffer = torch.from_numpy(buf).to(device)
         base = self.buffer.data_ptr()
         a = self.arrays
@@ -172,6 +189,7 @@ class DeviceTree:
         st.dof_entries, st.dof_depth = a.dof_entries, a.dof_depth
         for name, _ in a.sections():
             setattr(st, name, base + offs[name])
+        st.dof_sched = base + offs["dof_sched"] if sched is not None else None
         self.struct = st
         self.ptr = ctypes.pointer(st)
         self.device = device

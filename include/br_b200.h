@@ -87,7 +87,38 @@ typedef struct br_tree {
     const float* col_axis;          /* [nv*4]      column axis in its joint's frame */
     const float* lower;             /* [nq]        position limits (+-inf allowed) */
     const float* upper;             /* [nq]                                        */
+    const uint32_t* dof_sched;      /* elimination schedule of the LM's J^T J factorization
+                                       (br_dof_schedule), or NULL: the LM then eliminates one
+                                       DOF at a time                                        */
 } br_tree_t;
+
+/*
+ * Level schedule for the LM's factorization of J^T J + damp I over the DOF tree
+ * (tangent column c's parent is the previous column of its joint, or the last
+ * column of the nearest ancestor joint with columns; dof_parent[c] < c, -1 at a
+ * root).  The matrix is stored one row per DOF over its ancestors by depth; DOFs
+ * are eliminated leaves first, and all DOFs of one height in the DOF tree (0 at a
+ * leaf, 1 + the children's maximum above) at once: no two of them is an ancestor of
+ * the other, so within a level the rows read and the rows written are disjoint.  An
+ * entry that several DOFs of one level update (a pair of common ancestors) is one
+ * task that sums their contributions in a fixed order, so the result does not depend
+ * on scheduling.  The right-hand side rides along as one extra slot per DOF (forward
+ * substitution inside the factorization).
+ *
+ * Layout (uint32 words): [0] levels, [1] tasks, [2] extra contributions, [3] 1 + the
+ * deepest DOF depth, [4 .. 4 + levels] first task of each level (the last = tasks),
+ * then at word toff = roundup(5 + levels, 4) the tasks, 4 words each:
+ *   {dst | (n_extra << 16), a | (b << 16), d | (first_extra << 16), 0}
+ *   dst -= m[a] * m[b] / (m[d] + damp), then the same for each extra contribution,
+ * then at toff + 4 * tasks the extra contributions, 2 words each: {a | (b << 16), d}.
+ * Offsets index the packed rows (row c starts at sum_{c' < c} (depth(c') + 1), its
+ * diagonal at depth(c)) followed by the nv right-hand-side slots.
+ *
+ * Writes the schedule to `out` (HOST, `capacity` words) when it fits and returns
+ * the number of words it needs, or BR_EINVAL (bad dof_parent) / BR_ETOOBIG (more
+ * than 65,535 packed offsets or extra contributions).  Host-only: no device work.
+ */
+BR_API int64_t br_dof_schedule(const int32_t* dof_parent, int32_t nv, uint32_t* out, int64_t capacity);
 
 /*
  * Forward kinematics for `batch` configurations q[batch, nq].

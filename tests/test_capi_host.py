@@ -38,9 +38,10 @@ def test_library_loads_and_exports_every_declared_symbol():
 
 
 def test_tree_struct_layout_matches_header():
-    # 5 int32 + 3 reserved, then 14 pointers
-    assert ctypes.sizeof(_lib.BrTree) == 32 + 14 * 8
+    # 8 int32 (sizes, rounds, kinds, dof_entries, dof_depth), then 14 table pointers and dof_sched
+    assert ctypes.sizeof(_lib.BrTree) == 32 + 15 * 8
     assert _lib.BrTree.parent.offset == 32
+    assert _lib.BrTree.dof_sched.offset == 32 + 14 * 8
 
 
 @pytest.mark.parametrize("spec", [syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()])
