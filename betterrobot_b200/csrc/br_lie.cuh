@@ -148,6 +148,38 @@ __device__ __forceinline__ float4 so3_exp(float3 w) {
   return make_float4(k * w.x, k * w.y, k * w.z, cw);
 }
 
+// se3_exp for an LM increment: the same map, evaluated without trigonometric calls for
+// |w| < 1 rad (Taylor series of b, c above and of sin(th/2)/th, cos(th/2), truncated where
+// the next term is below float32 rounding) and with sincospif beyond.
+__device__ __forceinline__ Pose se3_exp_step(float3 v, float3 w) {
+  const float th2 = dot(w, w);
+  float b, c, k, cw;
+  if (th2 < 1.f) {
+    b = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 3628800.f, -1.f / 40320.f), 1.f / 720.f), -1.f / 24.f), 0.5f);
+    c = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 39916800.f, -1.f / 362880.f), 1.f / 5040.f), -1.f / 120.f),
+             1.f / 6.f);
+    const float x2 = 0.25f * th2;  // (th / 2)^2
+    // sin(x)/x = 1 - x^2/6 + x^4/120 - x^6/5040 + x^8/362880; k = sin(th/2)/th = (sin(x)/x) / 2
+    k = 0.5f * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 1.f / 362880.f, -1.f / 5040.f), 1.f / 120.f), -1.f / 6.f), 1.f);
+    // cos(x) = 1 - x^2/2 + x^4/24 - x^6/720 + x^8/40320 - x^10/3628800
+    cw = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -1.f / 3628800.f, 1.f / 40320.f), -1.f / 720.f), 1.f / 24.f),
+                   -0.5f), 1.f);
+  } else {
+    const float th = sqrtf(th2);
+    float s, co, sh;
+    sincospif(th * (1.f / 3.14159265358979f), &s, &co);
+    sincospif(th * (0.5f / 3.14159265358979f), &sh, &cw);
+    b = 2.f * sh * sh / th2;
+    c = (th - s) / (th * th2);
+    k = sh / th;
+  }
+  const float3 wv = cross(w, v);
+  Pose T;
+  T.t = axpy(c, cross(w, wv), axpy(b, wv, v));
+  T.q = make_float4(k * w.x, k * w.y, k * w.z, cw);
+  return T;
+}
+
 // se3_exp (_torch_native_backend.py:258-286): T = (V(w) v, exp(w))
 __device__ __forceinline__ Pose se3_exp(float3 v, float3 w) {
   float b, c;

@@ -811,9 +811,19 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         clampq(k, c);
         clampq(k + 1, s);
       } else if (jt == BR_JOINT_FREE_FLYER) {                        // free_flyer.py:47-51
+        // plain variant: the float32 step's exponential in float32 (its rounding is relative
+        // to the step), composed with the float64 iterate in float64; the general variant
+        // keeps the float64 exponential
         const DPose a{d3(x[iq], x[iq + 1], x[iq + 2]), make_double4(x[iq + 3], x[iq + 4], x[iq + 5], x[iq + 6])};
-        DPose n = dcompose(a, dse3_exp(d3(delta[iv], delta[iv + 1], delta[iv + 2]),
-                                       d3(delta[iv + 3], delta[iv + 4], delta[iv + 5])));
+        DPose inc;
+        if (kGeneral) {
+          inc = dse3_exp(d3(delta[iv], delta[iv + 1], delta[iv + 2]), d3(delta[iv + 3], delta[iv + 4], delta[iv + 5]));
+        } else {
+          const Pose e = se3_exp_step(f3(delta[iv], delta[iv + 1], delta[iv + 2]),
+                                      f3(delta[iv + 3], delta[iv + 4], delta[iv + 5]));
+          inc = DPose{d3(e.t.x, e.t.y, e.t.z), make_double4(e.q.x, e.q.y, e.q.z, e.q.w)};
+        }
+        DPose n = dcompose(a, inc);
         n.q = dqnormalize(n.q);
         const double v7[7] = {n.t.x, n.t.y, n.t.z, n.q.x, n.q.y, n.q.z, n.q.w};
         for (int k = 0; k < 7; ++k) xn[iq + k] = fmin(fmax(v7[k], (double)lower[iq + k]), (double)upper[iq + k]);
