@@ -833,59 +833,79 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   };
 
   // ---- the LM / GN loop (levenberg_marquardt.py:83-135, gauss_newton.py:27-76) ----
+  // fk, residual and solve each have ONE call site (they are inlined lambdas: a second
+  // site would duplicate their code and the kernel's instruction footprint): the first
+  // pass evaluates the start, every later pass the trial point of one iteration, and a
+  // last pass re-evaluates x when the stacked residual is wanted and the final trial
+  // point was rejected.
   const bool gn = S.optimizer == BR_OPT_GN;
-  double* pose = fk(x);
-  double cost = residual(x, pose);
+  const bool want_residual = P.r.residual && P.b.r_offset;
   float lam = gn ? 0.f : S.lam0;
   float gnorm = 0.f;
-  bool need_jac = true;
-  int flags = isfinite(cost) ? 0 : BR_IK_FLAG_NONFINITE;
+  double cost = 0.0;
+  bool need_jac = true, started = false, final_pass = false, last_at_x = true;
+  int flags = 0;
   int status = BR_IK_MAXITER;
   int it = 0;
-  for (; it < S.max_iter; ++it) {
-    if (need_jac) {
+  const double* xe = x;  // the point the next pass evaluates
+  for (;;) {
+    double* pose = fk(xe);
+    const double cn = residual(xe, pose);
+    if (final_pass) break;
+    if (!started) {
+      started = true;
+      cost = cn;
+      flags = isfinite(cost) ? 0 : BR_IK_FLAG_NONFINITE;
+    } else {
+      ++it;
+      if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
+      if (gn || cn < cost) {
+        for (int i = tl; i < nq; i += T) x[i] = xn[i];
+        tm.sync();
+        cost = cn;
+        if (!gn) lam = fmaxf(lam / S.factor, S.lam_min);
+        need_jac = true;
+        last_at_x = true;
+        if (gnorm < S.tol) { status = BR_IK_CONVERGED; break; }
+      } else {
+        lam = fminf(lam * S.factor, S.lam_max);
+        last_at_x = false;
+      }
+    }
+    if (it >= S.max_iter) {
+      if (want_residual && !last_at_x) {
+        final_pass = true;
+        xe = x;
+        continue;
+      }
+      break;
+    }
+    if (need_jac) {  // pose holds FK(x) here: x was the last point evaluated and kept
       gnorm = build_normal(x, pose);
       need_jac = false;
     }
     const float damp = gn ? S.gn_eps : lam;
-    bool ok = solve(damp);
-    if (!ok) {
-      // float32 factorization failed: add diagonal regularisation (x10 per retry)
+    // a failed float32 factorization is retried with diagonal regularisation 1e-6 .. 1e-1
+    bool ok = false;
+    float extra = 0.f;
+    for (int k = 0; k < 7; ++k) {
+      ok = solve(damp + extra);
+      if (ok) break;
       flags |= BR_IK_FLAG_REGULARIZED;
-      float extra = 1e-6f;
-      for (int k = 0; k < 6 && !ok; ++k, extra *= 10.f) ok = solve(damp + extra);
-      if (!ok) {
-        for (int i = tl; i < nv; i += T) delta[i] = 0.f;
-        tm.sync();
-      }
+      extra = k == 0 ? 1e-6f : extra * 10.f;
+    }
+    if (!ok) {
+      for (int i = tl; i < nv; i += T) delta[i] = 0.f;
+      tm.sync();
     }
     retract();
-    pose = fk(xn);
-    const double cn = residual(xn, pose);
-    if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
-    if (gn) {
-      for (int i = tl; i < nq; i += T) x[i] = xn[i];
-      tm.sync();
-      cost = cn;
-      need_jac = true;
-      if (gnorm < S.tol) { status = BR_IK_CONVERGED; ++it; break; }
-    } else if (cn < cost) {
-      for (int i = tl; i < nq; i += T) x[i] = xn[i];
-      tm.sync();
-      cost = cn;
-      lam = fmaxf(lam / S.factor, S.lam_min);
-      need_jac = true;
-      if (gnorm < S.tol) { status = BR_IK_CONVERGED; ++it; break; }
-    } else {
-      lam = fminf(lam * S.factor, S.lam_max);
-    }
+    xe = xn;
   }
   // ---- results ------------------------------------------------------------
   for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = (float)x[i];
-  if (P.r.residual && P.b.r_offset) {
-    // stacked residual at the returned x, CostStack order (stack.py:104-117)
-    pose = fk(x);
-    residual(x, pose);
+  if (want_residual) {
+    // stacked residual at the returned x, CostStack order (stack.py:104-117); the residual
+    // buffers hold x's values (last pass above)
     float* out = P.r.residual + P.b.r_offset[prob];
     int o = 0;  // rows of the targets: 6 per pose, 3 per position or orientation target
     for (int t = 0; t < nt; ++t) {
@@ -936,7 +956,7 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
 }
 
 template <bool kGeneral>
-__global__ void lm_solve_kernel(const LmParams P) {
+__global__ void __maxnreg__(128) lm_solve_kernel(const LmParams P) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
