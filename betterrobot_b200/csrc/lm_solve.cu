@@ -19,8 +19,10 @@
 //     pose Jacobian Jr^-1(xi) blockdiag(R^T, R^T) J_lwa (pose.py:68-103) with columns
 //     outside a target's support skipped;
 //   * H = J^T J + lambda I, stored per DOF over its ancestors in the DOF tree,
-//     factored leaves first as an unscaled LDL^T (no fill-in), triangular solves
-//     in registers with one shuffle per step;
+//     factored leaves first as an unscaled LDL^T (no fill-in), all DOFs of one
+//     height in the DOF tree at once (br_tree_t.dof_sched, built on the host by
+//     br_dof_schedule), the right-hand side updated in the same tasks, back
+//     substitution by depth with the right-hand sides in registers;
 //   * retraction q (+) dq (Model.integrate, model.py:160-174) and clamping to the
 //     joint limits (levenberg_marquardt.py:103-107).
 //
@@ -236,26 +238,12 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const double kc = S.kernel_param;
   const bool irls = kGeneral && S.kernel != BR_KERNEL_L2;
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
-  // packed lower-triangle pairs p -> (a, b), b <= a, p = tri(a) + b: the lane's first
-  // kPairRegs pair indices (p = tl + T r) decoded once, the rest decoded on the fly
-  constexpr int kPairRegs = 4;
+  // packed lower-triangle pair p -> (a, b), b <= a, p = tri(a) + b
   auto decode_pair = [](int p) {
     int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
     if (tri(a + 1) <= p) ++a;
     if (tri(a) > p) --a;
     return a | ((p - tri(a)) << 8);
-  };
-  int pdec[kPairRegs];
-#pragma unroll
-  for (int r = 0; r < kPairRegs; ++r) pdec[r] = decode_pair(tl + T * r);
-  auto for_pairs = [&](int np, auto&& f) {
-#pragma unroll
-    for (int r = 0; r < kPairRegs; ++r)
-      if (tl + T * r < np) f(pdec[r] & 0xff, pdec[r] >> 8);
-    for (int p = tl + T * kPairRegs; p < np; p += T) {
-      const int ab = decode_pair(p);
-      f(ab & 0xff, ab >> 8);
-    }
   };
 
   // ---- load the tree table and the problem -------------------------------
@@ -332,8 +320,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   tm.sync();
   // level schedule (br_tree_t.dof_sched): every offset it holds must address this
   // problem's factor storage; checked once per team and schedule
-  const uint32_t* sched = tree.dof_sched;
-  if (sched && sched != sched_ok && !misc[0]) {
+  const uint32_t* sched = tree.dof_sched;  // non-null: checked on the host
+  if (sched != sched_ok && !misc[0]) {
     const int nL0 = rowoff[nv], lim = nL0 + nv;
     const int nlev = (int)sched[0], ntask = (int)sched[1], nextra = (int)sched[2];
     bool bad = nlev < 0 || nlev > nv || ntask < 0 || nextra < 0 || (int)sched[3] != misc[1];
@@ -646,7 +634,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // eliminated together (tasks of the schedule, one lane each), the right-hand side
   // -g is updated in the same tasks (forward substitution), then back substitution
   // runs root first by depth: delta_i = (z_i - sum_a Lm[i][a] delta_anc(i, a)) / D_i.
-  auto solve_levels = [&](float damp) -> bool {
+  auto solve = [&](float damp) -> bool {
     float* Lm = work;
     float* z = work + nL;
     for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
@@ -705,83 +693,6 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
 #pragma unroll
       for (int r = 0; r < R; ++r)
         if (dr[r] > dl) zr[r] = fmaf(-Lm[ror[r] + dl], delta[ancd[(tl + T * r) * L.anc_stride + dl]], zr[r]);
-    }
-    tm.sync();
-    return true;
-  };
-
-  auto solve = [&](float damp) -> bool {
-    if (sched) return solve_levels(damp);
-    float* Lm = work;
-    for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
-    tm.sync();
-    for (int k = nv - 1; k >= 0; --k) {
-      const int dk = ddep[k], rk = rowoff[k];
-      const float piv = Lm[rk + dk] + damp;
-      if (!(piv > 0.f) || !isfinite(piv)) return false;  // every lane read the same pivot
-      const float inv = __frcp_rn(piv);                      // == 1.f / piv
-      if (tl == 0) dinv[k] = inv;
-      const unsigned char* anc = ancd + k * L.anc_stride;
-      for_pairs(tri(dk), [&](int a, int b) {                 // pairs (a, b), b <= a < dk, by depth
-        float* dst = Lm + rowoff[anc[a]] + b;
-        *dst = fmaf(-Lm[rk + a] * inv, Lm[rk + b], *dst);
-      });
-      tm.sync();
-    }
-    constexpr int R = lm_rows(T);  // DOFs per lane
-    float z[R], dv[R];
-    int rd[R];  // rowoff | ddep << 16 of the lane's DOFs
-    unsigned long long am[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = tl + T * r;
-      const bool in = i < nv;
-      z[r] = in ? -g[i] : 0.f;
-      dv[r] = in ? dinv[i] : 0.f;
-      rd[r] = in ? (rowoff[i] | (ddep[i] << 16)) : 0;
-      am[r] = in ? amask[i] : 0ull;
-    }
-    // leaves first: w_k = u_k / d_k, then u_i -= A_ki w_k for the ancestors i of k
-    for (int k = nv - 1; k >= 0; --k) {
-      const int rk = k / T, own = k % T, rowk = rowoff[k];
-      const unsigned long long mk = amask[k];
-      float a[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int i = tl + T * r;
-        a[r] = (i < nv && ((mk >> i) & 1ull)) ? Lm[rowk + (rd[r] >> 16)] : 0.f;
-      }
-      float zk = z[0], dk = dv[0];
-#pragma unroll
-      for (int r = 1; r < R; ++r)
-        if (r == rk) { zk = z[r]; dk = dv[r]; }
-      const float wk = tm.bcast(zk * dk, own);
-      if (tl == own) {
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          if (r == rk) z[r] = wk;
-      }
-#pragma unroll
-      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], wk, z[r]);
-    }
-    // ancestors first: delta_i is final, then w_m -= (A_mi / d_m) delta_i for the descendants m of i
-    for (int i = 0; i < nv; ++i) {
-      const int ri = i / T, di = ddep[i];
-      float a[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) a[r] = ((am[r] >> i) & 1ull) ? Lm[(rd[r] & 0xffff) + di] * dv[r] : 0.f;
-      float zi = z[0];
-#pragma unroll
-      for (int r = 1; r < R; ++r)
-        if (r == ri) zi = z[r];
-      const float xv = tm.bcast(zi, i % T);
-#pragma unroll
-      for (int r = 0; r < R; ++r) z[r] = fmaf(-a[r], xv, z[r]);
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = tl + T * r;
-      if (i < nv) delta[i] = z[r];
     }
     tm.sync();
     return true;
@@ -1010,6 +921,7 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
   for (int c = 0; c < b.n_classes; ++c) {
     const int st = validate_tree(&b.trees[c]);
     if (st) return st;
+    if (!b.trees[c].dof_sched) return BR_EINVAL;           // the factorization's level schedule
     const int T = b.team_size[c];
     if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
     p.trees[c] = b.trees[c];
@@ -1122,6 +1034,7 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
   for (int c = 0; c < b.n_classes; ++c) {
     st = validate_tree(&b.trees[c]);
     if (st) return st;
+    if (!b.trees[c].dof_sched) return BR_EINVAL;           // the factorization's level schedule
     const int T = b.team_size[c];
     if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
     p.trees[c] = b.trees[c];

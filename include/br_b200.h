@@ -87,9 +87,10 @@ typedef struct br_tree {
     const float* col_axis;          /* [nv*4]      column axis in its joint's frame */
     const float* lower;             /* [nq]        position limits (+-inf allowed) */
     const float* upper;             /* [nq]                                        */
-    const uint32_t* dof_sched;      /* elimination schedule of the LM's J^T J factorization
-                                       (br_dof_schedule), or NULL: the LM then eliminates one
-                                       DOF at a time                                        */
+    const uint32_t* dof_sched;      /* level schedule of the LM's J^T J factorization
+                                       (br_dof_schedule, copied to the device); required by
+                                       br_lm_solve / br_lm_solve_noalloc (BR_EINVAL if NULL),
+                                       unused by the other entry points                      */
 } br_tree_t;
 
 /*
@@ -224,7 +225,9 @@ typedef struct br_ik_result {
  * launch.  Replaces solve_ik (src/better_robot/tasks/ik.py:150-266) called once
  * per problem, i.e. LevenbergMarquardt.minimize / GaussNewton.minimize
  * (optim/optimizers/levenberg_marquardt.py:61-135, gauss_newton.py:27-76) over
- * the pose + limit + rest CostStack.
+ * the pose + limit + rest CostStack.  Every class tree must carry its level schedule
+ * (br_tree_t.dof_sched); a schedule whose offsets do not fit the tree's DOF tree makes
+ * the class's problems return BR_IK_FLAG_BADTREE.
  */
 BR_API int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
                        int32_t warps_per_cta, void* scratch, int64_t scratch_bytes, void* stream);
