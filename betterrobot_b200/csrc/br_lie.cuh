@@ -361,10 +361,11 @@ __device__ __forceinline__ void dse3_log(const DPose& T, double3& v, double3& w)
   if (th2 < 1e-8) {
     c = 1.0 / 12.0 + th2 / 720.0;
   } else {
+    // c = 1/th^2 - cot(th/2) / (2 th); with th = 2 atan2(|q_xyz|, |q_w|) (dso3_log),
+    // cot(th/2) = |q_w| / |q_xyz| exactly: no trigonometric call
     const double th = sqrt(th2);
-    double sh, ch;
-    sincos(0.5 * th, &sh, &ch);
-    c = 1.0 / th2 - (ch / sh) / (2.0 * th);
+    const double s = sqrt(T.q.x * T.q.x + T.q.y * T.q.y + T.q.z * T.q.z);
+    c = 1.0 / th2 - (fabs(T.q.w) / s) / (2.0 * th);
   }
   const double3 wt = dcross(w, T.t);
   v = dadd(dadd(T.t, dscale(wt, -0.5)), dscale(dcross(w, wt), c));

@@ -413,35 +413,37 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // float64 residual of the stack at q with world poses `pose`: fills tw, xi, dr; returns 0.5 |r|^2.
   auto residual = [&](const double* q, const double* pose) -> double {
     double acc = 0.0;
-    for (int t = tl; t < nt; t += T) {
-      const DPose Tee = dcompose(lds(pose, nj, fparent[t]), to_d(ld8(fplace + 8 * t)));
-      std8(tw + 8 * t, Tee);
-      double* e = xi + 8 * t;
-      const DPose Tt = ldd(tgt + 8 * t);
-      const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
-      if (kind == BR_TARGET_POSITION) {                              // pose.py:127-131
-        const double3 dp = dsub(Tee.t, Tt.t);
-        e[0] = dp.x; e[1] = dp.y; e[2] = dp.z; e[3] = 0.0; e[4] = 0.0; e[5] = 0.0;
-        acc += wpd * wpd * ddot(dp, dp);
-      } else if (kind == BR_TARGET_ORIENTATION) {                    // pose.py:165-173
-        const double3 w = dso3_log(dqmul(dqconj(Tt.q), Tee.q));
-        e[0] = 0.0; e[1] = 0.0; e[2] = 0.0; e[3] = w.x; e[4] = w.y; e[5] = w.z;
-        acc += wod * wod * ddot(w, w);
-      } else {
-        double3 v, w;
-        dse3_log(dcompose(dinverse(Tt), Tee), v, w);                 // pose.py:63-64
-        e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = w.x; e[4] = w.y; e[5] = w.z;
-        acc += wpd * wpd * ddot(v, v) + wod * wod * ddot(w, w);
-      }
-    }
-    if (use_limits) {                                                // limits.py:56-62
-      for (int i = tl; i < nq; i += T) {
-        const double lo = fmax((double)lower[i] - q[i], 0.0), hi = fmax(q[i] - (double)upper[i], 0.0);
-        acc += wld * wld * (lo * lo + hi * hi);
-      }
-    }
-    if (use_rest) {                                                  // regularization.py:48-54
-      for (int j = tl; j < nj; j += T) {
+    // one pass over the targets (jobs 0..nt-1) and, for the rest term, the joints (jobs
+    // nt..nt+nj-1), so that the SE3 log of pose targets and free-flyer rest residuals has
+    // one call site
+    const int njobs = nt + (use_rest ? nj : 0);
+    for (int jb = tl; jb < njobs; jb += T) {
+      DPose rel;
+      double* out = nullptr;  // 6 slots [v, w] when rel's SE3 log is wanted
+      double wv = 0.0, ww = 0.0;
+      if (jb < nt) {
+        const int t = jb;
+        const DPose Tee = dcompose(lds(pose, nj, fparent[t]), to_d(ld8(fplace + 8 * t)));
+        std8(tw + 8 * t, Tee);
+        double* e = xi + 8 * t;
+        const DPose Tt = ldd(tgt + 8 * t);
+        const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
+        if (kind == BR_TARGET_POSITION) {                            // pose.py:127-131
+          const double3 dp = dsub(Tee.t, Tt.t);
+          e[0] = dp.x; e[1] = dp.y; e[2] = dp.z; e[3] = 0.0; e[4] = 0.0; e[5] = 0.0;
+          acc += wpd * wpd * ddot(dp, dp);
+        } else if (kind == BR_TARGET_ORIENTATION) {                  // pose.py:165-173
+          const double3 w = dso3_log(dqmul(dqconj(Tt.q), Tee.q));
+          e[0] = 0.0; e[1] = 0.0; e[2] = 0.0; e[3] = w.x; e[4] = w.y; e[5] = w.z;
+          acc += wod * wod * ddot(w, w);
+        } else {
+          rel = dcompose(dinverse(Tt), Tee);                         // pose.py:63-64
+          out = e;
+          wv = wpd;
+          ww = wod;
+        }
+      } else {                                                       // regularization.py:48-54
+        const int j = jb - nt;
         const int jt = jtype[j];
         const int iq = idxq[j], iv = idxv[j];
         if (kGeneral ? joint_is_vector(jt) : (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC)) {
@@ -471,12 +473,23 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           const DPose a{d3(qrest[iq], qrest[iq + 1], qrest[iq + 2]),
                         make_double4(qrest[iq + 3], qrest[iq + 4], qrest[iq + 5], qrest[iq + 6])};
           const DPose b{d3(q[iq], q[iq + 1], q[iq + 2]), make_double4(q[iq + 3], q[iq + 4], q[iq + 5], q[iq + 6])};
-          double3 v, w;
-          dse3_log(dcompose(dinverse(a), b), v, w);
-          dr[iv] = v.x; dr[iv + 1] = v.y; dr[iv + 2] = v.z;
-          dr[iv + 3] = w.x; dr[iv + 4] = w.y; dr[iv + 5] = w.z;
-          acc += wrd * wrd * (ddot(v, v) + ddot(w, w));
+          rel = dcompose(dinverse(a), b);
+          out = dr + iv;
+          wv = wrd;
+          ww = wrd;
         }
+      }
+      if (out) {
+        double3 v, w;
+        dse3_log(rel, v, w);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = w.x; out[4] = w.y; out[5] = w.z;
+        acc += wv * wv * ddot(v, v) + ww * ww * ddot(w, w);
+      }
+    }
+    if (use_limits) {                                                // limits.py:56-62
+      for (int i = tl; i < nq; i += T) {
+        const double lo = fmax((double)lower[i] - q[i], 0.0), hi = fmax(q[i] - (double)upper[i], 0.0);
+        acc += wld * wld * (lo * lo + hi * hi);
       }
     }
 #pragma unroll

@@ -253,9 +253,12 @@ def test_autotune_and_graph_replay_match_direct_solve():
 
 @pytest.mark.parametrize("kernel", ["huber", "cauchy", "tukey"])
 def test_robust_kernels_vs_oracle(kernel):
-    """IRLS-reweighted LM on noisy humanoid starts against the oracle's float64 IRLS LM."""
+    """IRLS-reweighted LM on noisy humanoid starts against the oracle's float64 IRLS LM.
+
+    128 problems: verdict agreement sits at the float32 floor (~0.93 measured over the three
+    kernels and l2), and with 64 problems one binomial standard deviation is 3 points."""
     m, m64 = _models("humanoid")
-    P = 64
+    P = 128
     fids = [m.frame_id(f) for f in ("track0", "track2", "track4")]
     q_star = syn.random_q(m64, P, 80, rev_range=2.5, base_translation=0.5)
     oMi, _ = K.forward_kinematics(m64, q_star.numpy())
