@@ -69,7 +69,7 @@ extern "C" int64_t br_dof_schedule(const int32_t* dof_parent, int32_t nv, uint32
     };
     for (int k = nv - 1; k >= 0; --k) {  // descending DOF index: the one-at-a-time order
       if (height[k] != lev) continue;
-      const uint32_t rk = (uint32_t)rowoff[k], d = rk + (uint32_t)dep[k];
+      const uint32_t rk = (uint32_t)rowoff[k], d = (uint32_t)k;
       for (int a = 0; a < dep[k]; ++a)
         for (int b = 0; b <= a; ++b) add((uint32_t)(rowoff[anc[k][a]] + b), {rk + a, rk + b, d});
       for (int a = 0; a < dep[k]; ++a) add(zoff + (uint32_t)anc[k][a], {rk + a, zoff + (uint32_t)k, d});
@@ -90,6 +90,17 @@ extern "C" int64_t br_dof_schedule(const int32_t* dof_parent, int32_t nv, uint32
   }
   const uint32_t n_tasks = (uint32_t)(tasks.size() / 4);
   starts.push_back(n_tasks);
+  // the last task that updates DOF k's diagonal finalises its pivot: flag it (word 3 = k + 1)
+  // so that the lane running it also stores 1 / (pivot + damp) for the levels above
+  std::vector<int64_t> last(nv, -1);
+  for (uint32_t p = 0; p < n_tasks; ++p) {
+    const int dst = (int)(tasks[4 * p] & 0xffff);
+    if (dst >= nl) continue;
+    const int k = (int)(std::upper_bound(rowoff.begin(), rowoff.begin() + nv, dst) - rowoff.begin()) - 1;
+    if (dst == rowoff[k] + dep[k]) last[k] = p;
+  }
+  for (int k = 0; k < nv; ++k)
+    if (last[k] >= 0) tasks[4 * last[k] + 3] = (uint32_t)k + 1;
   const int64_t toff = ((5 + (int64_t)levels) + 3) & ~(int64_t)3;
   const int64_t words = toff + (int64_t)tasks.size() + (int64_t)extras.size();
   if (out && capacity >= words) {

@@ -337,11 +337,11 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       for (int p = tl; p < ntask; p += T) {
         const uint4 t4 = tk[p];
         bad |= (int)(t4.x & 0xffff) >= lim || (int)(t4.y & 0xffff) >= lim || (int)(t4.y >> 16) >= lim ||
-               (int)(t4.z & 0xffff) >= nL0 || (int)(t4.z >> 16) + (int)(t4.x >> 16) > nextra;
+               (int)(t4.z & 0xffff) >= nv || (int)(t4.z >> 16) + (int)(t4.x >> 16) > nextra || (int)t4.w > nv;
       }
       for (int e = tl; e < nextra; e += T) {
         const uint2 e2 = ex[e];
-        bad |= (int)(e2.x & 0xffff) >= lim || (int)(e2.x >> 16) >= lim || (int)e2.y >= nL0;
+        bad |= (int)(e2.x & 0xffff) >= lim || (int)(e2.x >> 16) >= lim || (int)e2.y >= nv;
       }
     }
     bad = __any_sync(tm.mask, bad);
@@ -651,7 +651,12 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     float* Lm = work;
     float* z = work + nL;
     for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
-    for (int i = tl; i < nv; i += T) z[i] = -g[i];
+    // pivots of the leaves (final already); a non-leaf's is stored by the task that
+    // finalises its diagonal (the schedule's flag)
+    for (int i = tl; i < nv; i += T) {
+      z[i] = -g[i];
+      dinv[i] = __frcp_rn(jtj[rowoff[i] + ddep[i]] + damp);
+    }
     tm.sync();
     const int nlev = (int)sched[0];
     const int toff = (5 + nlev + 3) & ~3;
@@ -665,12 +670,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         const uint4 tk = nx;                                   // the next pass's task is in flight
         if (p + T < t1) nx = __ldg(tasks + p + T);
         const int dst = tk.x & 0xffff;
-        float acc = fmaf(-Lm[tk.y & 0xffff] * __frcp_rn(Lm[tk.z & 0xffff] + damp), Lm[tk.y >> 16], Lm[dst]);
+        float acc = fmaf(-Lm[tk.y & 0xffff] * dinv[tk.z & 0xffff], Lm[tk.y >> 16], Lm[dst]);
         for (int e = (int)(tk.z >> 16), e1 = e + (int)(tk.x >> 16); e < e1; ++e) {
           const uint2 ex = __ldg(extra + e);
-          acc = fmaf(-Lm[ex.x & 0xffff] * __frcp_rn(Lm[ex.y] + damp), Lm[ex.x >> 16], acc);
+          acc = fmaf(-Lm[ex.x & 0xffff] * dinv[ex.y], Lm[ex.x >> 16], acc);
         }
         Lm[dst] = acc;
+        if (tk.w) dinv[tk.w - 1] = __frcp_rn(acc + damp);    // DOF tk.w - 1's pivot is final
       }
       tm.sync();
     }

@@ -109,9 +109,11 @@ typedef struct br_tree {
  * Layout (uint32 words): [0] levels, [1] tasks, [2] extra contributions, [3] 1 + the
  * deepest DOF depth, [4 .. 4 + levels] first task of each level (the last = tasks),
  * then at word toff = roundup(5 + levels, 4) the tasks, 4 words each:
- *   {dst | (n_extra << 16), a | (b << 16), d | (first_extra << 16), 0}
- *   dst -= m[a] * m[b] / (m[d] + damp), then the same for each extra contribution,
- * then at toff + 4 * tasks the extra contributions, 2 words each: {a | (b << 16), d}.
+ *   {dst | (n_extra << 16), a | (b << 16), k | (first_extra << 16), f}
+ *   dst -= m[a] * m[b] / (pivot_k + damp), then the same for each extra contribution;
+ *   f = c + 1 when the task is the last update of DOF c's diagonal (its pivot is then
+ *   final), else 0,
+ * then at toff + 4 * tasks the extra contributions, 2 words each: {a | (b << 16), k}.
  * Offsets index the packed rows (row c starts at sum_{c' < c} (depth(c') + 1), its
  * diagonal at depth(c)) followed by the nv right-hand-side slots.
  *

@@ -73,13 +73,18 @@ def _solve(s, dof_parent, A, g, damp):
         m[rowoff[c] + dep[c]] = A[c, c]
     m[nL:] = -g
     nlev, ndl, starts, tasks, extra = _decode(s)
+    # leaves' pivots are final from the start; a non-leaf's is stored by the flagged task
+    dinv = np.array([1.0 / (m[rowoff[i] + dep[i]] + damp) for i in range(nv)])
     for lev in range(nlev):
         for tk in tasks[starts[lev]:starts[lev + 1]]:
             acc = m[tk[0] & 0xffff]
-            for a, b, d in _contribs(tk, extra):
-                acc -= m[a] / (m[d] + damp) * m[b]
+            for a, b, k in _contribs(tk, extra):
+                acc -= m[a] * dinv[k] * m[b]
             m[tk[0] & 0xffff] = acc
+            if tk[3]:
+                dinv[tk[3] - 1] = 1.0 / (acc + damp)
     piv = np.array([m[rowoff[i] + dep[i]] + damp for i in range(nv)])
+    assert np.allclose(dinv, 1.0 / piv, rtol=0, atol=0)
     assert (piv > 0).all()
     x = np.zeros(nv)
     for dl in range(ndl):
@@ -142,14 +147,27 @@ def test_schedule_levels_are_race_free(name):
         row_of[nL + c] = c
     nlev, ndl, starts, tasks, extra = _decode(_schedule(dp))
     assert ndl == max(dep) + 1
+    parents = set(int(p) for p in dp if p >= 0)
+    final_later = set(parents)        # non-leaf DOFs whose pivot is not final yet
+    assert int((tasks[:, 3] != 0).sum()) == len(parents)
     seen = 0
     for lev in range(nlev):
         lt = tasks[starts[lev]:starts[lev + 1]]
         dsts = [int(t[0] & 0xffff) for t in lt]
         assert len(dsts) == len(set(dsts))
         written = {int(row_of[d]) for d in dsts}
-        read = {int(row_of[x]) for t in lt for a, b, d in _contribs(t, extra) for x in (a, b, d)}
+        read = {int(row_of[x]) for t in lt for a, b, k in _contribs(t, extra) for x in (a, b)}
+        read |= {int(k) for t in lt for a, b, k in _contribs(t, extra)}   # pivots read
         assert not (written & read)
+        # a pivot is read only after the level that finalised it
+        for t in lt:
+            for a, b, k in _contribs(t, extra):
+                assert k not in final_later, (k, lev)
+        for t in lt:
+            if t[3]:
+                c = int(t[3]) - 1
+                assert int(t[0] & 0xffff) == rowoff[c] + dep[c]
+                final_later.discard(c)
         seen += sum(1 + int(t[0] >> 16) for t in lt)
     # one contribution per (DOF, ancestor pair) plus one per (DOF, ancestor) for the right-hand side
     assert seen == sum(d * (d + 1) // 2 + d for d in dep)
