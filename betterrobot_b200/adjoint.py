@@ -19,7 +19,7 @@ from typing import Sequence
 import torch
 
 from . import _lib
-from .exceptions import UnsupportedJointError, ShapeError
+from .exceptions import ShapeError
 from .kinematics import _validate_q
 from .tree import device_tree
 
@@ -69,14 +69,10 @@ def pose_loss(model, q: torch.Tensor, frame_ids: Sequence[int], targets: torch.T
               mode: str = "auto", check_quaternion: bool = False) -> torch.Tensor:
     """Per-configuration pose loss ``(B,)``; differentiable w.r.t. ``q`` (B, nq) float32 CUDA.
 
-    The backward kernel maps gradients to raw q for fixed, revolute (bounded), prismatic and
-    free-flyer joints; other kinds raise ``UnsupportedJointError``.
+    The backward kernel maps gradients to raw q for every joint kind of the tree table
+    (fixed, revolute, unbounded revolute, prismatic, free-flyer, spherical, planar,
+    translation).
     """
-    bad = [jm.kind for jm in model.joint_models
-           if not (jm.kind in ("universe", "fixed", "free_flyer") or jm.kind.startswith("prismatic")
-                   or (jm.kind.startswith("revolute") and jm.kind != "revolute_unbounded"))]
-    if bad:
-        raise UnsupportedJointError(f"pose_loss: no raw-q adjoint for joint kinds {sorted(set(bad))}")
     _validate_q(model, q, check_quaternion)
     if q.dim() != 2:
         raise ShapeError("pose_loss takes q of shape (B, nq)")

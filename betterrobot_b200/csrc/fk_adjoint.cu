@@ -12,9 +12,11 @@
 //   * dL/dv_c = sum_{f : c supports f} <S_c, F_f> with S_c the world twist of tangent
 //     column c ([o x a; a] rotation, [a; 0] translation) — a reverse accumulation over
 //     the tree without any per-joint tape;
-//   * revolute / prismatic: dL/dq = dL/dv; free-flyer: the body twist of its joint
-//     maps to raw q = [t, quat] through R (translation) and the normalisation of the
-//     quaternion ((I - u u^T)/|quat| and du -> 2 vec(u* (x) du)).
+//   * revolute / prismatic / translation: dL/dq = dL/dv; free-flyer and spherical: the
+//     body twist of the joint maps to raw q = [t, quat] through R (translation) and the
+//     normalisation of the quaternion ((I - u u^T)/|quat| and du -> 2 vec(u* (x) du));
+//     unbounded revolute: th = atan2(s, c); planar: [x, y] through R, the angle through
+//     the reference's half-angle formula (dth/dc = -1/sin th, no dependence on s).
 // World joint placements are either recomputed from q (no saved state) or read
 // from the forward pass (store mode, [B, njoints, 7]).
 #include <cuda_runtime.h>
@@ -221,14 +223,39 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
       const int iq = s_idxq[j];
       if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
         gq[iq] = wg[tree.idx_v[j]];
-      } else if (jt == BR_JOINT_FREE_FLYER) {
+      } else if (jt == BR_JOINT_TRANSLATION) {                     // q is the body translation
         const int iv = tree.idx_v[j];
-        const float4 qr = make_float4(wq[iq + 3], wq[iq + 4], wq[iq + 5], wq[iq + 6]);
+        gq[iq] = wg[iv]; gq[iq + 1] = wg[iv + 1]; gq[iq + 2] = wg[iv + 2];
+      } else if (jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
+        // th = atan2(s, c) (revolute.py:206-211): dth/dc = -s / r^2, dth/ds = c / r^2
+        const float g = wg[tree.idx_v[j]];
+        const float c = wq[iq], sn = wq[iq + 1];
+        const float r2 = fmaxf(c * c + sn * sn, 1e-30f);
+        gq[iq] = -g * sn / r2;
+        gq[iq + 1] = g * c / r2;
+      } else if (jt == BR_JOINT_PLANAR) {
+        // T = ([x, y, 0], Rz(th)) with cos(th/2) = sqrt((1+c)/2), sin(th/2) = sqrt((1-c)/2) sign(s)
+        // (planar.py:20-41): body twist = (R^T [dx, dy, 0], e_z dth), dth/dc = -1 / sin(th),
+        // and th does not depend on s away from s = 0
+        const int iv = tree.idx_v[j];
+        const float c = wq[iq + 2], sn = wq[iq + 3];
+        const float4 hq = planar_quat(c, sn);
+        const float ct = hq.w * hq.w - hq.z * hq.z, st = 2.f * hq.z * hq.w;
+        const float g0 = wg[iv], g1 = wg[iv + 1], g2 = wg[iv + 2];
+        gq[iq] = ct * g0 - st * g1;
+        gq[iq + 1] = st * g0 + ct * g1;
+        gq[iq + 2] = -g2 / st;
+        gq[iq + 3] = 0.f;
+      } else if (jt == BR_JOINT_FREE_FLYER || jt == BR_JOINT_SPHERICAL) {
+        // free-flyer [t, quat] / spherical [quat]: the quaternion's body rotation
+        const bool ff = jt == BR_JOINT_FREE_FLYER;
+        const int iv = tree.idx_v[j];
+        const int qo = ff ? iq + 3 : iq;                          // first quaternion slot
+        const int vo = ff ? iv + 3 : iv;                          // first rotation column
+        const float4 qr = make_float4(wq[qo], wq[qo + 1], wq[qo + 2], wq[qo + 3]);
         const float4 u = qnormalize(qr);
         const float n = fmaxf(sqrtf(qr.x * qr.x + qr.y * qr.y + qr.z * qr.z + qr.w * qr.w), 1e-8f);
-        const float3 gl = f3(wg[iv], wg[iv + 1], wg[iv + 2]);
-        const float3 ga = f3(wg[iv + 3], wg[iv + 4], wg[iv + 5]);
-        const float3 gt = qrot(u, gl);  // translation: delta_lin = R^T dt
+        const float3 ga = f3(wg[vo], wg[vo + 1], wg[vo + 2]);
         // quaternion: delta_ang = 2 vec(u* (x) du), du = (I - u u^T) dquat / n
         float4 h;
         h.x = u.w * ga.x - u.z * ga.y + u.y * ga.z;
@@ -237,11 +264,14 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
         h.w = -u.x * ga.x - u.y * ga.y - u.z * ga.z;
         const float uh = u.x * h.x + u.y * h.y + u.z * h.z + u.w * h.w;
         const float s = 2.f / n;
-        gq[iq] = gt.x; gq[iq + 1] = gt.y; gq[iq + 2] = gt.z;
-        gq[iq + 3] = s * (h.x - u.x * uh);
-        gq[iq + 4] = s * (h.y - u.y * uh);
-        gq[iq + 5] = s * (h.z - u.z * uh);
-        gq[iq + 6] = s * (h.w - u.w * uh);
+        if (ff) {
+          const float3 gt = qrot(u, f3(wg[iv], wg[iv + 1], wg[iv + 2]));  // translation: delta_lin = R^T dt
+          gq[iq] = gt.x; gq[iq + 1] = gt.y; gq[iq + 2] = gt.z;
+        }
+        gq[qo] = s * (h.x - u.x * uh);
+        gq[qo + 1] = s * (h.y - u.y * uh);
+        gq[qo + 2] = s * (h.z - u.z * uh);
+        gq[qo + 3] = s * (h.w - u.w * uh);
       }
     }
     __syncwarp();
@@ -291,9 +321,9 @@ static int fill_loss(const br_tree_t* tree, LossParams& p, const int32_t* frame_
 
 using namespace br;
 
-// Joint kinds whose raw-q chain rule the backward implements (revolute, prismatic, free-flyer).
+// Joint kinds whose raw-q chain rule the backward implements: every kind of the tree table.
 static bool adjoint_kinds_ok(const br_tree_t* t) {
-  const int ok = (1 << BR_JOINT_FIXED) | (1 << BR_JOINT_REVOLUTE) | (1 << BR_JOINT_PRISMATIC) | (1 << BR_JOINT_FREE_FLYER);
+  const int ok = (1 << (BR_JOINT_TRANSLATION + 1)) - 1;
   return t && t->kinds != 0 && (t->kinds & ~ok) == 0;
 }
 

@@ -21,6 +21,8 @@ and outputs in ``tests/golden/*.npz``:
                       (``tasks/ik.py:191-226``) but with the configs' damping.
 * ``adjoint.npz``   — pose loss ``sum_f w_f |log(T_f^-1 oMf(q))|^2`` and its autograd
                       gradient w.r.t. raw ``q`` (free-flyer quaternion included).
+* ``adjoint_mixed.npz`` — the same on the robot with every multi-slot joint kind
+                      (planar, translation, spherical, unbounded revolute).
 """
 
 from __future__ import annotations
@@ -346,6 +348,10 @@ def main():
     if src:
         sys.path.insert(0, src)
     torch.set_default_dtype(D)
+    only = sys.argv[2:]
+    if only == ["adjoint_mixed"]:   # regenerate one fixture: make_golden.py <src> adjoint_mixed
+        make_adjoint(syn.mixed_spec(), 8, 33, os.path.join(HERE, "adjoint_mixed.npz"))
+        return
     make_lie(os.path.join(HERE, "lie.npz"))
     make_lie_ops(os.path.join(HERE, "lie_ops.npz"))
     chain, hum, dual = syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()
@@ -367,6 +373,7 @@ def main():
     make_ik("mixed", syn.mixed_spec(), ["ee", "mid"], 6, 32, "noisy", os.path.join(HERE, "ik_mixed.npz"),
             max_iter=100, rest_w=1e-3, **lm)
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
+    make_adjoint(syn.mixed_spec(), 8, 33, os.path.join(HERE, "adjoint_mixed.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
 
 

@@ -55,18 +55,23 @@ def _grad(m, q, fids, targets, w, mode):
 
 
 @pytest.mark.parametrize("mode", ["store", "recompute"])
-def test_matches_reference_autograd_golden(mode):
-    g = np.load(os.path.join(GOLDEN, "adjoint.npz"))
-    m = syn.model_from_spec(syn.humanoid_spec())
+@pytest.mark.parametrize("fixture,spec", [("adjoint.npz", syn.humanoid_spec()),
+                                          ("adjoint_mixed.npz", syn.mixed_spec())])
+def test_matches_reference_autograd_golden(mode, fixture, spec):
+    """Free-flyer humanoid, and the robot with planar, translation, spherical and unbounded
+    revolute joints, against the reference's float64 autograd gradient w.r.t. raw q."""
+    g = np.load(os.path.join(GOLDEN, fixture))
+    m = syn.model_from_spec(spec)
     fids = [int(f) for f in g["frame_ids"]]
     loss, grad = _grad(m, g["q"], fids, g["targets"], g["weights"], mode)
     np.testing.assert_allclose(loss, g["loss"], rtol=1e-5)
     assert _rel(grad, g["grad"]).max() <= GRAD_TOL, _rel(grad, g["grad"])
 
 
-@pytest.mark.parametrize("robot", ["humanoid", "chain7", "dual_arm"])
+@pytest.mark.parametrize("robot", ["humanoid", "chain7", "dual_arm", "mixed"])
 def test_matches_float64_central_differences(robot):
-    spec = {"humanoid": syn.humanoid_spec(), "chain7": syn.chain_spec(), "dual_arm": syn.dual_arm_spec()}[robot]
+    spec = {"humanoid": syn.humanoid_spec(), "chain7": syn.chain_spec(), "dual_arm": syn.dual_arm_spec(),
+            "mixed": syn.mixed_spec()}[robot]
     m, m64 = syn.model_from_spec(spec), syn.model_from_spec(spec, dtype=torch.float64)
     fids = syn.op_frame_ids(m) + [m.nframes - 1]
     B = 16
@@ -82,6 +87,15 @@ def test_matches_float64_central_differences(robot):
     np.testing.assert_allclose(loss, ref_loss, rtol=1e-5)
     fd = _fd(m64, q32, fids, t32, w32)
     rel = _rel(grad, fd)
+    if robot == "mixed":
+        # the planar angle is acos(cos) (the reference's half-angle formula): near 0 or pi its
+        # third derivative grows like 1/sin^5, and the central difference's truncation error
+        # with eps 1e-6 reaches percents (one of these 16 configurations has sin = 0.0024);
+        # the exact derivative there is checked against the reference's autograd instead
+        i_c = int(m.idx_qs[[jm.kind for jm in m.joint_models].index("planar")]) + 2
+        keep = np.sqrt(np.maximum(1.0 - q32[:, i_c] ** 2, 0.0)) >= 0.05
+        assert keep.sum() >= 12
+        rel = rel[keep]
     assert rel.max() <= GRAD_TOL, rel
 
 
@@ -117,13 +131,10 @@ def test_grad_output_scaling():
     torch.testing.assert_close(g, g1 * go[:, None], rtol=1e-6, atol=1e-6)
 
 
-def test_unsupported_joint_kinds_raise():
-    """The backward's raw-q chain rule covers revolute, prismatic and free-flyer joints only."""
+def test_trajopt_rejects_multi_slot_kinds():
+    """Trajectory optimisation needs q + v joints (knot difference q1 - q0)."""
     from betterrobot_b200.exceptions import UnsupportedJointError
     from betterrobot_b200 import trajopt as btr
     m = syn.model_from_spec(syn.mixed_spec())
-    q = torch.zeros(2, m.nq, device="cuda")
-    with pytest.raises(UnsupportedJointError):
-        pose_loss(m, q, [0], torch.zeros(2, 1, 7, device="cuda"), torch.ones(1, device="cuda"))
     with pytest.raises(UnsupportedJointError):
         btr.solve_trajopt_batched(m, 0, torch.zeros(1, 7, device="cuda"), torch.zeros(1, 4, m.nq, device="cuda"))

@@ -93,6 +93,30 @@ def test_pose_loss_matches_reference():
     np.testing.assert_allclose(loss, g["loss"], atol=1e-12, rtol=1e-12)
 
 
+def test_pose_loss_and_gradient_mixed_kinds_match_reference():
+    """Loss and (float64 central-difference) gradient on the robot with every multi-slot
+    joint kind against the reference's loss and autograd gradient."""
+    g = _load("adjoint_mixed.npz")
+    m = syn.model_from_spec(syn.mixed_spec(), dtype=torch.float64)
+    fids = [int(f) for f in g["frame_ids"]]
+
+    def loss_of(q):
+        oMi, _ = K.forward_kinematics(m, q)
+        oMf = K.frame_placements(m, oMi, fids)
+        xi = lie.se3_log(lie.se3_compose(lie.se3_inverse(g["targets"]), oMf))
+        return ((xi * xi).sum(-1) * g["weights"]).sum(-1)
+
+    np.testing.assert_allclose(loss_of(g["q"]), g["loss"], atol=1e-12, rtol=1e-12)
+    eps = 1e-6
+    fd = np.zeros_like(g["q"])
+    for i in range(g["q"].shape[1]):
+        qp, qm = g["q"].copy(), g["q"].copy()
+        qp[:, i] += eps
+        qm[:, i] -= eps
+        fd[:, i] = (loss_of(qp) - loss_of(qm)) / (2 * eps)
+    np.testing.assert_allclose(fd, g["grad"], atol=1e-6 * np.abs(g["grad"]).max(), rtol=0)
+
+
 def test_known_answers_one_joint_arm():
     """Reference known answers on a 1-joint arm (``tests/kinematics/test_fk.py:85-103``)."""
     import math
