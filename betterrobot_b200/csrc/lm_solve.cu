@@ -671,7 +671,16 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         if (p + T < t1) nx = __ldg(tasks + p + T);
         const int dst = tk.x & 0xffff;
         float acc = fmaf(-Lm[tk.y & 0xffff] * dinv[tk.z & 0xffff], Lm[tk.y >> 16], Lm[dst]);
-        for (int e = (int)(tk.z >> 16), e1 = e + (int)(tk.x >> 16); e < e1; ++e) {
+        int e = (int)(tk.z >> 16);
+        const int e1 = e + (int)(tk.x >> 16);
+        for (; e + 1 < e1; e += 2) {                           // two records in flight at once
+          const uint2 ea = __ldg(extra + e), eb = __ldg(extra + e + 1);
+          const float a1 = Lm[ea.x & 0xffff] * dinv[ea.y], a2 = Lm[ea.x >> 16];
+          const float b1 = Lm[eb.x & 0xffff] * dinv[eb.y], b2 = Lm[eb.x >> 16];
+          acc = fmaf(-a1, a2, acc);
+          acc = fmaf(-b1, b2, acc);
+        }
+        if (e < e1) {
           const uint2 ex = __ldg(extra + e);
           acc = fmaf(-Lm[ex.x & 0xffff] * dinv[ex.y], Lm[ex.x >> 16], acc);
         }
