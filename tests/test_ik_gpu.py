@@ -136,6 +136,46 @@ def test_noisy_start_vs_oracle(robot, frames, rest, P, agree_min):
     assert abs(conv.mean() - ref.converged.mean()) <= 0.08, (conv.mean(), ref.converged.mean())
 
 
+def test_inconsistent_tree_tables_are_refused():
+    """A class whose tree under-reports its DOF entries, or whose level schedule holds an offset
+    outside the factor storage, is refused problem by problem (status flag BADTREE, x = x0)
+    by the kernel's own checks before any of it is used; the same batch then solves normally."""
+    from betterrobot_b200.tree import TreeArrays
+    m, m64 = _models("humanoid")
+    fids = [m.frame_id(f) for f in ("track0", "track2")]
+    P = 64
+    q_star = syn.random_q(m64, P, 60, rev_range=2.5, base_translation=0.5)
+    oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+    targets = torch.from_numpy(K.frame_placements(m64, oMi, fids)).float().cuda()
+    q0 = syn.noisy_start(m64, q_star, 0.3, 61).float().cuda()
+    frames = np.tile(np.array(fids, np.int32), (P, 1))
+    pk = bik.PackedIK([m], [frames], [np.full(P, len(fids), np.int32)], team_sizes=[32], warps_per_cta=4)
+    pk.set_inputs([targets], [q0])
+    settings = bik.settings_from(bik.IKCostConfig(rest_weight=1e-3), bik.OptimizerConfig(max_iter=100))
+    badtree = 4  # BR_IK_FLAG_BADTREE
+    good_sched, good_ent = pk._trees[0].dof_sched, pk._trees[0].dof_entries
+
+    sched = TreeArrays(m).dof_schedule().copy()
+    toff = (5 + int(sched[0]) + 3) & ~3
+    sched[toff] = (sched[toff] & np.uint32(0xffff0000)) | np.uint32(0xffff)   # first task's destination
+    bad = torch.from_numpy(sched.view(np.int32)).cuda()
+    for field, value in (("dof_sched", bad.data_ptr()), ("dof_entries", 10)):
+        setattr(pk._trees[0], field, value)
+        pk.solve(settings)
+        st = pk.status.cpu().numpy()
+        assert (((st >> 8) & badtree) != 0).all(), (field, st[:4])
+        torch.testing.assert_close(pk.q_of(0), q0, rtol=0, atol=0)
+        pk._trees[0].dof_sched, pk._trees[0].dof_entries = good_sched, good_ent
+    pk.solve(settings)
+    st = pk.status.cpu().numpy()
+    assert (((st >> 8) & badtree) == 0).all()
+    fresh = bik.PackedIK([m], [frames], [np.full(P, len(fids), np.int32)], team_sizes=[32], warps_per_cta=4)
+    fresh.set_inputs([targets], [q0])
+    fresh.solve(settings)
+    np.testing.assert_array_equal(st, fresh.status.cpu().numpy())
+    torch.testing.assert_close(pk.q_of(0), fresh.q_of(0), rtol=0, atol=0)
+
+
 def test_uneven_mix_single_launch_matches_per_class():
     """Three robots, 1-6 targets, one launch == the same problems solved class by class."""
     models = [_models(n) for n in ("humanoid", "dual_arm", "chain7")]
