@@ -104,6 +104,48 @@ __device__ __forceinline__ float vinv_coeff(float th2) {
   return 1.f / th2 - (ch / sh) / (2.f * th);
 }
 
+// Jr^-1(xi)^T xi for xi = (v, w): the gradient of 1/2 |log(T0^-1 T)|^2 with respect to a
+// right perturbation of T, in closed form.  With Jr(xi) = [[A, B], [0, A]] (A = Jr_so3(w)),
+// A^-T = Jl_so3(w)^-1 = V(w)^-1 and A^-T w = w, B^T = Q_l(v, w) (the left-Jacobian block of
+// Barfoot, "State Estimation for Robotics", eq. 7.86b), so
+//   g_lin = V^-1 v,   g_ang = w - V^-1 Q_l(v, w) g_lin
+// with Q_l u = 1/2 v x u + c2 (w^v^ + v^w^ + w^v^w^) u + c3 (w^w^v^ + v^w^w^ - 3 w^v^w^) u
+//             + c4 (w^v^w^w^ + w^w^v^w^) u,
+// c2 = (th - sin th)/th^3, c3 = (th^2 + 2 cos th - 2)/(2 th^4), c4 = (2 th - 3 sin th + th cos th)/(2 th^5)
+// (Taylor series of each for th^2 < 2, where the closed forms cancel).  Equal to applying the
+// exact (infinite-series) Jr^-1 of jr_inv_se3 below, at a fraction of its arithmetic.
+__device__ __forceinline__ void jr_inv_T_xi(float3 v, float3 w, float3& gl, float3& ga) {
+  const float th2 = dot(w, w);
+  float c2, c3, c4;
+  if (th2 < 2.f) {
+    c2 = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 39916800.f, -1.f / 362880.f), 1.f / 5040.f), -1.f / 120.f),
+              1.f / 6.f);
+    c3 = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 479001600.f, -1.f / 3628800.f), 1.f / 40320.f),
+                   -1.f / 720.f), 1.f / 24.f);
+    c4 = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 1245404160.f, -1.f / 9979200.f), 1.f / 120960.f),
+                   -1.f / 2520.f), 1.f / 120.f);
+  } else {
+    const float th = sqrtf(th2);
+    float s, co;
+    sincospif(th * (1.f / 3.14159265358979f), &s, &co);
+    c2 = (th - s) / (th * th2);
+    c3 = (th2 + 2.f * co - 2.f) / (2.f * th2 * th2);
+    c4 = (2.f * th - 3.f * s + th * co) / (2.f * th2 * th2 * th);
+  }
+  const float c = vinv_coeff(th2);
+  auto vinv = [&](float3 x) { return axpy(c, cross(w, cross(w, x)), axpy(-0.5f, cross(w, x), x)); };
+  gl = vinv(v);
+  const float3 a1 = cross(w, gl), a2 = cross(w, a1);
+  const float3 b0 = cross(v, gl), b1 = cross(v, a1), b2 = cross(v, a2);
+  const float3 wb0 = cross(w, b0), wwb0 = cross(w, wb0), wb1 = cross(w, b1), wwb1 = cross(w, wb1);
+  const float3 wb2 = cross(w, b2);
+  float3 q = scale(b0, 0.5f);
+  q = axpy(c2, add(add(wb0, b1), wb1), q);
+  q = axpy(c3, add(add(wwb0, b2), scale(wb1, -3.f)), q);
+  q = axpy(c4, add(wb2, wwb1), q);
+  ga = sub(w, vinv(q));
+}
+
 // SE3 log -> (v, w)   (se3_log, _torch_native_backend.py:289-310)
 __device__ __forceinline__ void se3_log(const Pose& T, float3& v, float3& w) {
   w = so3_log(T.q);

@@ -6,7 +6,7 @@
 //
 // Adjoint, one warp per configuration:
 //   * g_f = 2 w_f Jr^-1(xi_f)^T xi_f is dL/d(body twist of frame f), with the exact
-//     SE3 Jr^-1 (series to 20 terms; autograd differentiates se3_log exactly);
+//     SE3 Jr^-1 (closed form jr_inv_T_xi; autograd differentiates se3_log exactly);
 //   * F_f = Ad(oMf^-1)^T g_f = [R g_lin; p x (R g_lin) + R g_ang] is the same
 //     sensitivity as a wrench at the world origin;
 //   * dL/dv_c = sum_{f : c supports f} <S_c, F_f> with S_c the world twist of tangent
@@ -183,9 +183,8 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
       const float wf = __ldg(p.weights + (p.weights_per_config ? b * nf + f : f));
       acc += wf * (dot(v, v) + dot(om, om));
       if (kBackward) {
-        const JrInv J = jr_inv_se3<20>(v, om);
         float3 gl, ga;
-        jr_inv_T_apply(J, v, om, gl, ga);
+        jr_inv_T_xi(v, om, gl, ga);
         const float s2 = 2.f * wf;
         const float3 fw = qrot(Tf.q, scale(gl, s2));
         const float3 tau = add(cross(Tf.t, fw), qrot(Tf.q, scale(ga, s2)));
