@@ -98,6 +98,25 @@ __device__ __forceinline__ void std8d(double* p, const DPose& P) {
   p[4] = P.q.x; p[5] = P.q.y; p[6] = P.q.z; p[7] = P.q.w;
 }
 
+// 1 / d for d > 0 (a pivot): the hardware reciprocal estimate refined by two Newton steps
+// r <- r + r (1 - d r), each of which squares the relative error (~2^-23 -> 2^-46 -> below
+// double rounding); within an ulp or two of 1.0 / d at a fraction of the division's latency.
+__device__ __forceinline__ double fast_rcp(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+// 1 / sqrt(x) for x > 0: estimate + two Newton steps y <- y (3 - x y^2) / 2
+__device__ __forceinline__ double fast_rsqrt(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = y * fma(-0.5 * x * y, y, 1.5);
+  return y * fma(-0.5 * x * y, y, 1.5);
+}
+
 __global__ void traj_gn_kernel(const TrajParams P) {
   extern __shared__ __align__(16) double sm[];
   const br_tree_t& tree = P.tree;
@@ -350,7 +369,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         const double l1 = (p >= 1) ? (hoff1(t - 1) - c2 * l1p) * di1 : 0.0;
         const double dp = hdiag(t, i, damp) - l1 * l1 * d1 - l2 * c2;
         if (!(dp > 0.0)) { good = false; break; }
-        const double dip = 1.0 / dp;
+        const double dip = fast_rcp(dp);
         bl1[p * nv + i] = l1; bl2[p * nv + i] = l2; bdi[p * nv + i] = dip;
         di2 = di1; di1 = dip; d1 = dp; l1p = l1;
       }
@@ -421,8 +440,8 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     for (int k = 0; k < nb; ++k) {                                  // chol(S), lower, in place
       const double dkk = Sb[k * nb + k];
       if (!(dkk > 0.0)) return false;
-      const double sk = sqrt(dkk);
-      const double inv = 1.0 / sk;
+      const double inv = fast_rsqrt(dkk);
+      const double sk = dkk * inv;
       __syncwarp();
       if (lane > k && lane < nb) Sb[lane * nb + k] *= inv;
       if (lane == k) { Sb[k * nb + k] = sk; sdi[k] = inv; }
