@@ -358,16 +358,23 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   auto newton_solve = [&](double damp) -> bool {
     const int m = T - 2, nb = 2 * nv;
     bool good = true;
+    // interior diagonals H[(p+1, i), (p+1, i)] by all lanes first (vy is free until the
+    // forward solve); the off-diagonal H[(p+1), (p)] of the interior is -4 c2
+    for (int e = lane; e < m * nv; e += kWarp) {
+      const int pp = e / nv;
+      vy[e] = hdiag(pp + 1, e - pp * nv, damp);
+    }
+    __syncwarp();
+    const double h1 = -4.0 * c2;
     if (lane < nv) {
       const int i = lane;
       // banded LDL^T of the interior of DOF i: L[p][p-2] = c2 / D[p-2],
       // L[p][p-1] = (H[p][p-1] - c2 L[p-1][p-2]) / D[p-1], D[p] = H[p][p] - L[p][p-1]^2 D[p-1] - L[p][p-2] c2
       double d1 = 0.0, di1 = 0.0, di2 = 0.0, l1p = 0.0;
       for (int p = 0; p < m; ++p) {
-        const int t = p + 1;
         const double l2 = (p >= 2) ? c2 * di2 : 0.0;
-        const double l1 = (p >= 1) ? (hoff1(t - 1) - c2 * l1p) * di1 : 0.0;
-        const double dp = hdiag(t, i, damp) - l1 * l1 * d1 - l2 * c2;
+        const double l1 = (p >= 1) ? (h1 - c2 * l1p) * di1 : 0.0;
+        const double dp = vy[p * nv + i] - l1 * l1 * d1 - l2 * c2;
         if (!(dp > 0.0)) { good = false; break; }
         const double dip = fast_rcp(dp);
         bl1[p * nv + i] = l1; bl2[p * nv + i] = l2; bdi[p * nv + i] = dip;
@@ -446,9 +453,9 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       if (lane > k && lane < nb) Sb[lane * nb + k] *= inv;
       if (lane == k) { Sb[k * nb + k] = sk; sdi[k] = inv; }
       __syncwarp();
-      for (int e = lane; e < nb * nb; e += kWarp) {
-        const int r = e / nb, cc = e - r * nb;
-        if (cc > k && r >= cc) Sb[e] -= Sb[r * nb + k] * Sb[cc * nb + k];
+      if (lane > k && lane < nb) {                                 // lane r updates row r
+        const double lrk = Sb[lane * nb + k];
+        for (int cc = k + 1; cc <= lane; ++cc) Sb[lane * nb + cc] -= lrk * Sb[cc * nb + k];
       }
       __syncwarp();
     }
