@@ -68,8 +68,9 @@ typedef struct br_tree {
     int32_t njoints, nq, nv, nframes;
     int32_t rounds;           /* ceil(log2(max joint depth)): pointer-jumping rounds */
     int32_t kinds;            /* bit k set if some joint has kind BR_JOINT_k; entry points
-                                 that support only some kinds (the FK adjoint, trajectory
-                                 optimisation) reject a tree whose mask names others or is 0 */
+                                 that support only some kinds (trajectory optimisation) reject
+                                 a tree whose mask names others; the FK adjoint and trajectory
+                                 optimisation reject a mask of 0                              */
     int32_t dof_entries;      /* sum over tangent columns of (depth in the DOF tree + 1): the
                                  LM's J^T J storage; 0 = not given (dense nv (nv + 1) / 2) */
     int32_t dof_depth;        /* 1 + deepest DOF-tree depth; 0 = not given (nv)            */
@@ -268,8 +269,9 @@ BR_API int br_pose_loss(const br_tree_t* tree, const float* q, int64_t batch, co
                         float* loss, float* joint_pose_world, void* stream);
 
 /*
- * Adjoint of br_pose_loss: grad_q[b, :] = grad_loss[b] * dloss[b]/dq (raw q,
- * free-flyer quaternion components included).  joint_pose_world from the
+ * Adjoint of br_pose_loss: grad_q[b, :] = grad_loss[b] * dloss[b]/dq (raw q of every
+ * joint kind: free-flyer and spherical quaternion components, planar [x, y, cos, sin],
+ * unbounded revolute [cos, sin] included).  joint_pose_world from the
  * forward pass, or NULL to recompute FK from q ("recompute" mode).  Replaces
  * torch autograd's backward through the reference FK tape
  * (forward.py:79-81 builds that tape on purpose).
