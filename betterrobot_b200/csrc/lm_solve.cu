@@ -31,7 +31,9 @@
 // test are decided as the float64 reference decides them; near the optimum the
 // cost decrease of an accepted step (~1e-12) is far below float32 resolution of
 // the cost.  Everything that scales with nv^2 or nv^3 — Jacobian columns, J^T J,
-// J^T r, the Cholesky factorization and the solves — is float32.
+// J^T r, the Cholesky factorization and the solves — is float32, and so is the
+// exponential of a free-flyer step in the plain variant (composed with the float64
+// iterate in float64; its rounding is relative to the step).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
