@@ -108,8 +108,14 @@ def gpu_reach(wl, q_list):
         T = torch.gather(d.frame_pose_world, 1, idx[..., None].expand(-1, -1, 7)).double()
         tg = c["targets"].double()
         pe = (T[..., :3] - tg[..., :3]).norm(dim=-1)
-        dq = torch.abs((T[..., 3:] * tg[..., 3:]).sum(-1)).clamp(max=1.0)
-        re = 2.0 * torch.acos(dq)
+        # rotation error = |so3_log(q_t^-1 q)| = 2 atan2(|vec(r)|, |w(r)|), r = conj(q_t) (x) q,
+        # as the oracle measures it; 2 acos(|<q_t, q>|) would be ill-conditioned near 0 (float32
+        # rounding of the quaternions alone reads as ~4e-4 rad there)
+        av, aw = tg[..., 3:6], tg[..., 6:7]
+        bv, bw = T[..., 3:6], T[..., 6:7]
+        rv = aw * bv - bw * av - torch.linalg.cross(av, bv, dim=-1)
+        rw = (aw * bw + (av * bv).sum(-1, keepdim=True)).squeeze(-1)
+        re = 2.0 * torch.atan2(rv.norm(dim=-1), rw.abs())
         k = torch.arange(6, device=q.device)[None, :] < torch.from_numpy(c["n_targets"]).cuda()[:, None]
         ok = ((pe <= REACH_TOL) & (re <= REACH_TOL)) | ~k
         total += int(ok.all(dim=1).sum())
