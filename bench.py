@@ -99,9 +99,14 @@ def gpu_targets(wl):
 
 def gpu_reach(wl, q_list):
     """Problems whose every target is reached within REACH_TOL (m and rad), via the library FK."""
+    return int(sum(int(f.sum()) for f in gpu_reach_flags(wl, q_list)))
+
+
+def gpu_reach_flags(wl, q_list):
+    """Per class, a bool array: the problem's every target is reached within REACH_TOL."""
     import torch
     import betterrobot_b200 as br
-    total = 0
+    flags = []
     for c, q in zip(wl, q_list):
         d = br.forward_kinematics(c["model"], q, compute_frames=True, check_quaternion=False)
         idx = torch.from_numpy(c["frames"]).long().cuda()
@@ -118,8 +123,8 @@ def gpu_reach(wl, q_list):
         re = 2.0 * torch.atan2(rv.norm(dim=-1), rw.abs())
         k = torch.arange(6, device=q.device)[None, :] < torch.from_numpy(c["n_targets"]).cuda()[:, None]
         ok = ((pe <= REACH_TOL) & (re <= REACH_TOL)) | ~k
-        total += int(ok.all(dim=1).sum())
-    return total
+        flags.append(ok.all(dim=1).cpu().numpy())
+    return flags
 
 
 # ---------------------------------------------------------------------------
