@@ -79,12 +79,12 @@ struct TrajLayout {
     vy = take(T * nv); vu = take(T * nv); vw = take(T * nv);
     Sb = take(4 * nv * nv); sdi = take(2 * nv); rb = take(2 * nv);   // boundary Schur complement
     Jg = take(6 * nv); Js = take(6 * nv); rg = take(8); rs = take(8); jtjg = take(nv * nv); jtjs = take(nv * nv);
-    pA = take(8 * nj); pB = take(8 * nj);
+    pA = take(16 * nj); pB = take(16 * nj);   // FK buffers of the two pose terms (goal, start)
     total_doubles = o;
     // 4-byte arrays: count in doubles (2 per double)
     auto take4 = [&](int n) { int r = o; o += ((n + 3) & ~3) / 2; return r; };
     parent = take4(nj); jtype = take4(nj); idxq = take4(nj); cjoint = take4(nv); ckind = take4(nv);
-    axis = take4(4 * nj); place = take4(8 * nj); caxis = take4(4 * nv); anc = take4(2 * nj);
+    axis = take4(4 * nj); place = take4(8 * nj); caxis = take4(4 * nv); anc = take4(4 * nj);
     lower = take4(nq); upper = take4(nq); misc = take4(8);
     total = o;
   }
@@ -155,7 +155,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   float* place = reinterpret_cast<float*>(sm + L.place);
   float* caxis = reinterpret_cast<float*>(sm + L.caxis);
   int* ancA = reinterpret_cast<int*>(sm + L.anc);
-  int* ancB = ancA + nj;
+  int* ancB = ancA + 2 * nj;
   float* lower = reinterpret_cast<float*>(sm + L.lower);
   float* upper = reinterpret_cast<float*>(sm + L.upper);
   const br_traj_settings_t& S = P.s;
@@ -202,24 +202,28 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   }
   __syncwarp();
 
-  // float64 FK of knot t of trajectory `xs`; returns the world pose buffer
-  auto fk = [&](const double* xs, int t) -> double* {
+  // The two pose terms (goal at knot T-1: term 0, start at knot 0: term 1) are evaluated
+  // together, one per half-warp, when the tree has at most 16 joints; otherwise one after
+  // the other by the whole warp.  Term h uses FK buffers pA / pB + 8 nj h and ancA / ancB + nj h.
+  const bool halves = nj <= 16;
+  // float64 FK of knot t of trajectory `xs` on lanes sl, sl + SL, ...; returns the world poses
+  auto fk = [&](const double* xs, int t, int h, int sl, int SL) -> double* {
     const double* q = xs + t * nv;
-    for (int j = lane; j < nj; j += kWarp) {
+    double* A = pA + 8 * nj * h;
+    double* B = pB + 8 * nj * h;
+    int* aA = ancA + nj * h;
+    int* aB = ancB + nj * h;
+    for (int j = sl; j < nj; j += SL) {
       const Pose Pj = load_pose8(place + 8 * j);
       const DPose Lj = dlocal_transform(jtype[j], DPose{d3(Pj.t.x, Pj.t.y, Pj.t.z),
                                                         make_double4(Pj.q.x, Pj.q.y, Pj.q.z, Pj.q.w)},
                                         axis + 4 * j, q + idxq[j]);
-      std8d(pA + 8 * j, Lj);
-      ancA[j] = parent[j];
+      std8d(A + 8 * j, Lj);
+      aA[j] = parent[j];
     }
     __syncwarp();
-    double* A = pA;
-    double* B = pB;
-    int* aA = ancA;
-    int* aB = ancB;
     for (int r = 0; r < tree.rounds; ++r) {
-      for (int j = lane; j < nj; j += kWarp) {
+      for (int j = sl; j < nj; j += SL) {
         const int a = aA[j];
         if (a >= 0) {
           std8d(B + 8 * j, dcompose(ldd8(A + 8 * a), ldd8(A + 8 * j)));
@@ -235,38 +239,49 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     return A;
   };
-  // pose term at knot t: xi (double, into r[0..5]); if J != null also J = Jr^-1 blockdiag(R^T,R^T) J_lwa (6 x nv)
-  auto pose_term = [&](const double* xs, int t, const Pose& target, double* r, double* J) {
-    double* pose = fk(xs, t);
-    const DPose Tee = dcompose(ldd8(pose + 8 * fpar),
-                               DPose{d3(fpl.t.x, fpl.t.y, fpl.t.z), make_double4(fpl.q.x, fpl.q.y, fpl.q.z, fpl.q.w)});
-    double3 v, w;
-    dse3_log(dcompose(dinverse(DPose{d3(target.t.x, target.t.y, target.t.z),
-                                     make_double4(target.q.x, target.q.y, target.q.z, target.q.w)}), Tee), v, w);
-    if (lane == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
-    if (J) {
-      const DJrInv Jr = djr_inv_se3<9>(v, w);
-      const double4 qc = dqconj(Tee.q);
-      for (int k = lane; k < nv; k += kWarp) {
-        double3 ol = d3(0, 0, 0), oa = d3(0, 0, 0);
-        if ((sup >> cjoint[k]) & 1ull) {
-          const DPose Tj = ldd8(pose + 8 * cjoint[k]);
-          const double3 a = dqrot(Tj.q, d3(caxis[4 * k], caxis[4 * k + 1], caxis[4 * k + 2]));
-          double3 lin, ang;
-          if (ckind[k] == 0) {
-            lin = dcross(a, dsub(Tee.t, Tj.t));
-            ang = a;
-          } else {
-            lin = a;
-            ang = d3(0, 0, 0);
+  // both pose terms at xs: xi (double, into rg / rs); with want_J also
+  // J = Jr^-1 blockdiag(R^T,R^T) J_lwa (6 x nv, into Jg / Js).  A term that is not in the
+  // problem (weight 0 or no start pose) is evaluated but not stored.
+  auto pose_terms = [&](const double* xs, bool want_J) {
+    const int npass = halves ? 1 : 2;
+    for (int pass = 0; pass < npass; ++pass) {
+      const int h = halves ? (lane >> 4) : pass;
+      const int sl = halves ? (lane & 15) : lane, SL = halves ? 16 : kWarp;
+      const bool active = h == 0 ? has_goal : has_start;
+      const Pose& target = h == 0 ? tgt_goal : tgt_start;
+      double* r = h == 0 ? rg : rs;
+      double* J = h == 0 ? Jg : Js;
+      double* pose = fk(xs, h == 0 ? T - 1 : 0, halves ? h : 0, sl, SL);
+      const DPose Tee = dcompose(ldd8(pose + 8 * fpar),
+                                 DPose{d3(fpl.t.x, fpl.t.y, fpl.t.z), make_double4(fpl.q.x, fpl.q.y, fpl.q.z, fpl.q.w)});
+      double3 v, w;
+      dse3_log(dcompose(dinverse(DPose{d3(target.t.x, target.t.y, target.t.z),
+                                       make_double4(target.q.x, target.q.y, target.q.z, target.q.w)}), Tee), v, w);
+      if (active && sl == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
+      if (want_J && active) {
+        const DJrInv Jr = djr_inv_se3<9>(v, w);
+        const double4 qc = dqconj(Tee.q);
+        for (int k = sl; k < nv; k += SL) {
+          double3 ol = d3(0, 0, 0), oa = d3(0, 0, 0);
+          if ((sup >> cjoint[k]) & 1ull) {
+            const DPose Tj = ldd8(pose + 8 * cjoint[k]);
+            const double3 a = dqrot(Tj.q, d3(caxis[4 * k], caxis[4 * k + 1], caxis[4 * k + 2]));
+            double3 lin, ang;
+            if (ckind[k] == 0) {
+              lin = dcross(a, dsub(Tee.t, Tj.t));
+              ang = a;
+            } else {
+              lin = a;
+              ang = d3(0, 0, 0);
+            }
+            djr_inv_apply(Jr, dqrot(qc, lin), dqrot(qc, ang), ol, oa);
           }
-          djr_inv_apply(Jr, dqrot(qc, lin), dqrot(qc, ang), ol, oa);
+          J[0 * nv + k] = ol.x; J[1 * nv + k] = ol.y; J[2 * nv + k] = ol.z;
+          J[3 * nv + k] = oa.x; J[4 * nv + k] = oa.y; J[5 * nv + k] = oa.z;
         }
-        J[0 * nv + k] = ol.x; J[1 * nv + k] = ol.y; J[2 * nv + k] = ol.z;
-        J[3 * nv + k] = oa.x; J[4 * nv + k] = oa.y; J[5 * nv + k] = oa.z;
       }
+      __syncwarp();
     }
-    __syncwarp();
   };
   auto warp_sum = [&](double v) {
 #pragma unroll
@@ -276,8 +291,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   // total cost 0.5 |r|^2 at xs (pose terms evaluated into rg / rs)
   auto cost_of = [&](const double* xs) -> double {
     double acc = 0.0;
-    if (has_goal) pose_term(xs, T - 1, tgt_goal, rg, nullptr);
-    if (has_start) pose_term(xs, 0, tgt_start, rs, nullptr);
+    pose_terms(xs, false);
     for (int e = lane; e < (T - 2) * nv; e += kWarp) {
       const double a = c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
       acc += a * a;
@@ -299,8 +313,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   };
   // J^T J of the pose terms and g = J^T r at x; returns |g|
   auto build = [&]() -> double {
-    if (has_goal) pose_term(x, T - 1, tgt_goal, rg, Jg);
-    if (has_start) pose_term(x, 0, tgt_start, rs, Js);
+    pose_terms(x, true);
     for (int e = lane; e < nv * nv; e += kWarp) {
       const int i = e / nv, j = e - i * nv;
       double a = 0.0, b = 0.0;
@@ -523,7 +536,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   float* xo = P.x + traj * (int64_t)n;
   for (int e = lane; e < n; e += kWarp) xo[e] = (float)x[e];
   if (P.goal_grad && has_goal) {
-    pose_term(x, T - 1, tgt_goal, rg, nullptr);
+    pose_terms(x, false);
     if (lane == 0) {
       const double3 v = d3(rg[0], rg[1], rg[2]);
       const double3 w = d3(rg[3], rg[4], rg[5]);
