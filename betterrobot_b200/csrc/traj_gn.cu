@@ -117,6 +117,8 @@ __device__ __forceinline__ double fast_rsqrt(double x) {
   return y * fma(-0.5 * x * y, y, 1.5);
 }
 
+constexpr int kTrajPairRegs = (2 * BR_MAX_TRAJ_NV * (2 * BR_MAX_TRAJ_NV - 1) / 2 + kWarp - 1) / kWarp;
+
 __global__ void traj_gn_kernel(const TrajParams P) {
   extern __shared__ __align__(16) double sm[];
   const br_tree_t& tree = P.tree;
@@ -202,6 +204,17 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   }
   __syncwarp();
 
+  // packed lower-triangle pairs of the boundary Cholesky's trailing updates (2 nv <= 16:
+  // at most 120 pairs, 4 per lane): p -> (a, b), b <= a, p = a (a + 1) / 2 + b
+  int spair[kTrajPairRegs];
+#pragma unroll
+  for (int i = 0; i < kTrajPairRegs; ++i) {
+    const int p = lane + kWarp * i;
+    int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+    if ((a + 1) * (a + 2) / 2 <= p) ++a;
+    if (a * (a + 1) / 2 > p) --a;
+    spair[i] = a | ((p - a * (a + 1) / 2) << 8);
+  }
   // The two pose terms (goal at knot T-1: term 0, start at knot 0: term 1) are evaluated
   // together, one per half-warp, when the tree has at most 16 joints; otherwise one after
   // the other by the whole warp.  Term h uses FK buffers pA / pB + 8 nj h and ancA / ancB + nj h.
@@ -466,9 +479,15 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       if (lane > k && lane < nb) Sb[lane * nb + k] *= inv;
       if (lane == k) { Sb[k * nb + k] = sk; sdi[k] = inv; }
       __syncwarp();
-      if (lane > k && lane < nb) {                                 // lane r updates row r
-        const double lrk = Sb[lane * nb + k];
-        for (int cc = k + 1; cc <= lane; ++cc) Sb[lane * nb + cc] -= lrk * Sb[cc * nb + k];
+      // trailing update S[r][cc] -= L[r][k] L[cc][k], k < cc <= r < nb, as packed pairs
+      // (r - k - 1, cc - k - 1) = pair p of the lane (decoded once, p = lane + 32 i)
+      const int np = (nb - k - 1) * (nb - k) / 2;
+#pragma unroll
+      for (int i = 0; i < kTrajPairRegs; ++i) {
+        if (lane + kWarp * i < np) {
+          const int r = (spair[i] & 0xff) + k + 1, cc = (spair[i] >> 8) + k + 1;
+          Sb[r * nb + cc] -= Sb[r * nb + k] * Sb[cc * nb + k];
+        }
       }
       __syncwarp();
     }
