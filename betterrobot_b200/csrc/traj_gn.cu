@@ -409,6 +409,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       if (good) {
         // forward L z = (r, h0, hT), r = -g on the interior; h0 / hT: the columns of knots 0 / T-1
         double y1 = 0, y2 = 0, u1 = 0, u2 = 0, w1 = 0, w2 = 0;
+#pragma unroll 2
         for (int p = 0; p < m; ++p) {
           const int t = p + 1;
           const double l1 = bl1[p * nv + i], l2 = bl2[p * nv + i];
@@ -422,6 +423,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         }
         // backward D L^T v = z
         y1 = y2 = u1 = u2 = w1 = w2 = 0;
+#pragma unroll 2
         for (int p = m - 1; p >= 0; --p) {
           const double di = bdi[p * nv + i];
           const double l1n = (p + 1 < m) ? bl1[(p + 1) * nv + i] : 0.0;   // L[p+1][p]
@@ -436,9 +438,10 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     if (!__all_sync(0xffffffffu, good)) return false;
     // boundary block H_bb: b = i for (knot 0, DOF i), nv + i for (knot T-1, DOF i)
-    for (int e = lane; e < nb * nb; e += kWarp) {
-      const int r = e / nb, cc = e - r * nb;
-      const int kr = r / nv, kc = cc / nv, ir = r - kr * nv, ic = cc - kc * nv;
+    for (int r0 = 0; r0 < nb; r0 += 2) {                          // two rows per pass (nb <= 16)
+      const int r = r0 + (lane >> 4), cc = lane & 15;
+      if (r >= nb || cc >= nb) continue;
+      const int kr = r >= nv, kc = cc >= nv, ir = r - kr * nv, ic = cc - kc * nv;
       double h = 0.0;
       if (kr == kc) {
         if (kr == 0 && has_start) h = jtjs[ir * nv + ic];
@@ -447,7 +450,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       } else if (ir == ic && T == 3) {
         h = c2;                                                    // row 0 couples knots 0 and 2
       }
-      Sb[e] = h;
+      Sb[r * nb + cc] = h;
     }
     __syncwarp();
     if (lane < nv) {
