@@ -44,6 +44,19 @@ def chain_spec(seed: int = 0, n: int = 7, name: str = "chain7") -> dict:
     return {"name": name, "joints": joints, "frames": frames}
 
 
+def floating_chain_spec(seed: int = 4, n: int = 4) -> dict:
+    """Floating-base chain: free-flyer root, ``n`` revolute-z joints, one tool frame ``ee``
+    (a floating-base robot small enough for the reference's dense trajectory solver)."""
+    rng = np.random.default_rng(seed)
+    joints = [{"name": "root_joint", "kind": "free_flyer", "parent": 0, "body": "base"}]
+    for i in range(n):
+        joints.append({"name": f"j{i + 1}", "kind": "revolute_rz", "parent": i + 1,
+                       "origin": _rand_pose(rng), "lower": -LIMIT, "upper": LIMIT,
+                       "body": f"link{i + 1}"})
+    frames = [{"name": "ee", "parent": n + 1, "placement": _rand_pose(rng)}]
+    return {"name": "floating_chain", "joints": joints, "frames": frames}
+
+
 def dual_arm_spec(seed: int = 2, n: int = 7) -> dict:
     """Fixed base with two ``n``-revolute chains; tool frames ``ee_l`` and ``ee_r``."""
     rng = np.random.default_rng(seed)
@@ -207,13 +220,28 @@ def _quat_mul_np(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 
 def trajopt_endpoints(model: Model, n: int, seed: int, spread: float = 1.0):
     """Start and goal configurations (float64) for trajectory problems: start uniform in
-    +-2.5 rad, goal = start + U(+-spread) per joint, both clamped to the joint limits."""
+    +-2.5 rad, goal = start + U(+-spread) per joint, both clamped to the joint limits.  A
+    free-flyer base starts at a translation U(+-0.5) m with a uniform random orientation and
+    moves by U(+-0.2 spread) m and a rotation exp(U(+-0.3 spread)) composed on the right."""
     rng = np.random.default_rng(seed)
     lo = model.lower_pos_limit.double().numpy()
     hi = model.upper_pos_limit.double().numpy()
     q0 = rng.uniform(-2.5, 2.5, size=(n, model.nq))
     q1 = np.clip(q0 + rng.uniform(-spread, spread, size=(n, model.nq)), lo, hi)
-    return torch.from_numpy(np.clip(q0, lo, hi)), torch.from_numpy(q1)
+    q0 = np.clip(q0, lo, hi)
+    for j, jm in enumerate(model.joint_models):
+        if jm.kind != "free_flyer":
+            continue
+        iq = model.idx_qs[j]
+        q0[:, iq:iq + 3] = rng.uniform(-0.5, 0.5, size=(n, 3))
+        u = rng.normal(size=(n, 4))
+        q0[:, iq + 3:iq + 7] = u / np.linalg.norm(u, axis=1, keepdims=True)
+        q1[:, iq:iq + 3] = q0[:, iq:iq + 3] + rng.uniform(-0.2 * spread, 0.2 * spread, size=(n, 3))
+        w = rng.uniform(-0.3 * spread, 0.3 * spread, size=(n, 3))
+        th = np.linalg.norm(w, axis=1, keepdims=True)
+        sh = np.where(th > 1e-12, np.sin(0.5 * th) / np.maximum(th, 1e-12), 0.5)
+        q1[:, iq + 3:iq + 7] = _quat_mul_np(q0[:, iq + 3:iq + 7], np.concatenate([sh * w, np.cos(0.5 * th)], 1))
+    return torch.from_numpy(q0), torch.from_numpy(q1)
 
 
 def ik_uneven_mix(n_problems: int, seed: int = 3) -> list[tuple[str, int]]:

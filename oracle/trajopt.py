@@ -11,8 +11,11 @@ or ``LevenbergMarquardt`` (``levenberg_marquardt.py:61-135``) on the cost stack
 * ``ref``:   ``ReferenceTrajectoryResidual(model, q_ref)`` (``residuals/regularization.py:66-152``),
 
 each with a scalar ``CostStack`` item weight (``costs/stack.py:104-144``), with the
-dense ``(dim, T*nv)`` Jacobian the reference builds.  Fixed-base models with
-``nq == nv`` only (``Model.difference`` is then ``q1 - q0``).
+dense ``(dim, T*nv)`` Jacobian the reference builds: the acceleration and reference
+residuals through ``Model.difference`` with identity Jacobian blocks (the reference's
+identity-right-Jacobian approximation, ``smoothness.py:98-108``), the limits through the
+``(nq, nv)`` projection of ``limits.py:36-48`` (zero rows for joints with ``nq != nv``),
+and the knot retraction through ``Model.integrate`` (``trajopt.py:159-169``).
 """
 
 from __future__ import annotations
@@ -76,7 +79,8 @@ def residual_jacobian(model, X, frame_id, goal, start, q_ref, s: TrajSettings, w
         pose_block(0, start, s.w_start)
     if s.w_accel > 0:                                                   # smoothness.py:118-142
         c = s.w_accel / s.dt ** 2
-        a = (X[:, 2:] - X[:, 1:-1]) - (X[:, 1:-1] - X[:, :-2])
+        d = np.stack([K.difference(model, X[:, t], X[:, t + 1]) for t in range(T - 1)], 1)  # (N, T-1, nv)
+        a = d[:, 1:] - d[:, :-1]
         rs.append((a * c).reshape(N, -1))
         if want_jac:
             J = np.zeros((N, (T - 2) * nv, T * nv))
@@ -89,6 +93,11 @@ def residual_jacobian(model, X, frame_id, goal, start, q_ref, s: TrajSettings, w
     if s.w_limit > 0:                                                   # limits.py:56-86 per knot
         lo = K._np(model.lower_pos_limit)
         hi = K._np(model.upper_pos_limit)
+        dq_dv = np.zeros((nq, nv))                                      # limits.py:36-48
+        for j, jm in enumerate(model.joint_models):
+            if jm.nq and jm.nq == jm.nv:
+                for k in range(jm.nq):
+                    dq_dv[model.idx_qs[j] + k, model.idx_vs[j] + k] = 1.0
         for t in range(T):
             q = X[:, t]
             rs.append(np.concatenate([np.maximum(lo - q, 0.0), np.maximum(q - hi, 0.0)], -1) * s.w_limit)
@@ -96,12 +105,12 @@ def residual_jacobian(model, X, frame_id, goal, start, q_ref, s: TrajSettings, w
                 full = np.zeros((N, 2 * nq, T * nv))
                 ld = np.where(q < lo, -1.0, 0.0)
                 ud = np.where(q > hi, 1.0, 0.0)
-                idx = np.arange(nv)
-                full[:, idx, t * nv + idx] = ld * s.w_limit
-                full[:, nq + idx, t * nv + idx] = ud * s.w_limit
+                full[:, :nq, t * nv:(t + 1) * nv] = ld[..., None] * dq_dv * s.w_limit
+                full[:, nq:, t * nv:(t + 1) * nv] = ud[..., None] * dq_dv * s.w_limit
                 Js.append(full)
     if s.w_ref > 0:                                                     # regularization.py:133-152
-        rs.append(((X - q_ref) * s.w_ref).reshape(N, -1))
+        r_ref = np.stack([K.difference(model, q_ref[:, t], X[:, t]) for t in range(T)], 1)
+        rs.append((r_ref * s.w_ref).reshape(N, -1))
         if want_jac:
             Js.append(np.broadcast_to(np.eye(T * nv) * s.w_ref, (N, T * nv, T * nv)))
     r = np.concatenate(rs, -1)
@@ -140,7 +149,8 @@ def solve(model, X0, frame_id, goal, start, s: TrajSettings, q_ref=None) -> Traj
         g = (np.swapaxes(J, -1, -2) @ r_a[..., None])[..., 0]
         damp = lam[idx] if s.optimizer == "lm" else np.full(idx.size, s.gn_eps)
         d = oik._solve(JtJ + damp[:, None, None] * np.eye(n), -g)
-        Xn = X[idx] + d.reshape(-1, T, nq)                                # knot retraction (trajopt.py:159-169)
+        d = d.reshape(-1, T, model.nv)                                   # knot retraction (trajopt.py:159-169)
+        Xn = np.stack([K.integrate(model, X[idx][:, t], d[:, t]) for t in range(T)], 1)
         rn, _ = residual_jacobian(model, Xn, frame_id, goal[idx], None if start is None else start[idx],
                                   q_ref[idx], s, want_jac=False)
         cn = 0.5 * (rn * rn).sum(-1)

@@ -21,6 +21,8 @@ and outputs in ``tests/golden/*.npz``:
                       (``tasks/ik.py:191-226``) but with the configs' damping.
 * ``adjoint.npz``   — pose loss ``sum_f w_f |log(T_f^-1 oMf(q))|^2`` and its autograd
                       gradient w.r.t. raw ``q`` (free-flyer quaternion included).
+* ``trajopt_floating.npz`` — the same ``solve_trajopt`` stack on a floating-base chain
+                      (acceleration and reference residuals through ``Model.difference``).
 * ``adjoint_mixed.npz`` — the same on the robot with every multi-slot joint kind
                       (planar, translation, spherical, unbounded revolute).
 """
@@ -352,6 +354,9 @@ def main():
     if only == ["adjoint_mixed"]:   # regenerate one fixture: make_golden.py <src> adjoint_mixed
         make_adjoint(syn.mixed_spec(), 8, 33, os.path.join(HERE, "adjoint_mixed.npz"))
         return
+    if only == ["trajopt_floating"]:
+        make_trajopt(syn.floating_chain_spec(), 3, 12, 43, os.path.join(HERE, "trajopt_floating.npz"))
+        return
     make_lie(os.path.join(HERE, "lie.npz"))
     make_lie_ops(os.path.join(HERE, "lie_ops.npz"))
     chain, hum, dual = syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()
@@ -375,6 +380,7 @@ def main():
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
     make_adjoint(syn.mixed_spec(), 8, 33, os.path.join(HERE, "adjoint_mixed.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
+    make_trajopt(syn.floating_chain_spec(), 3, 12, 43, os.path.join(HERE, "trajopt_floating.npz"))
 
 
 if __name__ == "__main__":
