@@ -64,15 +64,18 @@ struct TrajParams {
 
 struct TrajLayout {
   // doubles
-  int x, xn, xref, g, delta, bl1, bl2, bdi, vy, vu, vw, Sb, sdi, rb, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
+  int x, xn, xref, dd, dr, g, delta, bl1, bl2, bdi, vy, vu, vw, Sb, sdi, rb, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
   int total_doubles;
   // ints / floats (in units of doubles)
-  int parent, jtype, idxq, cjoint, ckind, axis, place, caxis, anc, lower, upper, misc;
+  int parent, jtype, idxq, idxv, dofq, cjoint, ckind, axis, place, caxis, anc, lower, upper, misc;
   int total;
   __host__ __device__ TrajLayout(int nj, int nq, int nv, int T) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };  // 16-byte aligned
-    x = take(T * nv); xn = take(T * nv); xref = take(T * nv); g = take(T * nv); delta = take(T * nv);
+    x = take(T * nq); xn = take(T * nq); xref = take(T * nq); g = take(T * nv); delta = take(T * nv);
+    // knot differences difference(x_t, x_{t+1}) and difference(xref_t, x_t) of the last
+    // evaluated trajectory (floating-base trees; fixed-base trees subtract inline)
+    dd = take(T * nv); dr = take(T * nv);
     // per-DOF interior bands (index p * nv + i, p = knot - 1): L[p][p-1], L[p][p-2], 1 / D[p];
     // solutions of P_i y = r, P_i u = h0, P_i w = hT
     bl1 = take(T * nv); bl2 = take(T * nv); bdi = take(T * nv);
@@ -83,7 +86,8 @@ struct TrajLayout {
     total_doubles = o;
     // 4-byte arrays: count in doubles (2 per double)
     auto take4 = [&](int n) { int r = o; o += ((n + 3) & ~3) / 2; return r; };
-    parent = take4(nj); jtype = take4(nj); idxq = take4(nj); cjoint = take4(nv); ckind = take4(nv);
+    parent = take4(nj); jtype = take4(nj); idxq = take4(nj); idxv = take4(nj); dofq = take4(nv);
+    cjoint = take4(nv); ckind = take4(nv);
     axis = take4(4 * nj); place = take4(8 * nj); caxis = take4(4 * nv); anc = take4(4 * nj);
     lower = take4(nq); upper = take4(nq); misc = take4(8);
     total = o;
@@ -117,8 +121,13 @@ __device__ __forceinline__ double fast_rsqrt(double x) {
   return y * fma(-0.5 * x * y, y, 1.5);
 }
 
-constexpr int kTrajPairRegs = (2 * BR_MAX_TRAJ_NV * (2 * BR_MAX_TRAJ_NV - 1) / 2 + kWarp - 1) / kWarp;
+// pair decodes of the boundary Cholesky kept in registers (p < 32 * kTrajPairRegs); larger
+// boundary blocks decode the rest on the fly
+constexpr int kTrajPairRegs = 4;
 
+// kFloating: the tree has free-flyer joints (nq != nv): knot differences and the retraction
+// go through Model.difference / Model.integrate; otherwise they are q1 - q0 and q + v.
+template <bool kFloating>
 __global__ void traj_gn_kernel(const TrajParams P) {
   extern __shared__ __align__(16) double sm[];
   const br_tree_t& tree = P.tree;
@@ -151,6 +160,10 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   int* parent = reinterpret_cast<int*>(sm + L.parent);
   int* jtype = reinterpret_cast<int*>(sm + L.jtype);
   int* idxq = reinterpret_cast<int*>(sm + L.idxq);
+  int* idxv = reinterpret_cast<int*>(sm + L.idxv);
+  int* dofq = reinterpret_cast<int*>(sm + L.dofq);  // q slot of a DOF with a position limit, else -1
+  double* dd = sm + L.dd;
+  double* dr = sm + L.dr;
   int* cjoint = reinterpret_cast<int*>(sm + L.cjoint);
   int* ckind = reinterpret_cast<int*>(sm + L.ckind);
   float* axis = reinterpret_cast<float*>(sm + L.axis);
@@ -166,12 +179,13 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   const double wl = S.w_limit, wr = S.w_ref, wg = S.w_goal, ws = S.w_start;
   const bool has_start = P.start != nullptr && S.w_start > 0.f;
   const bool has_goal = S.w_goal > 0.f;
-  const int n = T * nv;
+  const int n = T * nv, nqT = T * nq;
 
   for (int j = lane; j < nj; j += kWarp) {
     parent[j] = tree.parent[j];
     jtype[j] = tree.jtype[j];
     idxq[j] = tree.idx_q[j];
+    idxv[j] = tree.idx_v[j];
     for (int k = 0; k < 4; ++k) axis[4 * j + k] = tree.axis[4 * j + k];
     for (int k = 0; k < 8; ++k) place[8 * j + k] = tree.placement[8 * j + k];
   }
@@ -184,9 +198,15 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     lower[i] = tree.lower[i];
     upper[i] = tree.upper[i];
   }
-  const float* x0 = P.x0 + traj * (int64_t)n;
-  const float* xr = (P.xref ? P.xref : P.x0) + traj * (int64_t)n;
-  for (int i = lane; i < n; i += kWarp) {
+  __syncwarp();
+  for (int j = lane; j < nj; j += kWarp) {          // limits.py:36-48: nq == nv joints only
+    const int jt = jtype[j];
+    const bool vec = joint_is_vector(jt);
+    for (int k = 0; k < joint_nv(jt); ++k) dofq[idxv[j] + k] = vec ? idxq[j] + k : -1;
+  }
+  const float* x0 = P.x0 + traj * (int64_t)nqT;
+  const float* xr = (P.xref ? P.xref : P.x0) + traj * (int64_t)nqT;
+  for (int i = lane; i < nqT; i += kWarp) {
     x[i] = x0[i];
     xref[i] = xr[i];
   }
@@ -204,8 +224,8 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   }
   __syncwarp();
 
-  // packed lower-triangle pairs of the boundary Cholesky's trailing updates (2 nv <= 16:
-  // at most 120 pairs, 4 per lane): p -> (a, b), b <= a, p = a (a + 1) / 2 + b
+  // packed lower-triangle pairs of the boundary Cholesky's trailing updates: p -> (a, b),
+  // b <= a, p = a (a + 1) / 2 + b, for the lane's first kTrajPairRegs pair indices
   int spair[kTrajPairRegs];
 #pragma unroll
   for (int i = 0; i < kTrajPairRegs; ++i) {
@@ -221,7 +241,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   const bool halves = nj <= 16;
   // float64 FK of knot t of trajectory `xs` on lanes sl, sl + SL, ...; returns the world poses
   auto fk = [&](const double* xs, int t, int h, int sl, int SL) -> double* {
-    const double* q = xs + t * nv;
+    const double* q = xs + t * nq;
     double* A = pA + 8 * nj * h;
     double* B = pB + 8 * nj * h;
     int* aA = ancA + nj * h;
@@ -301,19 +321,76 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
   };
+  // floating-base trees: dd[t] = difference(xs_t, xs_{t+1}) (t < T-1) and dr[t] =
+  // difference(xref_t, xs_t) (model.py:176-190; free-flyer log(q_a^-1 q_b), free_flyer.py:53-57)
+  auto knot_differences = [&](const double* xs) {
+    const int npair = 2 * T - 1;
+    for (int e = lane; e < npair * nj; e += kWarp) {
+      const int pi = e / nj, j = e - pi * nj;
+      const int jt = jtype[j], nvj = joint_nv(jt);
+      if (nvj == 0) continue;
+      const double* qa;
+      const double* qb;
+      double* out;
+      if (pi < T - 1) {
+        qa = xs + pi * nq; qb = xs + (pi + 1) * nq; out = dd + pi * nv;
+      } else {
+        const int t = pi - (T - 1);
+        qa = xref + t * nq; qb = xs + t * nq; out = dr + t * nv;
+      }
+      const int iq = idxq[j], iv = idxv[j];
+      if (jt == BR_JOINT_FREE_FLYER) {
+        const DPose a{d3(qa[iq], qa[iq + 1], qa[iq + 2]), make_double4(qa[iq + 3], qa[iq + 4], qa[iq + 5], qa[iq + 6])};
+        const DPose b{d3(qb[iq], qb[iq + 1], qb[iq + 2]), make_double4(qb[iq + 3], qb[iq + 4], qb[iq + 5], qb[iq + 6])};
+        double3 v, w;
+        dse3_log(dcompose(dinverse(a), b), v, w);
+        out[iv] = v.x; out[iv + 1] = v.y; out[iv + 2] = v.z;
+        out[iv + 3] = w.x; out[iv + 4] = w.y; out[iv + 5] = w.z;
+      } else {
+        for (int k = 0; k < nvj; ++k) out[iv + k] = qb[iq + k] - qa[iq + k];
+      }
+    }
+    __syncwarp();
+  };
+  // floating-base trees: xn_t = integrate(x_t, delta_t) per knot (model.py:160-174;
+  // free-flyer normalize(q . exp(v)), free_flyer.py:47-51)
+  auto retract_knots = [&]() {
+    for (int e = lane; e < T * nj; e += kWarp) {
+      const int t = e / nj, j = e - t * nj;
+      const int jt = jtype[j], nvj = joint_nv(jt);
+      if (nvj == 0) continue;
+      const int iq = idxq[j], iv = idxv[j];
+      const double* q = x + t * nq;
+      const double* dv = delta + t * nv;
+      double* o = xn + t * nq;
+      if (jt == BR_JOINT_FREE_FLYER) {
+        const DPose a{d3(q[iq], q[iq + 1], q[iq + 2]), make_double4(q[iq + 3], q[iq + 4], q[iq + 5], q[iq + 6])};
+        DPose b = dcompose(a, dse3_exp(d3(dv[iv], dv[iv + 1], dv[iv + 2]), d3(dv[iv + 3], dv[iv + 4], dv[iv + 5])));
+        b.q = dqnormalize(b.q);
+        o[iq] = b.t.x; o[iq + 1] = b.t.y; o[iq + 2] = b.t.z;
+        o[iq + 3] = b.q.x; o[iq + 4] = b.q.y; o[iq + 5] = b.q.z; o[iq + 6] = b.q.w;
+      } else {
+        for (int k = 0; k < nvj; ++k) o[iq + k] = q[iq + k] + dv[iv + k];
+      }
+    }
+  };
   // total cost 0.5 |r|^2 at xs (pose terms evaluated into rg / rs)
   auto cost_of = [&](const double* xs) -> double {
     double acc = 0.0;
     pose_terms(xs, false);
-    for (int e = lane; e < (T - 2) * nv; e += kWarp) {
-      const double a = c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
+    if (kFloating) knot_differences(xs);
+    for (int e = lane; e < (T - 2) * nv; e += kWarp) {          // smoothness.py:118-125
+      const double a = kFloating ? c * (dd[e + nv] - dd[e]) : c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
       acc += a * a;
     }
-    for (int e = lane; e < n; e += kWarp) {
-      const int i = e % nv;
+    for (int e = lane; e < nqT; e += kWarp) {                   // limits.py:56-62
+      const int i = e % nq;
       const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
-      const double d = xs[e] - xref[e];
-      acc += wl * wl * (lo * lo + hi * hi) + wr * wr * d * d;
+      acc += wl * wl * (lo * lo + hi * hi);
+    }
+    for (int e = lane; e < n; e += kWarp) {                     // regularization.py:143-152
+      const double d = kFloating ? dr[e] : xs[e] - xref[e];
+      acc += wr * wr * d * d;
     }
     acc = warp_sum(acc);
     double pc = 0.0;
@@ -341,14 +418,22 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     for (int e = lane; e < n; e += kWarp) {
       const int t = e / nv, i = e - t * nv;
       double acc = 0.0;
-      // acceleration rows s = t, t-1, t-2 with coefficients +1, -2, +1 at knot t
-      auto arow = [&](int s) { return c * (x[(s + 2) * nv + i] - 2.0 * x[(s + 1) * nv + i] + x[s * nv + i]); };
+      // acceleration rows s = t, t-1, t-2 with coefficients +1, -2, +1 at knot t (the
+      // identity-Jacobian blocks of smoothness.py:127-142)
+      auto arow = [&](int s) {
+        return kFloating ? c * (dd[(s + 1) * nv + i] - dd[s * nv + i])
+                         : c * (x[(s + 2) * nv + i] - 2.0 * x[(s + 1) * nv + i] + x[s * nv + i]);
+      };
       if (t <= T - 3) acc += c * arow(t);
       if (t - 1 >= 0 && t - 1 <= T - 3) acc += -2.0 * c * arow(t - 1);
       if (t - 2 >= 0) acc += c * arow(t - 2);
-      if (x[e] < (double)lower[i]) acc -= wl * wl * ((double)lower[i] - x[e]);
-      if (x[e] > (double)upper[i]) acc += wl * wl * (x[e] - (double)upper[i]);
-      acc += wr * wr * (x[e] - xref[e]);
+      const int iq = kFloating ? dofq[i] : i;
+      if (iq >= 0) {
+        const double xq = x[t * nq + iq];
+        if (xq < (double)lower[iq]) acc -= wl * wl * ((double)lower[iq] - xq);
+        if (xq > (double)upper[iq]) acc += wl * wl * (xq - (double)upper[iq]);
+      }
+      acc += wr * wr * (kFloating ? dr[e] : x[e] - xref[e]);
       if (has_goal && t == T - 1)
         for (int r = 0; r < 6; ++r) acc += wg * wg * Jg[r * nv + i] * rg[r];
       if (has_start && t == 0)
@@ -368,10 +453,13 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     if (t <= T - 3) a += 1.0;
     if (t - 1 >= 0 && t - 1 <= T - 3) a += 4.0;
     if (t - 2 >= 0) a += 1.0;
-    const double xv = x[t * nv + i];
     double d = c2 * a + wr * wr + damp;
-    if (xv < (double)lower[i]) d += wl * wl;
-    if (xv > (double)upper[i]) d += wl * wl;
+    const int iq = kFloating ? dofq[i] : i;
+    if (iq >= 0) {
+      const double xv = x[t * nq + iq];
+      if (xv < (double)lower[iq]) d += wl * wl;
+      if (xv > (double)upper[iq]) d += wl * wl;
+    }
     return d;
   };
   auto hoff1 = [&](int t) -> double {
@@ -438,8 +526,9 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     if (!__all_sync(0xffffffffu, good)) return false;
     // boundary block H_bb: b = i for (knot 0, DOF i), nv + i for (knot T-1, DOF i)
-    for (int r0 = 0; r0 < nb; r0 += 2) {                          // two rows per pass (nb <= 16)
-      const int r = r0 + (lane >> 4), cc = lane & 15;
+    const bool two = nb <= 16;                                     // two rows per pass, else one
+    for (int r0 = 0; r0 < nb; r0 += two ? 2 : 1) {
+      const int r = r0 + (two ? (lane >> 4) : 0), cc = two ? (lane & 15) : lane;
       if (r >= nb || cc >= nb) continue;
       const int kr = r >= nv, kc = cc >= nv, ir = r - kr * nv, ic = cc - kc * nv;
       double h = 0.0;
@@ -492,6 +581,13 @@ __global__ void traj_gn_kernel(const TrajParams P) {
           Sb[r * nb + cc] -= Sb[r * nb + k] * Sb[cc * nb + k];
         }
       }
+      for (int pp = lane + kWarp * kTrajPairRegs; pp < np; pp += kWarp) {   // nb > 17 only
+        int a = (int)((sqrtf(8.f * pp + 1.f) - 1.f) * 0.5f);
+        if ((a + 1) * (a + 2) / 2 <= pp) ++a;
+        if (a * (a + 1) / 2 > pp) --a;
+        const int r = a + k + 1, cc = pp - a * (a + 1) / 2 + k + 1;
+        Sb[r * nb + cc] -= Sb[r * nb + k] * Sb[cc * nb + k];
+      }
       __syncwarp();
     }
     // z = S^-1 rb: lane b owns entry b; one finished entry broadcast per step
@@ -539,13 +635,17 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         __syncwarp();
       }
     }
-    for (int e = lane; e < n; e += kWarp) xn[e] = x[e] + delta[e];  // knot retraction: q + dv (nq == nv)
+    if (kFloating) {                                               // Model.integrate per knot (trajopt.py:159-169)
+      retract_knots();
+    } else {
+      for (int e = lane; e < n; e += kWarp) xn[e] = x[e] + delta[e];
+    }
     __syncwarp();
     const double cn = cost_of(xn);
     if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
     bool accept = !lm || cn < cost;
     if (accept) {
-      for (int e = lane; e < n; e += kWarp) x[e] = xn[e];
+      for (int e = lane; e < nqT; e += kWarp) x[e] = xn[e];
       __syncwarp();
       cost = cn;
       need = true;
@@ -555,8 +655,8 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       lam = fmin(lam * S.factor, (double)S.lam_max);
     }
   }
-  float* xo = P.x + traj * (int64_t)n;
-  for (int e = lane; e < n; e += kWarp) xo[e] = (float)x[e];
+  float* xo = P.x + traj * (int64_t)nqT;
+  for (int e = lane; e < nqT; e += kWarp) xo[e] = (float)x[e];
   if (P.goal_grad && has_goal) {
     pose_terms(x, false);
     if (lane == 0) {
@@ -590,12 +690,13 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
   if (st) return st;
   if (!settings || n_traj < 0 || knots < 3) return BR_EINVAL;
   if (knots > BR_MAX_TRAJ_KNOTS || tree->nv > BR_MAX_TRAJ_NV) return BR_ETOOBIG;
-  if (tree->nq != tree->nv) return BR_EINVAL;  // fixed-base trees: difference(q0, q1) = q1 - q0
   {
     const int ok = (1 << BR_JOINT_FIXED) | (1 << BR_JOINT_REVOLUTE) | (1 << BR_JOINT_PRISMATIC) |
-                   (1 << BR_JOINT_TRANSLATION);
-    if (tree->kinds == 0 || (tree->kinds & ~ok)) return BR_EINVAL;  // q + v kinds only
+                   (1 << BR_JOINT_TRANSLATION) | (1 << BR_JOINT_FREE_FLYER);
+    if (tree->kinds == 0 || (tree->kinds & ~ok)) return BR_EINVAL;  // q + v kinds and free-flyers
   }
+  const bool floating = (tree->kinds >> BR_JOINT_FREE_FLYER) & 1;
+  if (!floating && tree->nq != tree->nv) return BR_EINVAL;
   if (frame_id < 0 || frame_id >= tree->nframes) return BR_EINVAL;
   if (n_traj == 0) return BR_OK;
   if (!x0 || !goal || !x || !iters || !status || !cost) return BR_EINVAL;
@@ -612,13 +713,15 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
   const size_t bytes = (size_t)L.total * sizeof(double);
   const DeviceInfo& dev = device_info();
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  static int configured[16] = {0};
-  if ((int)bytes > configured[dev.device & 15]) {
-    cudaError_t e = cudaFuncSetAttribute(traj_gn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  auto kern = floating ? traj_gn_kernel<true> : traj_gn_kernel<false>;
+  static int configured[2][16] = {{0}};
+  int& conf = configured[floating ? 1 : 0][dev.device & 15];
+  if ((int)bytes > conf) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return (int)e;
-    configured[dev.device & 15] = (int)bytes;
+    conf = (int)bytes;
   }
   if (n_traj > 0x7fffffff) return BR_ETOOBIG;
-  traj_gn_kernel<<<(unsigned)n_traj, kWarp, bytes, (cudaStream_t)stream>>>(p);
+  kern<<<(unsigned)n_traj, kWarp, bytes, (cudaStream_t)stream>>>(p);
   return (int)cudaGetLastError();
 }

@@ -283,7 +283,7 @@ BR_API int br_pose_loss_backward(const br_tree_t* tree, const float* q, const fl
 
 /* ==== batched trajectory optimisation (Gauss-Newton / LM) ================ */
 #define BR_MAX_TRAJ_KNOTS 128
-#define BR_MAX_TRAJ_NV 8
+#define BR_MAX_TRAJ_NV 16
 
 /* Cost stack weights (CostStack item weights) and solver settings.  Terms with
  * weight 0 are left out. */
@@ -300,11 +300,13 @@ typedef struct br_traj_settings {
 
 /*
  * Solve n_traj independent trajectories of `knots` configurations each, one warp
- * per trajectory, with a bandwidth-2 block Cholesky of the block-pentadiagonal
- * normal equations.  x0 / x_ref / x are [n_traj, knots, nq] (x_ref NULL = x0),
- * goal / start are [n_traj, 7] poses of frame `frame_id` (start may be NULL).
- * goal_grad (NULL or [n_traj, 6]) receives d(final cost)/d(eps) for the goal
- * perturbed as T_goal * exp(eps).  Fixed-base trees only (nq == nv <= 8).
+ * per trajectory, with the Newton step in nested-dissection order (per-DOF
+ * pentadiagonal interior, dense Schur complement on the end knots).  x0 / x_ref / x
+ * are [n_traj, knots, nq] (x_ref NULL = x0), goal / start are [n_traj, 7] poses of
+ * frame `frame_id` (start may be NULL).  goal_grad (NULL or [n_traj, 6]) receives
+ * d(final cost)/d(eps) for the goal perturbed as T_goal * exp(eps).  Joints: fixed,
+ * revolute, prismatic, translation and free-flyer (knot differences and the
+ * retraction through Model.difference / Model.integrate); nv <= BR_MAX_TRAJ_NV.
  * Replaces solve_trajopt with the knot parameterisation and its dense LM / GN
  * (src/better_robot/tasks/trajopt.py:84-230) on the goal / start / acceleration /
  * limit / reference-trajectory stack.

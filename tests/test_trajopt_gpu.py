@@ -1,4 +1,4 @@
-"""GPU parity of the batched trajectory optimiser (block-banded GN / LM) and its goal adjoint.
+"""GPU parity of the batched trajectory optimiser (GN / LM) and its goal adjoint.
 
 Bars:
 * reference ``solve_trajopt`` (golden, float64): same converged verdict, trajectory
@@ -49,11 +49,15 @@ def _gpu(m, fid, goal, start, X0, cfg):
                                      start=torch.from_numpy(start).float().cuda(), cfg=cfg)
 
 
-def test_reference_solve_trajopt_golden():
-    g = np.load(os.path.join(GOLDEN, "trajopt_chain7.npz"))
+@pytest.mark.parametrize("fixture", ["trajopt_chain7.npz", "trajopt_floating.npz"])
+def test_reference_solve_trajopt_golden(fixture):
+    """The reference's float64 solve_trajopt: the 7-DOF chain, and a floating-base chain whose
+    knots move by Model.integrate and whose acceleration uses Model.difference."""
+    g = np.load(os.path.join(GOLDEN, fixture))
     T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
-    m = syn.model_from_spec(syn.chain_spec())
-    m64 = syn.model_from_spec(syn.chain_spec(), dtype=torch.float64)
+    spec = syn.chain_spec() if fixture == "trajopt_chain7.npz" else syn.floating_chain_spec()
+    m = syn.model_from_spec(spec)
+    m64 = syn.model_from_spec(spec, dtype=torch.float64)
     fid = m.frame_id("ee")
     X0 = np.repeat(g["q_start"][:, None, :], int(T), 1)
     cfg = btr.TrajOptConfig(dt=float(dt), w_goal=float(wg), w_start=float(ws), w_accel=float(wa), w_limit=float(wl),
@@ -128,8 +132,34 @@ def test_goal_gradient_envelope_vs_resolved_cost():
     assert (rel[ok] <= 2e-2).all(), rel
 
 
-def test_trajopt_rejects_free_flyer_and_bad_shapes():
-    m = syn.model_from_spec(syn.humanoid_spec())
+def test_floating_base_vs_oracle():
+    """Floating-base chain (free-flyer knots), 16 trajectories x 24 knots, against the float64 oracle."""
+    spec = syn.floating_chain_spec()
+    m, m64 = syn.model_from_spec(spec), syn.model_from_spec(spec, dtype=torch.float64)
+    fid = m.frame_id("ee")
+    N, T = 16, 24
+    qs, qg = syn.trajopt_endpoints(m64, N, 47, 0.5)
+    oMi, _ = K.forward_kinematics(m64, qg.numpy())
+    goal = K.frame_placements(m64, oMi, [fid])[:, 0]
+    oMi, _ = K.forward_kinematics(m64, qs.numpy())
+    start = K.frame_placements(m64, oMi, [fid])[:, 0]
+    X0 = np.repeat(qs.numpy()[:, None, :], T, 1)
+    out = _gpu(m, fid, goal, start, X0, btr.TrajOptConfig(max_iter=30))
+    # the oracle starts from the float32-rounded inputs the kernel saw
+    X0r = X0.astype(np.float32).astype(np.float64)
+    ref = ot.solve(m64, X0r, fid, goal.astype(np.float32).astype(np.float64),
+                   start.astype(np.float32).astype(np.float64), ot.TrajSettings(max_iter=30))
+    conv = out.converged.cpu().numpy()
+    assert (conv == ref.converged).mean() >= 0.9, (conv, ref.converged)
+    both = conv & ref.converged
+    X = out.q.cpu().double().numpy()
+    assert np.abs(X[both] - ref.X[both]).max() <= 1e-4, np.abs(X[both] - ref.X[both]).max()
+    c = out.cost.cpu().double().numpy()
+    assert (np.abs(c[both] - ref.cost[both]) <= 1e-6 + 1e-4 * np.abs(ref.cost[both])).all()
+
+
+def test_trajopt_rejects_oversized_trees_and_bad_shapes():
+    m = syn.model_from_spec(syn.humanoid_spec())     # nv = 36 > BR_MAX_TRAJ_NV
     X0 = torch.zeros(2, 8, m.nq, device="cuda")
     with pytest.raises(Exception):
         btr.solve_trajopt_batched(m, 0, torch.zeros(2, 7, device="cuda"), X0)
