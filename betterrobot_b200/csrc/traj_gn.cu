@@ -69,13 +69,13 @@ struct TrajLayout {
   // ints / floats (in units of doubles)
   int parent, jtype, idxq, idxv, dofq, cjoint, ckind, axis, place, caxis, anc, lower, upper, misc;
   int total;
-  __host__ __device__ TrajLayout(int nj, int nq, int nv, int T) {
+  __host__ __device__ TrajLayout(int nj, int nq, int nv, int T, bool floating) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };  // 16-byte aligned
     x = take(T * nq); xn = take(T * nq); xref = take(T * nq); g = take(T * nv); delta = take(T * nv);
     // knot differences difference(x_t, x_{t+1}) and difference(xref_t, x_t) of the last
     // evaluated trajectory (floating-base trees; fixed-base trees subtract inline)
-    dd = take(T * nv); dr = take(T * nv);
+    dd = take(floating ? T * nv : 0); dr = take(floating ? T * nv : 0);
     // per-DOF interior bands (index p * nv + i, p = knot - 1): L[p][p-1], L[p][p-2], 1 / D[p];
     // solutions of P_i y = r, P_i u = h0, P_i w = hT
     bl1 = take(T * nv); bl2 = take(T * nv); bdi = take(T * nv);
@@ -134,7 +134,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, T = P.T, lane = threadIdx.x;
   const int64_t traj = blockIdx.x;
   if (traj >= P.n) return;
-  const TrajLayout L(nj, nq, nv, T);
+  const TrajLayout L(nj, nq, nv, T, kFloating);
   double* x = sm + L.x;
   double* xn = sm + L.xn;
   double* xref = sm + L.xref;
@@ -383,14 +383,20 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       const double a = kFloating ? c * (dd[e + nv] - dd[e]) : c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
       acc += a * a;
     }
-    for (int e = lane; e < nqT; e += kWarp) {                   // limits.py:56-62
-      const int i = e % nq;
-      const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
-      acc += wl * wl * (lo * lo + hi * hi);
-    }
-    for (int e = lane; e < n; e += kWarp) {                     // regularization.py:143-152
-      const double d = kFloating ? dr[e] : xs[e] - xref[e];
-      acc += wr * wr * d * d;
+    if (kFloating) {
+      for (int e = lane; e < nqT; e += kWarp) {                 // limits.py:56-62
+        const int i = e % nq;
+        const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
+        acc += wl * wl * (lo * lo + hi * hi);
+      }
+      for (int e = lane; e < n; e += kWarp) acc += wr * wr * dr[e] * dr[e];   // regularization.py:143-152
+    } else {                                                    // nq == nv: one pass for both
+      for (int e = lane; e < n; e += kWarp) {
+        const int i = e % nv;
+        const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
+        const double d = xs[e] - xref[e];
+        acc += wl * wl * (lo * lo + hi * hi) + wr * wr * d * d;
+      }
     }
     acc = warp_sum(acc);
     double pc = 0.0;
@@ -695,8 +701,7 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
                    (1 << BR_JOINT_TRANSLATION) | (1 << BR_JOINT_FREE_FLYER);
     if (tree->kinds == 0 || (tree->kinds & ~ok)) return BR_EINVAL;  // q + v kinds and free-flyers
   }
-  const bool floating = (tree->kinds >> BR_JOINT_FREE_FLYER) & 1;
-  if (!floating && tree->nq != tree->nv) return BR_EINVAL;
+  if (!((tree->kinds >> BR_JOINT_FREE_FLYER) & 1) && tree->nq != tree->nv) return BR_EINVAL;
   if (frame_id < 0 || frame_id >= tree->nframes) return BR_EINVAL;
   if (n_traj == 0) return BR_OK;
   if (!x0 || !goal || !x || !iters || !status || !cost) return BR_EINVAL;
@@ -709,7 +714,8 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
   p.n = n_traj;
   p.x0 = x0; p.xref = x_ref; p.goal = goal; p.start = start;
   p.x = x; p.iters = iters; p.status = status; p.cost = cost; p.goal_grad = goal_grad;
-  const TrajLayout L(tree->njoints, tree->nq, tree->nv, knots);
+  const bool floating = (tree->kinds >> BR_JOINT_FREE_FLYER) & 1;
+  const TrajLayout L(tree->njoints, tree->nq, tree->nv, knots, floating);
   const size_t bytes = (size_t)L.total * sizeof(double);
   const DeviceInfo& dev = device_info();
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
