@@ -125,16 +125,17 @@ __device__ __forceinline__ double fast_rsqrt(double x) {
 // boundary blocks decode the rest on the fly
 constexpr int kTrajPairRegs = 4;
 
-// kFloating: the tree has free-flyer joints (nq != nv): knot differences and the retraction
-// go through Model.difference / Model.integrate; otherwise they are q1 - q0 and q + v.
-template <bool kFloating>
+// kManifold: the tree has joints whose configuration is not their tangent coordinates
+// (free-flyer, spherical, planar, unbounded revolute): knot differences and the retraction go
+// through Model.difference / Model.integrate; otherwise they are q1 - q0 and q + v.
+template <bool kManifold>
 __global__ void traj_gn_kernel(const TrajParams P) {
   extern __shared__ __align__(16) double sm[];
   const br_tree_t& tree = P.tree;
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, T = P.T, lane = threadIdx.x;
   const int64_t traj = blockIdx.x;
   if (traj >= P.n) return;
-  const TrajLayout L(nj, nq, nv, T, kFloating);
+  const TrajLayout L(nj, nq, nv, T, kManifold);
   double* x = sm + L.x;
   double* xn = sm + L.xn;
   double* xref = sm + L.xref;
@@ -321,8 +322,10 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
   };
-  // floating-base trees: dd[t] = difference(xs_t, xs_{t+1}) (t < T-1) and dr[t] =
-  // difference(xref_t, xs_t) (model.py:176-190; free-flyer log(q_a^-1 q_b), free_flyer.py:53-57)
+  // dd[t] = difference(xs_t, xs_{t+1}) (t < T-1) and dr[t] = difference(xref_t, xs_t)
+  // (model.py:176-190): free-flyer log(q_a^-1 q_b) (free_flyer.py:53-57), spherical
+  // log(normalize(q_a^-1 q_b)) (spherical.py:58-62), angle differences of atan2 for the
+  // unbounded revolute and planar joints (revolute.py:233-237, planar.py:70-76)
   auto knot_differences = [&](const double* xs) {
     const int npair = 2 * T - 1;
     for (int e = lane; e < npair * nj; e += kWarp) {
@@ -346,14 +349,23 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         dse3_log(dcompose(dinverse(a), b), v, w);
         out[iv] = v.x; out[iv + 1] = v.y; out[iv + 2] = v.z;
         out[iv + 3] = w.x; out[iv + 4] = w.y; out[iv + 5] = w.z;
+      } else if (jt == BR_JOINT_SPHERICAL) {
+        const double3 w = dso3_log(dqnormalize(dqmul(dqconj(make_double4(qa[iq], qa[iq + 1], qa[iq + 2], qa[iq + 3])),
+                                                     make_double4(qb[iq], qb[iq + 1], qb[iq + 2], qb[iq + 3]))));
+        out[iv] = w.x; out[iv + 1] = w.y; out[iv + 2] = w.z;
+      } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
+        const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
+        if (k) { out[iv] = qb[iq] - qa[iq]; out[iv + 1] = qb[iq + 1] - qa[iq + 1]; }
+        out[iv + k] = atan2(qb[iq + k + 1], qb[iq + k]) - atan2(qa[iq + k + 1], qa[iq + k]);
       } else {
         for (int k = 0; k < nvj; ++k) out[iv + k] = qb[iq + k] - qa[iq + k];
       }
     }
     __syncwarp();
   };
-  // floating-base trees: xn_t = integrate(x_t, delta_t) per knot (model.py:160-174;
-  // free-flyer normalize(q . exp(v)), free_flyer.py:47-51)
+  // xn_t = integrate(x_t, delta_t) per knot (model.py:160-174): free-flyer normalize(q . exp(v))
+  // (free_flyer.py:47-51), spherical normalize(q . exp(w)) (spherical.py:52-56), unbounded
+  // revolute / planar angle atan2(s, c) + v as (cos, sin) (revolute.py:223-231, planar.py:61-68)
   auto retract_knots = [&]() {
     for (int e = lane; e < T * nj; e += kWarp) {
       const int t = e / nj, j = e - t * nj;
@@ -369,6 +381,17 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         b.q = dqnormalize(b.q);
         o[iq] = b.t.x; o[iq + 1] = b.t.y; o[iq + 2] = b.t.z;
         o[iq + 3] = b.q.x; o[iq + 4] = b.q.y; o[iq + 5] = b.q.z; o[iq + 6] = b.q.w;
+      } else if (jt == BR_JOINT_SPHERICAL) {
+        const double4 r = dqnormalize(dqmul(make_double4(q[iq], q[iq + 1], q[iq + 2], q[iq + 3]),
+                                            dse3_exp(d3(0.0, 0.0, 0.0), d3(dv[iv], dv[iv + 1], dv[iv + 2])).q));
+        o[iq] = r.x; o[iq + 1] = r.y; o[iq + 2] = r.z; o[iq + 3] = r.w;
+      } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
+        const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
+        if (k) { o[iq] = q[iq] + dv[iv]; o[iq + 1] = q[iq + 1] + dv[iv + 1]; }
+        double sn, cs;
+        sincos(atan2(q[iq + k + 1], q[iq + k]) + dv[iv + k], &sn, &cs);
+        o[iq + k] = cs;
+        o[iq + k + 1] = sn;
       } else {
         for (int k = 0; k < nvj; ++k) o[iq + k] = q[iq + k] + dv[iv + k];
       }
@@ -378,12 +401,12 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   auto cost_of = [&](const double* xs) -> double {
     double acc = 0.0;
     pose_terms(xs, false);
-    if (kFloating) knot_differences(xs);
+    if (kManifold) knot_differences(xs);
     for (int e = lane; e < (T - 2) * nv; e += kWarp) {          // smoothness.py:118-125
-      const double a = kFloating ? c * (dd[e + nv] - dd[e]) : c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
+      const double a = kManifold ? c * (dd[e + nv] - dd[e]) : c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
       acc += a * a;
     }
-    if (kFloating) {
+    if (kManifold) {
       for (int e = lane; e < nqT; e += kWarp) {                 // limits.py:56-62
         const int i = e % nq;
         const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
@@ -427,19 +450,19 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       // acceleration rows s = t, t-1, t-2 with coefficients +1, -2, +1 at knot t (the
       // identity-Jacobian blocks of smoothness.py:127-142)
       auto arow = [&](int s) {
-        return kFloating ? c * (dd[(s + 1) * nv + i] - dd[s * nv + i])
+        return kManifold ? c * (dd[(s + 1) * nv + i] - dd[s * nv + i])
                          : c * (x[(s + 2) * nv + i] - 2.0 * x[(s + 1) * nv + i] + x[s * nv + i]);
       };
       if (t <= T - 3) acc += c * arow(t);
       if (t - 1 >= 0 && t - 1 <= T - 3) acc += -2.0 * c * arow(t - 1);
       if (t - 2 >= 0) acc += c * arow(t - 2);
-      const int iq = kFloating ? dofq[i] : i;
+      const int iq = kManifold ? dofq[i] : i;
       if (iq >= 0) {
         const double xq = x[t * nq + iq];
         if (xq < (double)lower[iq]) acc -= wl * wl * ((double)lower[iq] - xq);
         if (xq > (double)upper[iq]) acc += wl * wl * (xq - (double)upper[iq]);
       }
-      acc += wr * wr * (kFloating ? dr[e] : x[e] - xref[e]);
+      acc += wr * wr * (kManifold ? dr[e] : x[e] - xref[e]);
       if (has_goal && t == T - 1)
         for (int r = 0; r < 6; ++r) acc += wg * wg * Jg[r * nv + i] * rg[r];
       if (has_start && t == 0)
@@ -460,7 +483,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     if (t - 1 >= 0 && t - 1 <= T - 3) a += 4.0;
     if (t - 2 >= 0) a += 1.0;
     double d = c2 * a + wr * wr + damp;
-    const int iq = kFloating ? dofq[i] : i;
+    const int iq = kManifold ? dofq[i] : i;
     if (iq >= 0) {
       const double xv = x[t * nq + iq];
       if (xv < (double)lower[iq]) d += wl * wl;
@@ -641,7 +664,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         __syncwarp();
       }
     }
-    if (kFloating) {                                               // Model.integrate per knot (trajopt.py:159-169)
+    if (kManifold) {                                               // Model.integrate per knot (trajopt.py:159-169)
       retract_knots();
     } else {
       for (int e = lane; e < n; e += kWarp) xn[e] = x[e] + delta[e];
@@ -697,11 +720,12 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
   if (!settings || n_traj < 0 || knots < 3) return BR_EINVAL;
   if (knots > BR_MAX_TRAJ_KNOTS || tree->nv > BR_MAX_TRAJ_NV) return BR_ETOOBIG;
   {
-    const int ok = (1 << BR_JOINT_FIXED) | (1 << BR_JOINT_REVOLUTE) | (1 << BR_JOINT_PRISMATIC) |
-                   (1 << BR_JOINT_TRANSLATION) | (1 << BR_JOINT_FREE_FLYER);
-    if (tree->kinds == 0 || (tree->kinds & ~ok)) return BR_EINVAL;  // q + v kinds and free-flyers
+    const int ok = (1 << (BR_JOINT_TRANSLATION + 1)) - 1;        // every kind of the tree table
+    if (tree->kinds == 0 || (tree->kinds & ~ok)) return BR_EINVAL;
   }
-  if (!((tree->kinds >> BR_JOINT_FREE_FLYER) & 1) && tree->nq != tree->nv) return BR_EINVAL;
+  const int manifold_kinds = (1 << BR_JOINT_FREE_FLYER) | (1 << BR_JOINT_SPHERICAL) | (1 << BR_JOINT_PLANAR) |
+                             (1 << BR_JOINT_REVOLUTE_UNBOUNDED);
+  if (!(tree->kinds & manifold_kinds) && tree->nq != tree->nv) return BR_EINVAL;
   if (frame_id < 0 || frame_id >= tree->nframes) return BR_EINVAL;
   if (n_traj == 0) return BR_OK;
   if (!x0 || !goal || !x || !iters || !status || !cost) return BR_EINVAL;
@@ -714,7 +738,7 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
   p.n = n_traj;
   p.x0 = x0; p.xref = x_ref; p.goal = goal; p.start = start;
   p.x = x; p.iters = iters; p.status = status; p.cost = cost; p.goal_grad = goal_grad;
-  const bool floating = (tree->kinds >> BR_JOINT_FREE_FLYER) & 1;
+  const bool floating = (tree->kinds & manifold_kinds) != 0;
   const TrajLayout L(tree->njoints, tree->nq, tree->nv, knots, floating);
   const size_t bytes = (size_t)L.total * sizeof(double);
   const DeviceInfo& dev = device_info();

@@ -222,7 +222,9 @@ def trajopt_endpoints(model: Model, n: int, seed: int, spread: float = 1.0):
     """Start and goal configurations (float64) for trajectory problems: start uniform in
     +-2.5 rad, goal = start + U(+-spread) per joint, both clamped to the joint limits.  A
     free-flyer base starts at a translation U(+-0.5) m with a uniform random orientation and
-    moves by U(+-0.2 spread) m and a rotation exp(U(+-0.3 spread)) composed on the right."""
+    moves by U(+-0.2 spread) m and a rotation exp(U(+-0.3 spread)) composed on the right;
+    spherical joints likewise in rotation; planar and unbounded joints start at a uniform
+    angle and turn by U(+-spread) (planar: translation as the free-flyer's in x, y)."""
     rng = np.random.default_rng(seed)
     lo = model.lower_pos_limit.double().numpy()
     hi = model.upper_pos_limit.double().numpy()
@@ -230,9 +232,27 @@ def trajopt_endpoints(model: Model, n: int, seed: int, spread: float = 1.0):
     q1 = np.clip(q0 + rng.uniform(-spread, spread, size=(n, model.nq)), lo, hi)
     q0 = np.clip(q0, lo, hi)
     for j, jm in enumerate(model.joint_models):
+        iq = model.idx_qs[j]
+        if jm.kind in ("spherical", "planar", "revolute_unbounded"):
+            if jm.kind == "spherical":          # unit quaternion, then a rotation exp(U(+-0.3 spread))
+                u = rng.normal(size=(n, 4))
+                q0[:, iq:iq + 4] = u / np.linalg.norm(u, axis=1, keepdims=True)
+                w = rng.uniform(-0.3 * spread, 0.3 * spread, size=(n, 3))
+                th = np.linalg.norm(w, axis=1, keepdims=True)
+                sh = np.where(th > 1e-12, np.sin(0.5 * th) / np.maximum(th, 1e-12), 0.5)
+                q1[:, iq:iq + 4] = _quat_mul_np(q0[:, iq:iq + 4], np.concatenate([sh * w, np.cos(0.5 * th)], 1))
+            else:                               # [x, y,] cos, sin of a uniform angle, moved by U(+-spread)
+                k = iq + (2 if jm.kind == "planar" else 0)
+                th0 = rng.uniform(-np.pi, np.pi, size=n)
+                th1 = th0 + rng.uniform(-spread, spread, size=n)
+                q0[:, k], q0[:, k + 1] = np.cos(th0), np.sin(th0)
+                q1[:, k], q1[:, k + 1] = np.cos(th1), np.sin(th1)
+                if jm.kind == "planar":
+                    q0[:, iq:iq + 2] = rng.uniform(-0.5, 0.5, size=(n, 2))
+                    q1[:, iq:iq + 2] = q0[:, iq:iq + 2] + rng.uniform(-0.2 * spread, 0.2 * spread, size=(n, 2))
+            continue
         if jm.kind != "free_flyer":
             continue
-        iq = model.idx_qs[j]
         q0[:, iq:iq + 3] = rng.uniform(-0.5, 0.5, size=(n, 3))
         u = rng.normal(size=(n, 4))
         q0[:, iq + 3:iq + 7] = u / np.linalg.norm(u, axis=1, keepdims=True)

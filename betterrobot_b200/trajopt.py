@@ -64,11 +64,10 @@ def solve_trajopt_batched(model, frame_id: int, goal: torch.Tensor, initial_q_tr
                           cfg: TrajOptConfig | None = None, want_goal_grad: bool = True) -> BatchTrajResult:
     """``initial_q_traj (N, T, nq)``, ``goal (N, 7)`` (and ``start (N, 7)``) float32 CUDA tensors."""
     bad = [jm.kind for jm in model.joint_models
-           if not (jm.kind in ("universe", "fixed", "translation", "free_flyer") or jm.kind.startswith("prismatic")
-                   or (jm.kind.startswith("revolute") and jm.kind != "revolute_unbounded"))]
+           if not (jm.kind in ("universe", "fixed", "translation", "free_flyer", "spherical", "planar")
+                   or jm.kind.startswith("prismatic") or jm.kind.startswith("revolute"))]
     if bad:
-        raise UnsupportedJointError(f"trajopt: the knot stack takes q + v joints and free-flyers; "
-                                    f"got {sorted(set(bad))}")
+        raise UnsupportedJointError(f"trajopt: no knot difference / retraction for joint kinds {sorted(set(bad))}")
     cfg = cfg or TrajOptConfig()
     if initial_q_traj.dim() != 3 or initial_q_traj.shape[-1] != model.nq:
         raise ShapeError(f"initial_q_traj must be (N, T, {model.nq}), got {tuple(initial_q_traj.shape)}")

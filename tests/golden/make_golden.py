@@ -21,7 +21,8 @@ and outputs in ``tests/golden/*.npz``:
                       (``tasks/ik.py:191-226``) but with the configs' damping.
 * ``adjoint.npz``   — pose loss ``sum_f w_f |log(T_f^-1 oMf(q))|^2`` and its autograd
                       gradient w.r.t. raw ``q`` (free-flyer quaternion included).
-* ``trajopt_floating.npz`` — the same ``solve_trajopt`` stack on a floating-base chain
+* ``trajopt_floating.npz``, ``trajopt_mixed.npz`` — the same ``solve_trajopt`` stack on a
+                      floating-base chain and on the robot with every multi-slot joint kind
                       (acceleration and reference residuals through ``Model.difference``).
 * ``adjoint_mixed.npz`` — the same on the robot with every multi-slot joint kind
                       (planar, translation, spherical, unbounded revolute).
@@ -304,7 +305,7 @@ def make_adjoint(spec, B, seed, out):
 
 
 def make_trajopt(spec, N, T, seed, out, dt=0.05, w_goal=1.0, w_start=1.0, w_accel=1e-2, w_limit=0.1,
-                 w_ref=1e-3, tol=1e-6, max_iter=30):
+                 w_ref=1e-3, tol=1e-6, max_iter=30, spread=1.0):
     """Reference solve_trajopt (knots, GaussNewton) on the config-4 stack, float64."""
     from better_robot.costs.stack import CostStack
     from better_robot.kinematics.forward import forward_kinematics
@@ -315,7 +316,7 @@ def make_trajopt(spec, N, T, seed, out, dt=0.05, w_goal=1.0, w_start=1.0, w_acce
 
     m = reference_model(spec)
     mine = syn.model_from_spec(spec, dtype=D)
-    q_start, q_goal = syn.trajopt_endpoints(mine, N, seed)
+    q_start, q_goal = syn.trajopt_endpoints(mine, N, seed, spread)
     fid = m.frame_id("ee")
     res = {"X": [], "iters": [], "converged": [], "residual": []}
     goals, starts = [], []
@@ -357,6 +358,9 @@ def main():
     if only == ["trajopt_floating"]:
         make_trajopt(syn.floating_chain_spec(), 3, 12, 43, os.path.join(HERE, "trajopt_floating.npz"))
         return
+    if only == ["trajopt_mixed"]:
+        make_trajopt(syn.mixed_spec(), 3, 12, 45, os.path.join(HERE, "trajopt_mixed.npz"), spread=0.3)
+        return
     make_lie(os.path.join(HERE, "lie.npz"))
     make_lie_ops(os.path.join(HERE, "lie_ops.npz"))
     chain, hum, dual = syn.chain_spec(), syn.humanoid_spec(), syn.dual_arm_spec()
@@ -381,6 +385,7 @@ def main():
     make_adjoint(syn.mixed_spec(), 8, 33, os.path.join(HERE, "adjoint_mixed.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
     make_trajopt(syn.floating_chain_spec(), 3, 12, 43, os.path.join(HERE, "trajopt_floating.npz"))
+    make_trajopt(syn.mixed_spec(), 3, 12, 45, os.path.join(HERE, "trajopt_mixed.npz"), spread=0.3)
 
 
 if __name__ == "__main__":

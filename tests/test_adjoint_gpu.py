@@ -129,12 +129,3 @@ def test_grad_output_scaling():
     q2 = q.detach().clone().requires_grad_(True)
     (g1,) = torch.autograd.grad(pose_loss(m, q2, fids, T, w).sum(), q2)
     torch.testing.assert_close(g, g1 * go[:, None], rtol=1e-6, atol=1e-6)
-
-
-def test_trajopt_rejects_multi_slot_kinds():
-    """Trajectory optimisation needs q + v joints (knot difference q1 - q0)."""
-    from betterrobot_b200.exceptions import UnsupportedJointError
-    from betterrobot_b200 import trajopt as btr
-    m = syn.model_from_spec(syn.mixed_spec())
-    with pytest.raises(UnsupportedJointError):
-        btr.solve_trajopt_batched(m, 0, torch.zeros(1, 7, device="cuda"), torch.zeros(1, 4, m.nq, device="cuda"))

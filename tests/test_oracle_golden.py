@@ -130,14 +130,17 @@ def test_known_answers_one_joint_arm():
     assert abs(oMi[2, 5] - math.sin(math.pi / 4)) < 1e-12 and abs(oMi[2, 6] - math.cos(math.pi / 4)) < 1e-12
 
 
-@pytest.mark.parametrize("fixture,spec", [("trajopt_chain7.npz", "chain7"), ("trajopt_floating.npz", "floating")])
+@pytest.mark.parametrize("fixture,spec", [("trajopt_chain7.npz", "chain7"), ("trajopt_floating.npz", "floating"),
+                                          ("trajopt_mixed.npz", "mixed")])
 def test_trajopt_matches_reference_solve_trajopt(fixture, spec):
     """GN trajectory optimisation (goal/start pose, acceleration, per-knot limits, reference
-    trajectory), on the fixed-base chain and on a floating-base chain (free-flyer knots)."""
+    trajectory), on the fixed-base chain, a floating-base chain (free-flyer knots) and the
+    robot with planar, translation, spherical and unbounded-revolute joints."""
     from oracle import trajopt as ot
     g = _load(fixture)
     T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
-    m = syn.model_from_spec(SPECS["chain7"] if spec == "chain7" else syn.floating_chain_spec(), dtype=torch.float64)
+    m = syn.model_from_spec({"chain7": SPECS["chain7"], "floating": syn.floating_chain_spec(),
+                             "mixed": syn.mixed_spec()}[spec], dtype=torch.float64)
     s = ot.TrajSettings(dt=dt, w_goal=wg, w_start=ws, w_accel=wa, w_limit=wl, w_ref=wr, tol=tol, max_iter=int(mi))
     X0 = np.repeat(g["q_start"][:, None, :], int(T), 1)
     fid = m.frame_id("ee")

@@ -49,13 +49,15 @@ def _gpu(m, fid, goal, start, X0, cfg):
                                      start=torch.from_numpy(start).float().cuda(), cfg=cfg)
 
 
-@pytest.mark.parametrize("fixture", ["trajopt_chain7.npz", "trajopt_floating.npz"])
+@pytest.mark.parametrize("fixture", ["trajopt_chain7.npz", "trajopt_floating.npz", "trajopt_mixed.npz"])
 def test_reference_solve_trajopt_golden(fixture):
-    """The reference's float64 solve_trajopt: the 7-DOF chain, and a floating-base chain whose
-    knots move by Model.integrate and whose acceleration uses Model.difference."""
+    """The reference's float64 solve_trajopt: the 7-DOF chain, a floating-base chain, and the
+    robot with planar, translation, spherical and unbounded-revolute joints (knots moved by
+    Model.integrate, acceleration and reference residuals through Model.difference)."""
     g = np.load(os.path.join(GOLDEN, fixture))
     T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
-    spec = syn.chain_spec() if fixture == "trajopt_chain7.npz" else syn.floating_chain_spec()
+    spec = {"trajopt_chain7.npz": syn.chain_spec(), "trajopt_floating.npz": syn.floating_chain_spec(),
+            "trajopt_mixed.npz": syn.mixed_spec()}[fixture]
     m = syn.model_from_spec(spec)
     m64 = syn.model_from_spec(spec, dtype=torch.float64)
     fid = m.frame_id("ee")
