@@ -67,9 +67,8 @@ extern "C" {
 typedef struct br_tree {
     int32_t njoints, nq, nv, nframes;
     int32_t rounds;           /* ceil(log2(max joint depth)): pointer-jumping rounds */
-    int32_t kinds;            /* bit k set if some joint has kind BR_JOINT_k; entry points
-                                 that support only some kinds (trajectory optimisation) reject
-                                 a tree whose mask names others; the FK adjoint and trajectory
+    int32_t kinds;            /* bit k set if some joint has kind BR_JOINT_k (the LM picks its
+                                 kernel variant from it); the FK adjoint and trajectory
                                  optimisation reject a mask of 0                              */
     int32_t dof_entries;      /* sum over tangent columns of (depth in the DOF tree + 1): the
                                  LM's J^T J storage; 0 = not given (dense nv (nv + 1) / 2) */
@@ -304,9 +303,9 @@ typedef struct br_traj_settings {
  * pentadiagonal interior, dense Schur complement on the end knots).  x0 / x_ref / x
  * are [n_traj, knots, nq] (x_ref NULL = x0), goal / start are [n_traj, 7] poses of
  * frame `frame_id` (start may be NULL).  goal_grad (NULL or [n_traj, 6]) receives
- * d(final cost)/d(eps) for the goal perturbed as T_goal * exp(eps).  Joints: fixed,
- * revolute, prismatic, translation and free-flyer (knot differences and the
- * retraction through Model.difference / Model.integrate); nv <= BR_MAX_TRAJ_NV.
+ * d(final cost)/d(eps) for the goal perturbed as T_goal * exp(eps).  Every joint kind
+ * (knot differences and the retraction through Model.difference / Model.integrate);
+ * nv <= BR_MAX_TRAJ_NV.
  * Replaces solve_trajopt with the knot parameterisation and its dense LM / GN
  * (src/better_robot/tasks/trajopt.py:84-230) on the goal / start / acceleration /
  * limit / reference-trajectory stack.
