@@ -276,7 +276,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   // both pose terms at xs: xi (double, into rg / rs); with want_J also
   // J = Jr^-1 blockdiag(R^T,R^T) J_lwa (6 x nv, into Jg / Js).  A term that is not in the
   // problem (weight 0 or no start pose) is evaluated but not stored.
-  auto pose_terms = [&](const double* xs, bool want_J) {
+  auto pose_terms = [&](const double* xs, bool want_J) __attribute__((always_inline)) {
     const int npass = halves ? 1 : 2;
     for (int pass = 0; pass < npass; ++pass) {
       const int h = halves ? (lane >> 4) : pass;
