@@ -1,5 +1,5 @@
-// traj_gn.cu — batched trajectory optimisation (Gauss-Newton / LM) with a
-// block-banded Cholesky, one warp per trajectory.
+// traj_gn.cu — batched trajectory optimisation (Gauss-Newton / LM), one warp per
+// trajectory, Newton step in nested-dissection order.
 //
 // Reference: solve_trajopt with knot parameterisation
 // (src/better_robot/tasks/trajopt.py:84-230) flattens a (T, nq) trajectory into one
@@ -7,9 +7,10 @@
 // dense Cholesky every iteration (448 x 448 for T = 64, nv = 7).  The stack here is
 //   goal  : PoseResidual at knot T-1        (TimeIndexedResidual, residuals/temporal.py:20-126)
 //   start : PoseResidual at knot 0          (optional)
-//   accel : (q_{s+2} - 2 q_{s+1} + q_s)/dt^2 (AccelerationResidual, residuals/smoothness.py:98-161)
+//   accel : (d_{s+1} - d_s)/dt^2, d_t = difference(q_t, q_{t+1}) (= q_{t+1} - q_t for q + v
+//           joints)                         (AccelerationResidual, residuals/smoothness.py:98-161)
 //   limits: JointPositionLimit at every knot (residuals/limits.py:56-86)
-//   ref   : q_t - q_ref_t                   (ReferenceTrajectoryResidual, residuals/regularization.py:133-152)
+//   ref   : difference(q_ref_t, q_t)        (ReferenceTrajectoryResidual, residuals/regularization.py:133-152)
 // each with a CostStack item weight.  In its J^T J + damp I every term except the
 // two pose terms acts on one DOF at a time: the acceleration rows couple knots
 // t, t+1, t+2 of the same DOF, limits / reference / damping are diagonal.  So H is
@@ -74,7 +75,7 @@ struct TrajLayout {
     auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };  // 16-byte aligned
     x = take(T * nq); xn = take(T * nq); xref = take(T * nq); g = take(T * nv); delta = take(T * nv);
     // knot differences difference(x_t, x_{t+1}) and difference(xref_t, x_t) of the last
-    // evaluated trajectory (floating-base trees; fixed-base trees subtract inline)
+    // evaluated trajectory (kManifold variant; the other subtracts inline)
     dd = take(floating ? T * nv : 0); dr = take(floating ? T * nv : 0);
     // per-DOF interior bands (index p * nv + i, p = knot - 1): L[p][p-1], L[p][p-2], 1 / D[p];
     // solutions of P_i y = r, P_i u = h0, P_i w = hT

@@ -1,4 +1,4 @@
-"""Batched kinematic trajectory optimisation on the sm_100a block-banded solver.
+"""Batched kinematic trajectory optimisation on the sm_100a nested-dissection solver.
 
 Counterpart of ``solve_trajopt`` with the knot parameterisation
 (``src/better_robot/tasks/trajopt.py:84-230``) for the cost stack
