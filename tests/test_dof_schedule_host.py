@@ -179,3 +179,17 @@ def test_schedule_rejects_bad_parents():
     assert lib.br_dof_schedule(bad.ctypes.data, 2, None, 0) < 0
     big = np.zeros(65, np.int32)
     assert lib.br_dof_schedule(big.ctypes.data, 65, None, 0) < 0
+
+
+def test_schedule_at_the_size_limit():
+    """A 62-DOF serial chain (64 joints with the universe and root) and a 64-DOF binary-ish tree."""
+    chain = np.arange(-1, 61, dtype=np.int32)                 # c's parent is c - 1
+    tree = np.array([-1] + [(c - 1) // 2 for c in range(1, 64)], np.int32)
+    rng = np.random.default_rng(5)
+    for dp in (chain, tree):
+        s = _schedule(dp)
+        A = _random_tree_matrix(dp, rng, n_terms=20)
+        g = rng.normal(size=len(dp))
+        x = _solve(s, dp, A, g, 1e-2)
+        ref = np.linalg.solve(A + 1e-2 * np.eye(len(dp)), -g)
+        assert np.abs(x - ref).max() <= 1e-8 * max(1.0, np.abs(ref).max())

@@ -136,6 +136,35 @@ def test_noisy_start_vs_oracle(robot, frames, rest, P, agree_min):
     assert abs(conv.mean() - ref.converged.mean()) <= 0.08, (conv.mean(), ref.converged.mean())
 
 
+@pytest.mark.parametrize("spec", [syn.chain_spec(seed=9, n=62, name="chain62"),
+                                  syn.floating_chain_spec(seed=9, n=58)], ids=["chain62", "floating58"])
+def test_size_limit_trees_vs_oracle(spec):
+    """Trees at the size limits: a 62-revolute chain (64 joints = BR_MAX_JOINTS) and a free-flyer
+    with 58 revolutes (nv = 64 = BR_MAX_NV).  FK + frame Jacobian against the oracle, and 16
+    noisy-start LM solves with the same verdicts and residuals."""
+    m, m64 = syn.model_from_spec(spec), syn.model_from_spec(spec, dtype=torch.float64)
+    fid = m.frame_id("ee")
+    P = 16
+    q_star = syn.random_q(m64, P, 70, rev_range=2.5, base_translation=1.0)
+    oMi, _ = K.forward_kinematics(m64, q_star.numpy())
+    targets = K.frame_placements(m64, oMi, [fid])
+    import betterrobot_b200 as br
+    T, J = br.frame_jacobians(m, q_star.float().cuda(), [fid])
+    Jref = K.frame_jacobian(m64, oMi, q_star.numpy(), fid, "local_world_aligned")
+    assert np.abs(T.cpu().double().numpy()[:, 0, :3] - targets[:, 0, :3]).max() <= 1e-4
+    assert np.abs(J.cpu().double().numpy()[:, 0] - Jref).max() <= 1e-4 * np.abs(Jref).max()
+    q0 = syn.noisy_start(m64, q_star, 0.3, 71)
+    s = oik.IKSettings(lam0=1e-3, factor=10.0, tol=1e-6, max_iter=100, rest_weight=0.0)
+    ref = oik.solve(m64, [fid], targets, q0.numpy(), s)
+    assert ref.converged.all()
+    out = bik.solve_ik_batched(m, [fid], torch.from_numpy(targets).float().cuda(), q0.float().cuda(),
+                               cost_cfg=bik.IKCostConfig(rest_weight=0.0),
+                               optimizer_cfg=bik.OptimizerConfig(max_iter=100, lam0=1e-3, factor=10.0),
+                               with_residual=True)
+    ok, conv, dres = _agreement(out, ref.converged, ref.residual)
+    assert ok.mean() >= 0.9, (conv.mean(), dres.max())
+
+
 def test_inconsistent_tree_tables_are_refused():
     """A class whose tree under-reports its DOF entries, or whose level schedule holds an offset
     outside the factor storage, is refused problem by problem (status flag BADTREE, x = x0)

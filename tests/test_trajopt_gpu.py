@@ -134,13 +134,12 @@ def test_goal_gradient_envelope_vs_resolved_cost():
     assert (rel[ok] <= 2e-2).all(), rel
 
 
-def test_floating_base_vs_oracle():
-    """Floating-base chain (free-flyer knots), 16 trajectories x 24 knots, against the float64 oracle."""
-    spec = syn.floating_chain_spec()
+def _vs_oracle(spec, N, T, seed):
+    """N trajectories of T knots on ``spec`` against the float64 oracle (same verdicts on >= 90%,
+    trajectories within 1e-4 and costs within 1e-6 + 1e-4 relative where both converged)."""
     m, m64 = syn.model_from_spec(spec), syn.model_from_spec(spec, dtype=torch.float64)
     fid = m.frame_id("ee")
-    N, T = 16, 24
-    qs, qg = syn.trajopt_endpoints(m64, N, 47, 0.5)
+    qs, qg = syn.trajopt_endpoints(m64, N, seed, 0.5)
     oMi, _ = K.forward_kinematics(m64, qg.numpy())
     goal = K.frame_placements(m64, oMi, [fid])[:, 0]
     oMi, _ = K.forward_kinematics(m64, qs.numpy())
@@ -154,10 +153,24 @@ def test_floating_base_vs_oracle():
     conv = out.converged.cpu().numpy()
     assert (conv == ref.converged).mean() >= 0.9, (conv, ref.converged)
     both = conv & ref.converged
+    assert both.any()
     X = out.q.cpu().double().numpy()
     assert np.abs(X[both] - ref.X[both]).max() <= 1e-4, np.abs(X[both] - ref.X[both]).max()
     c = out.cost.cpu().double().numpy()
     assert (np.abs(c[both] - ref.cost[both]) <= 1e-6 + 1e-4 * np.abs(ref.cost[both])).all()
+
+
+def test_floating_base_vs_oracle():
+    """Floating-base chain (free-flyer knots), 16 trajectories x 24 knots, against the float64 oracle."""
+    _vs_oracle(syn.floating_chain_spec(), 16, 24, 47)
+
+
+@pytest.mark.parametrize("spec,N,T", [(syn.chain_spec(seed=11, n=16, name="chain16"), 16, 16),
+                                      (syn.chain_spec(), 8, 128)], ids=["nv16", "knots128"])
+def test_size_limits_vs_oracle(spec, N, T):
+    """The trajectory limits: nv = 16 = BR_MAX_TRAJ_NV (18 joints: pose terms on the whole
+    warp, a 32 x 32 boundary system) and T = 128 = BR_MAX_TRAJ_KNOTS knots."""
+    _vs_oracle(spec, N, T, 53)
 
 
 def test_trajopt_rejects_oversized_trees_and_bad_shapes():
