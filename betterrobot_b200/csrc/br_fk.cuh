@@ -103,7 +103,7 @@ __device__ __forceinline__ DPose dlocal_transform(int jt, const DPose& P, const 
   if (jt == BR_JOINT_REVOLUTE || (kAllKinds && jt == BR_JOINT_REVOLUTE_UNBOUNDED)) {
     const double th = jt == BR_JOINT_REVOLUTE ? qv[0] : atan2(qv[1], qv[0]);
     double s, c;
-    sincos(0.5 * th, &s, &c);
+    sincospi(th * (0.5 / 3.141592653589793), &s, &c);  // sin, cos of th / 2 (no large-argument reduction path)
     L.q = dqmul(P.q, make_double4(s * axis4[0], s * axis4[1], s * axis4[2], c));
   } else if (jt == BR_JOINT_PRISMATIC) {
     L.t = dadd(P.t, dqrot(P.q, d3(qv[0] * axis4[0], qv[0] * axis4[1], qv[0] * axis4[2])));

@@ -381,8 +381,8 @@ __device__ __forceinline__ DPose dinverse(const DPose& a) {
   return r;
 }
 __device__ __forceinline__ double4 dqnormalize(double4 q) {
-  const double n = fmax(sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-8);
-  return make_double4(q.x / n, q.y / n, q.z / n, q.w / n);
+  const double r = 1.0 / fmax(sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-8);
+  return make_double4(q.x * r, q.y * r, q.z * r, q.w * r);
 }
 __device__ __forceinline__ double3 dso3_log(double4 q) {
   if (q.w < 0.0) q = make_double4(-q.x, -q.y, -q.z, -q.w);
@@ -397,17 +397,21 @@ __device__ __forceinline__ double3 dso3_log(double4 q) {
   return d3(factor * q.x, factor * q.y, factor * q.z);
 }
 __device__ __forceinline__ void dse3_log(const DPose& T, double3& v, double3& w) {
-  w = dso3_log(T.q);
+  // the rotation part as dso3_log: w = f q_xyz with f = 2 atan2(s, |q_w|) / s, s = |q_xyz|
+  double4 q = T.q;
+  if (q.w < 0.0) q = make_double4(-q.x, -q.y, -q.z, -q.w);
+  const double s2 = q.x * q.x + q.y * q.y + q.z * q.z;
+  const double s = sqrt(s2);
+  const double f = s2 < 1e-8 / 4.0 ? 2.0 + s2 * (2.0 / 3.0) : 2.0 * atan2(s, fmin(q.w, 1.0)) / s;
+  w = d3(f * q.x, f * q.y, f * q.z);
   const double th2 = ddot(w, w);
   double c;
   if (th2 < 1e-8) {
     c = 1.0 / 12.0 + th2 / 720.0;
   } else {
-    // c = 1/th^2 - cot(th/2) / (2 th); with th = 2 atan2(|q_xyz|, |q_w|) (dso3_log),
-    // cot(th/2) = |q_w| / |q_xyz| exactly: no trigonometric call
-    const double th = sqrt(th2);
-    const double s = sqrt(T.q.x * T.q.x + T.q.y * T.q.y + T.q.z * T.q.z);
-    c = 1.0 / th2 - (fabs(T.q.w) / s) / (2.0 * th);
+    // c = 1/th^2 - cot(th/2) / (2 th) with th = f s and cot(th/2) = |q_w| / s exactly
+    // (no trigonometric call): c = (1 - f |q_w| / 2) / th^2
+    c = fma(-0.5 * f, q.w, 1.0) / th2;
   }
   const double3 wt = dcross(w, T.t);
   v = dadd(dadd(T.t, dscale(wt, -0.5)), dscale(dcross(w, wt), c));

@@ -513,22 +513,21 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     }
     for (int t = tl; t < nt; t += T) {
       const double* e = xi + 8 * t;
-      JrInv J;
+      float* o = jri + 16 * t;
       if (!kGeneral || tkind[t] == BR_TARGET_POSE) {                   // SE3 Jr^-1(xi), tangents.py:204-207
-        J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
+        const JrInv J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
+        o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
+        for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
       } else {  // orientation: SO3 Jr^-1(r) (tangents.py:122-145) as the angular block, no coupling;
                 // position: identity (its rows are replaced by J_lwa's linear rows)
         const bool ori = tkind[t] == BR_TARGET_ORIENTATION;
-        J.w = f3((float)e[3], (float)e[4], (float)e[5]);
-        J.b0 = 1.f;
-        J.b1 = ori ? 0.5f : 0.f;
-        J.b2 = ori ? vinv_coeff(dot(J.w, J.w)) : 0.f;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) J.B[k] = 0.f;
+        const float3 w = f3((float)e[3], (float)e[4], (float)e[5]);
+        o[0] = w.x; o[1] = w.y; o[2] = w.z;
+        o[3] = 1.f;
+        o[4] = ori ? 0.5f : 0.f;
+        o[5] = ori ? vinv_coeff(dot(w, w)) : 0.f;
+        for (int k = 0; k < 9; ++k) o[6 + k] = 0.f;
       }
-      float* o = jri + 16 * t;
-      o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
-      for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
     }
     for (int e = tl; e < nL; e += T) jtj[e] = 0.f;
     tm.sync();
@@ -617,13 +616,13 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           const int iq = idxq[j] + (c - idxv[j]);
           if (q[iq] < (double)lower[iq]) {
             const double d = (double)lower[iq] - q[iq];
-            const float w = irls_weight(S.kernel, kc, wld * wld * d * d);
+            const float w = irls ? irls_weight(S.kernel, kc, wld * wld * d * d) : 1.f;
             dg += wl * wl * w;
             gc -= wl * wl * w * (float)d;
           }
           if (q[iq] > (double)upper[iq]) {
             const double d = q[iq] - (double)upper[iq];
-            const float w = irls_weight(S.kernel, kc, wld * wld * d * d);
+            const float w = irls ? irls_weight(S.kernel, kc, wld * wld * d * d) : 1.f;
             dg += wl * wl * w;
             gc += wl * wl * w * (float)d;
           }
