@@ -401,18 +401,25 @@ __device__ __forceinline__ void dse3_log(const DPose& T, double3& v, double3& w)
   double4 q = T.q;
   if (q.w < 0.0) q = make_double4(-q.x, -q.y, -q.z, -q.w);
   const double s2 = q.x * q.x + q.y * q.y + q.z * q.z;
-  const double s = sqrt(s2);
-  const double f = s2 < 1e-8 / 4.0 ? 2.0 + s2 * (2.0 / 3.0) : 2.0 * atan2(s, fmin(q.w, 1.0)) / s;
+  // c = 1/th^2 - cot(th/2) / (2 th) with th = 2a, a = atan2(s, |q_w|), s = |q_xyz|, and
+  // cot(th/2) = |q_w| / s exactly (no trigonometric call): c = (1 - a |q_w| / s) / (4 a^2);
+  // f = 2a / s.  One division: r = 1 / (a s) gives 1/s = a r and 1/a = s r.
+  double f, c = 0.0;
+  const bool small = s2 < 1e-8 / 4.0;
+  if (small) {
+    f = 2.0 + s2 * (2.0 / 3.0);
+  } else {
+    const double s = sqrt(s2);
+    const double a = atan2(s, fmin(q.w, 1.0));
+    const double r = 1.0 / (a * s);
+    const double ar = a * a * r;  // a / s
+    const double sr = s * r;      // 1 / a
+    f = 2.0 * ar;
+    c = fma(-ar, q.w, 1.0) * (0.25 * sr * sr);
+  }
   w = d3(f * q.x, f * q.y, f * q.z);
   const double th2 = ddot(w, w);
-  double c;
-  if (th2 < 1e-8) {
-    c = 1.0 / 12.0 + th2 / 720.0;
-  } else {
-    // c = 1/th^2 - cot(th/2) / (2 th) with th = f s and cot(th/2) = |q_w| / s exactly
-    // (no trigonometric call): c = (1 - f |q_w| / 2) / th^2
-    c = fma(-0.5 * f, q.w, 1.0) / th2;
-  }
+  if (small || th2 < 1e-8) c = 1.0 / 12.0 + th2 / 720.0;
   const double3 wt = dcross(w, T.t);
   v = dadd(dadd(T.t, dscale(wt, -0.5)), dscale(dcross(w, wt), c));
 }

@@ -242,7 +242,9 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
   // packed lower-triangle pair p -> (a, b), b <= a, p = tri(a) + b
   auto decode_pair = [](int p) {
-    int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+    float r;  // approximate square root: the two corrections below make the decode exact
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(8.f * p + 1.f));
+    int a = (int)((r - 1.f) * 0.5f);
     if (tri(a + 1) <= p) ++a;
     if (tri(a) > p) --a;
     return a | ((p - tri(a)) << 8);
