@@ -381,7 +381,8 @@ __device__ __forceinline__ DPose dinverse(const DPose& a) {
   return r;
 }
 __device__ __forceinline__ double4 dqnormalize(double4 q) {
-  const double r = 1.0 / fmax(sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-8);
+  const double n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+  const double r = n2 > 1e-16 ? rsqrt(n2) : 1e8;  // 1 / max(|q|, 1e-8)
   return make_double4(q.x * r, q.y * r, q.z * r, q.w * r);
 }
 __device__ __forceinline__ double3 dso3_log(double4 q) {
