@@ -251,6 +251,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   };
 
   // ---- load the tree table and the problem -------------------------------
+#pragma unroll 1
   for (int j = tl; j < nj; j += T) {
     parent[j] = tree.parent[j];
     jtype[j] = tree.jtype[j];
@@ -258,12 +259,14 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     idxv[j] = tree.idx_v[j];
     support[j] = tree.support[j];
   }
+#pragma unroll 1
   for (int c = tl; c < nv; c += T) {
     cjoint[c] = tree.col_joint[c];
     ckind[c] = tree.col_kind[c];
     *reinterpret_cast<float4*>(caxis + 4 * c) = *reinterpret_cast<const float4*>(tree.col_axis + 4 * c);
   }
   const int64_t qoff = P.b.q_offset[prob];
+#pragma unroll 1
   for (int i = tl; i < nq; i += T) {
     lower[i] = tree.lower[i];
     upper[i] = tree.upper[i];
@@ -311,6 +314,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       if (dc > As) {
         bad = true;  // deeper than the tree's dof_depth claims: the ancestor table would overflow
       } else {
+#pragma unroll 1
         for (int a = 0; a + 1 < dc; ++a) ancd[c * As + a] = ancd[pc * As + a];
         if (pc >= 0) ancd[c * As + dc - 1] = (unsigned char)pc;
       }
@@ -330,6 +334,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     const int nlev = (int)sched[0], ntask = (int)sched[1], nextra = (int)sched[2];
     bool bad = nlev < 0 || nlev > nv || ntask < 0 || nextra < 0 || (int)sched[3] != misc[1];
     if (!bad) {
+#pragma unroll 1
       for (int l = tl; l <= nlev; l += T) {
         const int s0 = (int)sched[4 + l];
         bad |= (l == 0 && s0 != 0) || (l == nlev && s0 != ntask) || s0 < 0 || s0 > ntask ||
@@ -343,6 +348,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         bad |= (int)(t4.x & 0xffff) >= lim || (int)(t4.y & 0xffff) >= lim || (int)(t4.y >> 16) >= lim ||
                (int)(t4.z & 0xffff) >= nv || (int)(t4.z >> 16) + (int)(t4.x >> 16) > nextra || (int)t4.w > nv;
       }
+#pragma unroll 1
       for (int e = tl; e < nextra; e += T) {
         const uint2 e2 = ex[e];
         bad |= (int)(e2.x & 0xffff) >= lim || (int)(e2.x >> 16) >= lim || (int)e2.y >= nv;
@@ -371,6 +377,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   for (int t = 0; t < nt; ++t) {
     const unsigned long long sp = support[fparent[t]];
     int base = 0;
+#pragma unroll 1
     for (int c0 = 0; c0 < nv; c0 += T) {
       const int c = c0 + tl;
       const bool in = c < nv && ((sp >> cjoint[c]) & 1ull);
@@ -491,6 +498,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       }
     }
     if (use_limits) {                                                // limits.py:56-62
+#pragma unroll 1
       for (int i = tl; i < nq; i += T) {
         const double lo = fmax((double)lower[i] - q[i], 0.0), hi = fmax(q[i] - (double)upper[i], 0.0);
         acc += wld * wld * (lo * lo + hi * hi);
@@ -531,6 +539,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         for (int k = 0; k < 9; ++k) o[6 + k] = 0.f;
       }
     }
+#pragma unroll 1
     for (int e = tl; e < nL; e += T) jtj[e] = 0.f;
     tm.sync();
     float* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
@@ -653,6 +662,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   auto solve = [&](float damp) -> bool {
     float* Lm = work;
     float* z = work + nL;
+#pragma unroll 1
     for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
     // pivots of the leaves (final already); a non-leaf's is stored by the task that
     // finalises its diagonal (the schedule's flag)
@@ -716,6 +726,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       ror[r] = in ? rowoff[i] : 0;
     }
     const int ndl = misc[1];
+#pragma unroll 1
     for (int dl = 0; dl < ndl; ++dl) {
 #pragma unroll
       for (int r = 0; r < R; ++r)
@@ -767,8 +778,10 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         }
         DPose n = dcompose(a, inc);
         n.q = dqnormalize(n.q);
-        const double v7[7] = {n.t.x, n.t.y, n.t.z, n.q.x, n.q.y, n.q.z, n.q.w};
-        for (int k = 0; k < 7; ++k) xn[iq + k] = fmin(fmax(v7[k], (double)lower[iq + k]), (double)upper[iq + k]);
+        xn[iq] = n.t.x; xn[iq + 1] = n.t.y; xn[iq + 2] = n.t.z;
+        xn[iq + 3] = n.q.x; xn[iq + 4] = n.q.y; xn[iq + 5] = n.q.z; xn[iq + 6] = n.q.w;
+#pragma unroll 1
+        for (int k = 0; k < 7; ++k) clampq(k, xn[iq + k]);
       }
     }
     tm.sync();
@@ -802,6 +815,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       ++it;
       if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
       if (gn || cn < cost) {
+#pragma unroll 1
         for (int i = tl; i < nq; i += T) x[i] = xn[i];
         tm.sync();
         cost = cn;
@@ -837,6 +851,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       extra = k == 0 ? 1e-6f : extra * 10.f;
     }
     if (!ok) {
+#pragma unroll 1
       for (int i = tl; i < nv; i += T) delta[i] = 0.f;
       tm.sync();
     }
@@ -844,12 +859,14 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     xe = xn;
   }
   // ---- results ------------------------------------------------------------
+#pragma unroll 1
   for (int i = tl; i < nq; i += T) P.r.x[qoff + i] = (float)x[i];
   if (want_residual) {
     // stacked residual at the returned x, CostStack order (stack.py:104-117); the residual
     // buffers hold x's values (last pass above)
     float* out = P.r.residual + P.b.r_offset[prob];
     int o = 0;  // rows of the targets: 6 per pose, 3 per position or orientation target
+#pragma unroll 1
     for (int t = 0; t < nt; ++t) {
       const double* e = xi + 8 * t;
       const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
@@ -865,6 +882,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       o += kind == BR_TARGET_POSE ? 6 : 3;
     }
     if (use_limits) {  // the limit and rest rows keep their place when their weight is 0
+#pragma unroll 1
       for (int i = tl; i < nq; i += T) {
         out[o + i] = (float)(wld * fmax((double)lower[i] - x[i], 0.0));
         out[o + nq + i] = (float)(wld * fmax(x[i] - (double)upper[i], 0.0));
@@ -872,6 +890,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     }
     o += 2 * nq;
     if (use_rest)
+#pragma unroll 1
       for (int c = tl; c < nv; c += T) out[o + c] = (float)(wrd * dr[c]);
   }
   if (tl == 0) {
