@@ -257,16 +257,19 @@ def bench_ik(steps: int, warmup: int, seed: int, pinned=None):
     for _ in range(warmup):
         pk.solve(settings)
     torch.cuda.synchronize()
-    times = []
+    # every step is enqueued without a host wait (the host runs ahead of the device, so the
+    # device never idles inside a timed step waiting for the next launch); one synchronize
+    # after the last step, then the per-step event pairs are read
+    evs = []
     for _ in range(steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         pk.solve(settings)
         e1.record(stream)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
-    ms = float(np.mean(times))
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
     reached = gpu_reach(wl, [pk.q_of(c).clone() for c in range(len(wl))])
     conv = int(((pk.status & 0xFF) == 0).sum())
     iters = pk.iters.float()
@@ -288,28 +291,29 @@ def bench_ik(steps: int, warmup: int, seed: int, pinned=None):
     for _ in range(warmup):
         e2e_step()
     torch.cuda.synchronize()
-    et = []
+    evs = []
     for _ in range(steps):
         flush.fill_(1.0)
-        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         e2e_step()
         e1.record(stream)
-        torch.cuda.synchronize()
-        et.append(e0.elapsed_time(e1))
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    et = [a.elapsed_time(b) for a, b in evs]
     # the same solve replayed from a CUDA graph
     g = pk.capture(settings)
     torch.cuda.synchronize()
-    gt = []
+    evs = []
     for _ in range(steps):
         flush.fill_(1.0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         g.replay()
         e1.record(stream)
-        torch.cuda.synchronize()
-        gt.append(e0.elapsed_time(e1))
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    gt = [a.elapsed_time(b) for a, b in evs]
     return {"ms": ms, "reached": reached, "converged": conv, "problems": pk.P, "iters_mean": float(iters.mean()),
             "e2e_ms": float(np.mean(et)), "h2d": h2d, "d2h": d2h, "launches": steps, "wl": wl,
             "graph_ms": float(np.mean(gt)), "team_sizes": teams, "warps_per_cta": warps}
