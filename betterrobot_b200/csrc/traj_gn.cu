@@ -95,6 +95,18 @@ struct TrajLayout {
   }
 };
 
+// floor(e / d) by a multiply: e * ceil(2^32 / d) >> 32 is exact for 0 <= e < 2^16 and
+// 1 <= d <= 128 (the error term e (ceil(2^32/d) d - 2^32) / (d 2^32) stays below 1/d), which
+// covers every flattened (knot, joint / DOF / slot) index of this kernel.  An integer
+// division by a runtime divisor is a ~20-instruction dependent sequence.
+struct FastDiv {
+  unsigned long long m;
+  int d;
+  __device__ explicit FastDiv(int d_) : m((0x100000000ull + (unsigned long long)d_ - 1ull) / (unsigned long long)d_), d(d_) {}
+  __device__ __forceinline__ int div(int e) const { return (int)(((unsigned long long)e * m) >> 32); }
+  __device__ __forceinline__ int mod(int e) const { return e - div(e) * d; }
+};
+
 __device__ __forceinline__ DPose ldd8(const double* p) {
   return DPose{d3(p[0], p[1], p[2]), make_double4(p[4], p[5], p[6], p[7])};
 }
@@ -182,6 +194,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   const bool has_start = P.start != nullptr && S.w_start > 0.f;
   const bool has_goal = S.w_goal > 0.f;
   const int n = T * nv, nqT = T * nq;
+  const FastDiv divj(nj > 0 ? nj : 1), divv(nv > 0 ? nv : 1), divq(nq > 0 ? nq : 1);
 
   for (int j = lane; j < nj; j += kWarp) {
     parent[j] = tree.parent[j];
@@ -330,7 +343,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   auto knot_differences = [&](const double* xs) {
     const int npair = 2 * T - 1;
     for (int e = lane; e < npair * nj; e += kWarp) {
-      const int pi = e / nj, j = e - pi * nj;
+      const int pi = divj.div(e), j = e - pi * nj;
       const int jt = jtype[j], nvj = joint_nv(jt);
       if (nvj == 0) continue;
       const double* qa;
@@ -369,7 +382,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   // revolute / planar angle atan2(s, c) + v as (cos, sin) (revolute.py:223-231, planar.py:61-68)
   auto retract_knots = [&]() {
     for (int e = lane; e < T * nj; e += kWarp) {
-      const int t = e / nj, j = e - t * nj;
+      const int t = divj.div(e), j = e - t * nj;
       const int jt = jtype[j], nvj = joint_nv(jt);
       if (nvj == 0) continue;
       const int iq = idxq[j], iv = idxv[j];
@@ -409,14 +422,14 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     if (kManifold) {
       for (int e = lane; e < nqT; e += kWarp) {                 // limits.py:56-62
-        const int i = e % nq;
+        const int i = divq.mod(e);
         const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
         acc += wl * wl * (lo * lo + hi * hi);
       }
       for (int e = lane; e < n; e += kWarp) acc += wr * wr * dr[e] * dr[e];   // regularization.py:143-152
     } else {                                                    // nq == nv: one pass for both
       for (int e = lane; e < n; e += kWarp) {
-        const int i = e % nv;
+        const int i = divv.mod(e);
         const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
         const double d = xs[e] - xref[e];
         acc += wl * wl * (lo * lo + hi * hi) + wr * wr * d * d;
@@ -435,7 +448,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   auto build = [&]() -> double {
     pose_terms(x, true);
     for (int e = lane; e < nv * nv; e += kWarp) {
-      const int i = e / nv, j = e - i * nv;
+      const int i = divv.div(e), j = e - i * nv;
       double a = 0.0, b = 0.0;
       for (int r = 0; r < 6; ++r) {
         if (has_goal) a += Jg[r * nv + i] * Jg[r * nv + j];
@@ -446,7 +459,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     double gg = 0.0;
     for (int e = lane; e < n; e += kWarp) {
-      const int t = e / nv, i = e - t * nv;
+      const int t = divv.div(e), i = e - t * nv;
       double acc = 0.0;
       // acceleration rows s = t, t-1, t-2 with coefficients +1, -2, +1 at knot t (the
       // identity-Jacobian blocks of smoothness.py:127-142)
@@ -505,7 +518,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     // interior diagonals H[(p+1, i), (p+1, i)] by all lanes first (vy is free until the
     // forward solve); the off-diagonal H[(p+1), (p)] of the interior is -4 c2
     for (int e = lane; e < m * nv; e += kWarp) {
-      const int pp = e / nv;
+      const int pp = divv.div(e);
       vy[e] = hdiag(pp + 1, e - pp * nv, damp);
     }
     __syncwarp();
@@ -637,7 +650,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     __syncwarp();
     // interior: y - u z(knot 0) - w z(knot T-1)
     for (int e = lane; e < m * nv; e += kWarp) {
-      const int i = e % nv;
+      const int i = divv.mod(e);
       delta[nv + e] = vy[e] - vu[e] * delta[i] - vw[e] * delta[(T - 1) * nv + i];
     }
     __syncwarp();
