@@ -55,6 +55,18 @@ struct DeviceInfo {
 };
 
 // Cached per current device.
+// floor(e / d) by a multiply: e * ceil(2^32 / d) >> 32 is exact for 0 <= e < 2^16 and
+// 1 <= d <= 128 (the error term e (ceil(2^32/d) d - 2^32) / (d 2^32) stays below 1/d), which
+// covers the flattened (item, slot) indices the kernels split.  An integer
+// division by a runtime divisor is a ~20-instruction dependent sequence.
+struct FastDiv {
+  unsigned long long m;
+  int d;
+  __device__ explicit FastDiv(int d_) : m((0x100000000ull + (unsigned long long)d_ - 1ull) / (unsigned long long)d_), d(d_) {}
+  __device__ __forceinline__ int div(int e) const { return (int)(((unsigned long long)e * m) >> 32); }
+  __device__ __forceinline__ int mod(int e) const { return e - div(e) * d; }
+};
+
 const DeviceInfo& device_info();
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }

@@ -95,18 +95,6 @@ struct TrajLayout {
   }
 };
 
-// floor(e / d) by a multiply: e * ceil(2^32 / d) >> 32 is exact for 0 <= e < 2^16 and
-// 1 <= d <= 128 (the error term e (ceil(2^32/d) d - 2^32) / (d 2^32) stays below 1/d), which
-// covers every flattened (knot, joint / DOF / slot) index of this kernel.  An integer
-// division by a runtime divisor is a ~20-instruction dependent sequence.
-struct FastDiv {
-  unsigned long long m;
-  int d;
-  __device__ explicit FastDiv(int d_) : m((0x100000000ull + (unsigned long long)d_ - 1ull) / (unsigned long long)d_), d(d_) {}
-  __device__ __forceinline__ int div(int e) const { return (int)(((unsigned long long)e * m) >> 32); }
-  __device__ __forceinline__ int mod(int e) const { return e - div(e) * d; }
-};
-
 __device__ __forceinline__ DPose ldd8(const double* p) {
   return DPose{d3(p[0], p[1], p[2]), make_double4(p[4], p[5], p[6], p[7])};
 }
