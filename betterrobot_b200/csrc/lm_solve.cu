@@ -67,7 +67,9 @@ struct TeamLayout {
   int total;
   // ent / dep: the tree's DOF entry count and depth bound (br_tree_t.dof_entries /
   // dof_depth), 0 for the dense bounds.
-  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T, int ent = 0, int dep = 0) {
+  // rounds: the tree's pointer-jumping FK rounds (br_tree_t.rounds), which decide the
+  // pose buffer FK returns.
+  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T, int ent, int dep, int rounds) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += round4(n); return r; };
     parent = take(nj); jtype = take(nj); idxq = take(nj); idxv = take(nj);
@@ -88,8 +90,11 @@ struct TeamLayout {
     n_ent = (ent > 0 && ent < ntri) ? ent : ntri;
     anc_stride = (dep > 0 && dep < nv) ? dep : (nv > 0 ? nv : 1);
     jtj = take(n_ent);                         // J^T J, one row per DOF over its ancestors
-    // one target's J columns (build) / the factor and its right-hand-side slots (solve)
-    work = take(6 * nv > n_ent + nv ? 6 * nv : n_ent + nv);
+    // one target's J columns (build) / the factor and its right-hand-side slots (solve):
+    // in the pose buffer that FK does not return (poseA after an odd number of rounds, else
+    // poseB), dead while the normal equations are built and solved, when it is large enough
+    const int wneed = 6 * nv > n_ent + nv ? 6 * nv : n_ent + nv;
+    work = wneed <= 14 * nj ? ((rounds & 1) ? poseA : poseB) : take(wneed);
     misc = take(8);
     amask = take(2 * nv);                      // uint64 strict ancestors of each DOF
     dpar = take((nv + 3) / 4);                 // int8 parent DOF (-1 at a root)
@@ -191,7 +196,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
                               const uint32_t*& sched_ok) {
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
   const int K = P.b.max_targets;
-  const TeamLayout L(nj, nq, nv, K, T, tree.dof_entries, tree.dof_depth);
+  const TeamLayout L(nj, nq, nv, K, T, tree.dof_entries, tree.dof_depth, tree.rounds);
   int* parent = reinterpret_cast<int*>(sm + L.parent);
   int* jtype = reinterpret_cast<int*>(sm + L.jtype);
   int* idxq = reinterpret_cast<int*>(sm + L.idxq);
@@ -909,7 +914,7 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
   tm.tl = lane % T;
   tm.mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (team * T));
   const br_tree_t& tree = P.trees[cls];
-  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T, tree.dof_entries, tree.dof_depth);
+  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T, tree.dof_entries, tree.dof_depth, tree.rounds);
   if (team < count) {
     const int prob = P.b.order[first + team];
     solve_problem<T, kGeneral>(P, tree, prob, wsm + team * L.total, tm, sched_ok);
@@ -944,7 +949,7 @@ using namespace br;
 extern "C" int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets) {
   if (!tree || max_targets < 0) return BR_EINVAL;
   const int T = kLmTeam;
-  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T, tree->dof_entries, tree->dof_depth).total;
+  return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T, tree->dof_entries, tree->dof_depth, tree->rounds).total;
 }
 
 extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
@@ -977,7 +982,7 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const br_tree_t& tc = b.trees[c];
-    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth).total;
+    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth, tc.rounds).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;
@@ -1090,7 +1095,7 @@ extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_setti
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const br_tree_t& tc = b.trees[c];
-    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth).total;
+    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth, tc.rounds).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;
