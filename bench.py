@@ -195,6 +195,32 @@ def shard_seed(rank: int) -> int:
     return 7 + 1000 * rank
 
 
+def launch_replicas(cmd: list[str], n: int, timeout_s: float = 3600.0) -> int:
+    """Run ``cmd`` as ``n`` ranks on this node (what ``torchrun --nproc-per-node n`` does for this
+    script): rank i gets RANK = LOCAL_RANK = i, WORLD_SIZE = n and a rendezvous on 127.0.0.1.
+    Rank 0 writes to this process's stdout; the other ranks' stdout is dropped (they print
+    nothing).  Returns the first non-zero exit code, else 0."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen(cmd, env=env, stdout=None if r == 0 else subprocess.DEVNULL))
+    deadline = time.time() + timeout_s
+    rc = 0
+    for p in procs:
+        try:
+            code = p.wait(timeout=max(1.0, deadline - time.time()))
+        except subprocess.TimeoutExpired:
+            p.kill()
+            code = p.wait()
+        rc = rc or code
+    return rc
+
+
 def dist_setup():
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -205,7 +231,8 @@ def dist_setup():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -575,6 +602,9 @@ def main():
                     help="comma-separated lanes per problem for humanoid,dual_arm,chain7 (skips the autotuner)")
     ap.add_argument("--ik-warps", type=int, default=4, help="warps per CTA with --ik-teams")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not started by torchrun: launch the N replicas here, one process per GPU
+        sys.exit(launch_replicas([sys.executable, os.path.abspath(__file__), *sys.argv[1:]], args.gpus))
     warmup = max(args.warmup, 3)
     metric = "batched LM-IK solves/s reaching 1e-4 m and 1e-4 rad pose error"
     config = {"workload": "uneven batched IK: 8192 problems (40% chain7 7-DOF, 30% dual_arm 14-DOF, 30% humanoid "

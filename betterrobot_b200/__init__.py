@@ -11,6 +11,7 @@ uneven-batch LM) and ``pose_loss`` (FK pose loss with a hand-written adjoint).
 from .data import Data, KinematicsLevel
 from .exceptions import (BackendNotAvailableError, BetterRobotError, DeviceMismatchError, DtypeMismatchError,
                          KernelError, QuaternionNormError, ShapeError, StaleCacheError, UnsupportedJointError)
+from .ik import BatchIKResult, IKCostConfig, IKResult, OptimizerConfig, PackedIK, solve_ik, solve_ik_batched
 from .kinematics import (compute_joint_jacobians, forward_kinematics, frame_jacobians, get_frame_jacobian,
                          get_joint_jacobian, update_frame_placements)
 from .model import Frame, JointModel, Model, build_model
@@ -19,6 +20,7 @@ __all__ = [
     "Data", "KinematicsLevel", "Model", "Frame", "JointModel", "build_model",
     "forward_kinematics", "update_frame_placements", "compute_joint_jacobians", "get_joint_jacobian",
     "get_frame_jacobian", "frame_jacobians",
+    "solve_ik", "IKCostConfig", "OptimizerConfig", "IKResult", "solve_ik_batched", "PackedIK", "BatchIKResult",
     "BetterRobotError", "BackendNotAvailableError", "DeviceMismatchError", "DtypeMismatchError", "KernelError",
     "QuaternionNormError", "ShapeError", "StaleCacheError", "UnsupportedJointError",
 ]

@@ -118,7 +118,7 @@ def call(name: str, *args) -> None:
     st = getattr(load(), name)(*args)
     if st != 0:
         msg = STATUS.get(st, f"CUDA error {st}")
-        raise KernelError(f"{name} returned {st} ({msg})")
+        raise KernelError(f"{name} returned {st} ({msg})", st)
 
 
 def require_cuda(t) -> None:

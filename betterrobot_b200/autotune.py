@@ -13,6 +13,9 @@ import itertools
 
 import torch
 
+from .exceptions import KernelError
+
+BR_ETOOBIG = -2  # include/br_b200.h: a launch shape above the library limit
 _CACHE: dict = {}
 
 
@@ -50,7 +53,9 @@ def tune(make_packed, settings, warps=(2, 4, 8), reps: int = 3, max_candidates: 
                 e1.record(stream)
                 torch.cuda.synchronize()
                 ms = e0.elapsed_time(e1) / reps
-            except Exception:
+            except KernelError as e:  # a shape the library refuses is skipped; any other error propagates
+                if e.status != BR_ETOOBIG:
+                    raise
                 continue
             if best is None or ms < best[2]:
                 best = (list(teams), w, ms)

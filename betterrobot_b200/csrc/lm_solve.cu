@@ -952,15 +952,27 @@ extern "C" int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets)
   return TeamLayout(tree->njoints, tree->nq, tree->nv, max_targets, T, tree->dof_entries, tree->dof_depth, tree->rounds).total;
 }
 
-extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
-                           int32_t warps_per_cta, void* scratch, int64_t scratch_bytes, void* stream) {
+#include <mutex>
+
+namespace {
+std::mutex g_lm_mu;  // guards the two per-device caches below
+// Dynamic shared memory each lm_solve_kernel variant has been allowed on each device
+// (cudaFuncAttributeMaxDynamicSharedMemorySize only ever raised, so a launch that
+// needs less than an earlier one still fits).  Shared by every entry point below.
+int g_smem_allowed[2][64] = {};
+}  // namespace
+
+// Argument checks of both LM entry points: BR_OK, an error, or kLmNothing when the batch
+// has no problem to launch.
+constexpr int kLmNothing = 1;
+static int lm_check(const br_ik_batch_t* batch, const br_ik_settings_t* settings, const br_ik_result_t* result,
+                    int32_t warps_per_cta) {
   if (!batch || !settings || !result) return BR_EINVAL;
   const br_ik_batch_t& b = *batch;
   if (b.n_problems < 0 || b.n_items < 0 || b.n_classes < 1) return BR_EINVAL;
   if (b.n_classes > BR_MAX_IK_CLASSES || b.max_targets > BR_MAX_IK_TARGETS) return BR_ETOOBIG;
   if (b.max_targets < 1 || !b.trees || !b.team_size) return BR_EINVAL;
-  if (!scratch || scratch_bytes < BR_LM_SCRATCH_BYTES) return BR_EINVAL;
-  if (b.n_problems == 0 || b.n_items == 0) return BR_OK;
+  if (b.n_problems == 0 || b.n_items == 0) return kLmNothing;
   if (!b.items || !b.order || !b.n_targets || !b.frames || !b.targets || !b.q_offset || !b.x0 || !b.q_rest)
     return BR_EINVAL;
   if (!result->x || !result->iters || !result->status || !result->cost) return BR_EINVAL;
@@ -968,10 +980,17 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
   if (settings->kernel < BR_KERNEL_L2 || settings->kernel > BR_KERNEL_TUKEY) return BR_EINVAL;
   if (settings->kernel != BR_KERNEL_L2 && !(settings->kernel_param > 0.f)) return BR_EINVAL;
   if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
+  return BR_OK;
+}
+
+// Launch shape, shared-memory attribute, queue reset and launch of both LM entry points
+// (arguments already checked by lm_check); `queue` is BR_LM_SCRATCH_BYTES of device memory.
+static int lm_launch(const br_ik_batch_t& b, const br_ik_settings_t& settings, const br_ik_result_t& result,
+                     int32_t warps_per_cta, void* queue, cudaStream_t s) {
   LmParams p = {};
-  p.s = *settings;
+  p.s = settings;
   p.b = b;
-  p.r = *result;
+  p.r = result;
   int warp_floats = 0;
   for (int c = 0; c < b.n_classes; ++c) {
     const int st = validate_tree(&b.trees[c]);
@@ -986,8 +1005,9 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;
-  p.queue = reinterpret_cast<int32_t*>(scratch);
+  p.queue = reinterpret_cast<int32_t*>(queue);
   const DeviceInfo& dev = device_info();
+  if (dev.device < 0 || dev.device >= 64) return BR_EINVAL;
   int wpc = warps_per_cta;
   size_t bytes = (size_t)wpc * warp_floats * sizeof(float);
   while ((int64_t)bytes > dev.max_smem_optin && wpc > 1) {
@@ -995,15 +1015,17 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
     bytes = (size_t)wpc * warp_floats * sizeof(float);
   }
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  bool general = b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2;
+  bool general = b.target_kind != nullptr || settings.kernel != BR_KERNEL_L2;
   for (int c = 0; c < b.n_classes; ++c) general |= (b.trees[c].kinds & ~kBasicKinds) != 0 || b.trees[c].kinds == 0;
   auto kern = general ? lm_solve_kernel<true> : lm_solve_kernel<false>;
-  static int configured[2][16] = {};
-  int& have = configured[general][dev.device & 15];
-  if ((int)bytes > have) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return (int)e;
-    have = (int)bytes;
+  {
+    std::lock_guard<std::mutex> lock(g_lm_mu);
+    int& have = g_smem_allowed[general][dev.device];
+    if ((int)bytes > have) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      if (e != cudaSuccess) return (int)e;
+      have = (int)bytes;
+    }
   }
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpc * kWarp, bytes);
@@ -1011,11 +1033,18 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
   const int64_t need = (b.n_items + wpc - 1) / wpc;
   const int64_t cap = (int64_t)per_sm * dev.sms;
   const int grid = (int)(need < cap ? need : cap);
-  cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int32_t), s);
+  cudaError_t e = cudaMemsetAsync(queue, 0, BR_LM_SCRATCH_BYTES, s);  // the queue counter starts at zero
   if (e != cudaSuccess) return (int)e;
   kern<<<grid, wpc * kWarp, bytes, s>>>(p);
   return (int)cudaGetLastError();
+}
+
+extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* settings, br_ik_result_t* result,
+                           int32_t warps_per_cta, void* scratch, int64_t scratch_bytes, void* stream) {
+  if (batch && (!scratch || scratch_bytes < BR_LM_SCRATCH_BYTES)) return BR_EINVAL;
+  const int st = lm_check(batch, settings, result, warps_per_cta);
+  if (st) return st == kLmNothing ? BR_OK : st;
+  return lm_launch(*batch, *settings, *result, warps_per_cta, scratch, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -1032,14 +1061,13 @@ extern "C" int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* s
 // The array exists once per device that loads this library and lives until the
 // process exits.  All calls on a device share it: two calls that run at the same
 // time on the GPU (e.g. on two streams) race on the work queue and must not
-// overlap.  Each call zeroes the part it uses before its launch.
+// overlap.  Each call zeroes the part it uses before its launch.  The array's device
+// address is looked up on the first call on each device and kept: a cudaDeviceReset
+// between calls reloads the module at another address and is not supported.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 static __device__ __align__(256) unsigned char g_lm_noalloc_scratch[BR_LM_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[64] = {};  // device address of g_lm_noalloc_scratch, per device ordinal
 }  // namespace
 
@@ -1050,7 +1078,7 @@ static int noalloc_scratch_address(void** out) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
   if (dev < 0 || dev >= 64) return BR_EINVAL;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  std::lock_guard<std::mutex> lock(g_lm_mu);
   if (!g_noalloc_ptr[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_lm_noalloc_scratch);
@@ -1063,65 +1091,11 @@ static int noalloc_scratch_address(void** out) {
 
 extern "C" int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_settings_t* settings,
                                    br_ik_result_t* result, int32_t warps_per_cta, void* stream) {
-  const int64_t need = BR_LM_SCRATCH_BYTES;  // scratch one launch of lm_solve_kernel uses
-  if (need > BR_LM_NOALLOC_SCRATCH_BYTES) return BR_ETOOBIG;
-  if (!batch || !settings || !result) return BR_EINVAL;
-  const br_ik_batch_t& b = *batch;
-  if (b.n_problems < 0 || b.n_items < 0 || b.n_classes < 1) return BR_EINVAL;
-  if (b.n_classes > BR_MAX_IK_CLASSES || b.max_targets > BR_MAX_IK_TARGETS) return BR_ETOOBIG;
-  if (b.max_targets < 1 || !b.trees || !b.team_size) return BR_EINVAL;
-  if (b.n_problems == 0 || b.n_items == 0) return BR_OK;
-  if (!b.items || !b.order || !b.n_targets || !b.frames || !b.targets || !b.q_offset || !b.x0 || !b.q_rest)
-    return BR_EINVAL;
-  if (!result->x || !result->iters || !result->status || !result->cost) return BR_EINVAL;
-  if (settings->max_iter < 0) return BR_EINVAL;
-  if (settings->kernel < BR_KERNEL_L2 || settings->kernel > BR_KERNEL_TUKEY) return BR_EINVAL;
-  if (settings->kernel != BR_KERNEL_L2 && !(settings->kernel_param > 0.f)) return BR_EINVAL;
-  if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
+  static_assert(BR_LM_SCRATCH_BYTES <= BR_LM_NOALLOC_SCRATCH_BYTES, "the static scratch is too small");
+  const int st = lm_check(batch, settings, result, warps_per_cta);
+  if (st) return st == kLmNothing ? BR_OK : st;
   void* scratch = nullptr;
-  int st = noalloc_scratch_address(&scratch);
-  if (st) return st;
-  LmParams p = {};
-  p.s = *settings;
-  p.b = b;
-  p.r = *result;
-  int warp_floats = 0;
-  for (int c = 0; c < b.n_classes; ++c) {
-    st = validate_tree(&b.trees[c]);
-    if (st) return st;
-    if (!b.trees[c].dof_sched) return BR_EINVAL;           // the factorization's level schedule
-    const int T = b.team_size[c];
-    if (T != kLmTeam) return BR_EINVAL;                    // the kernel is built for 32-lane teams
-    p.trees[c] = b.trees[c];
-    p.team[c] = T;
-    const br_tree_t& tc = b.trees[c];
-    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth, tc.rounds).total;
-    if (f > warp_floats) warp_floats = f;
-  }
-  p.warp_floats = warp_floats;
-  p.queue = reinterpret_cast<int32_t*>(scratch);
-  const DeviceInfo& dev = device_info();
-  int wpc = warps_per_cta;
-  size_t bytes = (size_t)wpc * warp_floats * sizeof(float);
-  while ((int64_t)bytes > dev.max_smem_optin && wpc > 1) {
-    wpc >>= 1;
-    bytes = (size_t)wpc * warp_floats * sizeof(float);
-  }
-  if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
-  bool general = b.target_kind != nullptr || settings->kernel != BR_KERNEL_L2;
-  for (int c = 0; c < b.n_classes; ++c) general |= (b.trees[c].kinds & ~kBasicKinds) != 0 || b.trees[c].kinds == 0;
-  auto kern = general ? lm_solve_kernel<true> : lm_solve_kernel<false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e != cudaSuccess) return (int)e;
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpc * kWarp, bytes);
-  if (per_sm < 1) per_sm = 1;
-  const int64_t want = (b.n_items + wpc - 1) / wpc;
-  const int64_t cap = (int64_t)per_sm * dev.sms;
-  const int grid = (int)(want < cap ? want : cap);
-  cudaStream_t s = (cudaStream_t)stream;
-  e = cudaMemsetAsync(scratch, 0, (size_t)need, s);  // the queue counter must start at zero
-  if (e != cudaSuccess) return (int)e;
-  kern<<<grid, wpc * kWarp, bytes, s>>>(p);
-  return (int)cudaGetLastError();
+  const int sa = noalloc_scratch_address(&scratch);
+  if (sa) return sa;
+  return lm_launch(*batch, *settings, *result, warps_per_cta, scratch, (cudaStream_t)stream);
 }

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import weakref
 
 import numpy as np
 import torch
@@ -176,7 +177,7 @@ class DeviceTree:
     """Tree table resident on one CUDA device plus its ``br_tree_t`` struct."""
 
     def __init__(self, model, device: torch.device):
-        self.model = model
+        self._model = _weak(model)
         self.arrays = TreeArrays(model)
         sched = self.arrays.dof_schedule() if self.arrays.nv else None
         buf, offs = self.arrays.blob([("dof_sched", sched)] if sched is not None else [])
@@ -198,7 +199,27 @@ class DeviceTree:
         self.n_active = len(act)
 
 
+    @property
+    def model(self):
+        """The model this table was built from (None once it has been garbage collected)."""
+        return self._model()
+
+
+def _weak(model):
+    """A weak reference to ``model``, or a strong one for objects that cannot be weakly referenced."""
+    try:
+        return weakref.ref(model)
+    except TypeError:
+        return lambda: model
+
+
+# (id(model), device) -> DeviceTree.  Entries refer to their model weakly and are dropped
+# when it is collected, so the cache keeps no model (nor its device table) alive.
 _CACHE: dict[tuple[int, str], DeviceTree] = {}
+
+
+def _drop(key) -> None:
+    _CACHE.pop(key, None)
 
 
 def device_tree(model, device) -> DeviceTree:
@@ -210,4 +231,8 @@ def device_tree(model, device) -> DeviceTree:
     if dt is None or dt.model is not model:
         dt = DeviceTree(model, device)
         _CACHE[key] = dt
+        try:
+            weakref.finalize(model, _drop, key)
+        except TypeError:
+            pass
     return dt

@@ -242,7 +242,8 @@ BR_API int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* setti
  * of BR_LM_NOALLOC_SCRATCH_BYTES inside the library (one per device, kept until
  * the process exits) instead of a caller pointer; a launch needing more than that
  * returns BR_ETOOBIG.  The first call on each device looks up the array's device
- * address and should be made before any stream capture.  Calls share the array:
+ * address and should be made before any stream capture; the address is kept, so a
+ * cudaDeviceReset between calls is not supported.  Calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.  No
  * counterpart in the reference (BetterRobot has no native code).
  */

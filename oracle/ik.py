@@ -155,6 +155,11 @@ class IKOutcome:
     cost: np.ndarray       # (P,)   0.5 |r|^2
     iters: np.ndarray      # (P,)   int
     converged: np.ndarray  # (P,)   bool
+    # (P,) smallest |cost_new - cost| in units of the cost's float64 spacing over the accept
+    # tests that decide convergence (pre-step |J^T r| < tol); inf if there was none.  A few
+    # units mean the verdict was decided by the rounding of a float64 sum: any implementation
+    # that sums in another order (BetterRobot's torch code included) flips it at random.
+    margin: np.ndarray | None = None
 
 
 def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None, kinds=None) -> IKOutcome:
@@ -171,6 +176,7 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None, kinds=None)
     active = np.ones(P, dtype=bool)
     iters = np.full(P, s.max_iter, dtype=np.int64)
     conv = np.zeros(P, dtype=bool)
+    margin = np.full(P, np.inf)
     nv = model.nv
     for it in range(s.max_iter):
         idx = np.nonzero(active)[0]
@@ -193,6 +199,9 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None, kinds=None)
         rn, _ = residual_and_jacobian(model, qn, frame_ids, targets[idx], q_rest, s, want_jac=False, kinds=kinds)
         cn = 0.5 * np.sum(rn * rn, -1)
         gnorm = np.linalg.norm(Jtr, axis=-1)
+        ulps = np.abs(cn - cost[idx]) / np.spacing(np.maximum(cn, cost[idx]))
+        dec = gnorm < s.tol
+        margin[idx[dec]] = np.minimum(margin[idx[dec]], ulps[dec])
         if s.optimizer == "lm":
             acc = cn < cost[idx]
             a_idx = idx[acc]
@@ -212,7 +221,7 @@ def solve(model, frame_ids, targets, q0, s: IKSettings, q_rest=None, kinds=None)
         conv[d_idx] = True
         iters[d_idx] = it + 1
         active[d_idx] = False
-    return IKOutcome(q=q, residual=r, cost=cost, iters=iters, converged=conv)
+    return IKOutcome(q=q, residual=r, cost=cost, iters=iters, converged=conv, margin=margin)
 
 
 def pose_errors(model, q, frame_ids, targets):

@@ -85,3 +85,16 @@ def test_shape_error_before_device_check():
     m = syn.model_from_spec(syn.chain_spec())
     with pytest.raises(ShapeError):
         forward_kinematics(m, torch.zeros(4, m.nq + 1))
+
+
+def test_device_tree_cache_keeps_no_model_alive():
+    import gc
+    from betterrobot_b200 import tree as tr
+    m = syn.model_from_spec(syn.chain_spec())
+    dt = tr.device_tree(m, "cpu")
+    key = (id(m), "cpu")
+    assert tr._CACHE[key] is dt and dt.model is m
+    assert tr.device_tree(m, "cpu") is dt  # cached
+    del m
+    gc.collect()
+    assert key not in tr._CACHE and dt.model is None

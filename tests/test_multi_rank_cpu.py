@@ -51,3 +51,22 @@ def test_two_gloo_ranks_disjoint_shards_and_reductions():
     assert mx0 == mx1 == 11.0 and sm0 == sm1 == 3.0
     assert n0 == n1 and sum(n0) == 64          # same mix per rank (weak scaling)
     assert all(a != b for a, b in zip(d0, d1))  # different problems on each rank
+
+
+def test_bench_replica_launcher_runs_two_ranks(capfd):
+    """``bench.py --gpus N`` started without torchrun launches N ranks itself (``launch_replicas``);
+    each joins the process group from RANK / WORLD_SIZE / MASTER_* and rank 0 reports n_gpus = N."""
+    import json
+    import sys
+
+    import bench
+    probe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "replica_probe.py")
+    env_before = {k: os.environ.pop(k) for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK") if k in os.environ}
+    try:
+        rc = bench.launch_replicas([sys.executable, probe], 2, timeout_s=240)
+    finally:
+        os.environ.update(env_before)
+    out = capfd.readouterr().out.strip().splitlines()
+    assert rc == 0
+    line = json.loads(out[-1])
+    assert line == {"n_gpus": 2, "max": 11.0, "sum": 3.0, "local_rank": 0}

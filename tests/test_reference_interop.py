@@ -7,9 +7,12 @@
 * The reference's public ``forward_kinematics(..., backend=BACKEND)`` dispatches into this
   package (on a machine without a GPU the call stops at the CUDA check).
 
-Skipped where the reference source tree is not present (``BETTERROBOT_SRC``).
+Runs where BetterRobot is importable: its source tree named by ``BETTERROBOT_SRC`` (the
+directory that holds the ``better_robot`` package), or an installed ``better_robot``.
+Elsewhere every test here is skipped.
 """
 
+import importlib.util
 import os
 import sys
 
@@ -17,14 +20,14 @@ import numpy as np
 import pytest
 import torch
 
-SRC = os.environ.get("BETTERROBOT_SRC", "/root/reference/src")
-if not os.path.isdir(os.path.join(SRC, "better_robot")):
-    pytest.skip("BetterRobot source tree not available", allow_module_level=True)
-sys.path.insert(0, SRC)
+SRC = os.environ.get("BETTERROBOT_SRC")
+if SRC and os.path.isdir(os.path.join(SRC, "better_robot")) and SRC not in sys.path:
+    sys.path.insert(0, SRC)
+HAVE_REFERENCE = importlib.util.find_spec("better_robot") is not None
+pytestmark = pytest.mark.skipif(not HAVE_REFERENCE, reason="BetterRobot is not importable (set BETTERROBOT_SRC)")
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 
 from betterrobot_b200 import synthetic as syn  # noqa: E402
-from betterrobot_b200.backend import BACKEND  # noqa: E402
 from betterrobot_b200.tree import TreeArrays  # noqa: E402
 
 SPECS = {"chain7": syn.chain_spec(), "humanoid": syn.humanoid_spec(), "dual_arm": syn.dual_arm_spec()}
@@ -44,6 +47,7 @@ def test_reference_model_packs_identically(name):
 
 def test_backend_satisfies_reference_protocols():
     from better_robot.backends.protocol import Backend, DynamicsOps, KinematicsOps, LieOps
+    from betterrobot_b200.backend import BACKEND
     assert isinstance(BACKEND, Backend)
     assert isinstance(BACKEND.lie, LieOps)
     assert isinstance(BACKEND.kinematics, KinematicsOps)
@@ -53,6 +57,7 @@ def test_backend_satisfies_reference_protocols():
 def test_reference_entry_point_dispatches_here():
     import better_robot as br_ref
     from make_golden import reference_model
+    from betterrobot_b200.backend import BACKEND
     from betterrobot_b200.exceptions import BetterRobotError
     if torch.cuda.is_available():
         pytest.skip("CPU-only check")
@@ -60,3 +65,44 @@ def test_reference_entry_point_dispatches_here():
     q = torch.zeros(2, m.nq, dtype=torch.float32)
     with pytest.raises(BetterRobotError, match="CUDA"):
         br_ref.forward_kinematics(m, q, backend=BACKEND)
+
+
+def test_reference_except_clauses_catch_errors_raised_here():
+    """With BetterRobot importable, this package's exception classes derive from the reference's:
+    an error raised by these kernels through the reference's own entry point is caught by
+    ``except better_robot.exceptions.<Name>``.  Run in a fresh interpreter so that the import
+    order (reference first or not) is the one a user has."""
+    import subprocess
+    import textwrap
+    code = textwrap.dedent("""
+        import sys, torch
+        import better_robot as br_ref
+        from better_robot import exceptions as rex
+        from betterrobot_b200 import exceptions as ex
+        from betterrobot_b200.backend import BACKEND
+        from make_golden import reference_model
+        from betterrobot_b200 import synthetic as syn
+        names = ["BetterRobotError", "ModelInconsistencyError", "DeviceMismatchError", "DtypeMismatchError",
+                 "QuaternionNormError", "ShapeError", "ConvergenceError", "BackendNotAvailableError",
+                 "StaleCacheError", "UnsupportedJointError"]
+        for n in names:
+            assert issubclass(getattr(ex, n), getattr(rex, n)), n
+            assert issubclass(getattr(ex, n), ex.BetterRobotError), n
+        assert issubclass(ex.KernelError, rex.BetterRobotError)
+        m = reference_model(syn.chain_spec())
+        q = torch.zeros(2, m.nq, dtype=torch.float32)   # a CPU tensor: this backend refuses it
+        try:
+            br_ref.forward_kinematics(m, q, backend=BACKEND)
+        except rex.BetterRobotError as e:
+            assert isinstance(e, ex.BetterRobotError), type(e)
+            print("caught", type(e).__name__)
+        else:
+            raise SystemExit("no error raised")
+    """)
+    here = os.path.dirname(os.path.abspath(__file__))
+    path = [p for p in (SRC, os.path.dirname(here), os.path.join(here, "golden")) if p]
+    env = dict(os.environ, PYTHONPATH=os.pathsep.join(path + [os.environ.get("PYTHONPATH", "")]),
+               CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "caught" in r.stdout
