@@ -40,7 +40,7 @@ class IKSettings(ctypes.Structure):
                 ("pos_weight", ctypes.c_float), ("ori_weight", ctypes.c_float),
                 ("limit_weight", ctypes.c_float), ("rest_weight", ctypes.c_float),
                 ("max_iter", c_int32), ("optimizer", c_int32), ("kernel", c_int32),
-                ("kernel_param", ctypes.c_float)]
+                ("kernel_param", ctypes.c_float), ("precision", c_int32)]
 
 
 class IKBatch(ctypes.Structure):

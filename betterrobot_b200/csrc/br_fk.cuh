@@ -43,6 +43,16 @@ __host__ __device__ __forceinline__ int joint_nv(int jt) {
     default: return 0;
   }
 }
+__host__ __device__ __forceinline__ int joint_nq(int jt) {
+  switch (jt) {
+    case BR_JOINT_REVOLUTE: case BR_JOINT_PRISMATIC: return 1;
+    case BR_JOINT_REVOLUTE_UNBOUNDED: return 2;
+    case BR_JOINT_TRANSLATION: return 3;
+    case BR_JOINT_SPHERICAL: case BR_JOINT_PLANAR: return 4;
+    case BR_JOINT_FREE_FLYER: return 7;
+    default: return 0;
+  }
+}
 // Kinds whose configuration slots are their tangent coordinates (q + v, nq == nv).
 __host__ __device__ __forceinline__ bool joint_is_vector(int jt) {
   return jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC || jt == BR_JOINT_TRANSLATION;

@@ -37,6 +37,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/br_b200.h"
 #include "br_common.cuh"
 #include "br_fk.cuh"
@@ -69,7 +71,8 @@ struct TeamLayout {
   // dof_depth), 0 for the dense bounds.
   // rounds: the tree's pointer-jumping FK rounds (br_tree_t.rounds), which decide the
   // pose buffer FK returns.
-  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T, int ent, int dep, int rounds) {
+  // rs: floats per scalar of the Jacobian / normal-equation regions (1: float32, 2: float64).
+  __host__ __device__ TeamLayout(int nj, int nq, int nv, int K, int T, int ent, int dep, int rounds, int rs = 1) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += round4(n); return r; };
     parent = take(nj); jtype = take(nj); idxq = take(nj); idxv = take(nj);
@@ -82,26 +85,26 @@ struct TeamLayout {
     poseA = take(14 * nj); poseB = take(14 * nj); tw = take(16 * K); xi = take(16 * K);
     d = take(2 * nv);
     tgt = take(16 * K);
-    // float32 / int regions
-    ancA = take(nj); ancB = take(nj);
-    jri = take(16 * K); colw = take(8 * nv);
-    g = take(nv); delta = take(nv);
+    // normal-equation regions (rs floats per scalar), then float32 / int regions
+    jri = take(16 * K * rs); colw = take(8 * nv * rs);
+    g = take(nv * rs); delta = take(nv * rs);
     const int ntri = nv * (nv + 1) / 2;
     n_ent = (ent > 0 && ent < ntri) ? ent : ntri;
     anc_stride = (dep > 0 && dep < nv) ? dep : (nv > 0 ? nv : 1);
-    jtj = take(n_ent);                         // J^T J, one row per DOF over its ancestors
+    jtj = take(n_ent * rs);                    // J^T J, one row per DOF over its ancestors
     // one target's J columns (build) / the factor and its right-hand-side slots (solve):
     // in the pose buffer that FK does not return (poseA after an odd number of rounds, else
     // poseB), dead while the normal equations are built and solved, when it is large enough
-    const int wneed = 6 * nv > n_ent + nv ? 6 * nv : n_ent + nv;
+    const int wneed = (6 * nv > n_ent + nv ? 6 * nv : n_ent + nv) * rs;
     work = wneed <= 14 * nj ? ((rounds & 1) ? poseA : poseB) : take(wneed);
+    dinv = take(nv * rs);                      // 1 / L_jj
+    ancA = take(nj); ancB = take(nj);
     misc = take(8);
     amask = take(2 * nv);                      // uint64 strict ancestors of each DOF
     dpar = take((nv + 3) / 4);                 // int8 parent DOF (-1 at a root)
     ddep = take((nv + 3) / 4);                 // uint8 DOF depth
     rowoff = take((nv + 2) / 2);               // uint16 first entry of each row, nv + 1 values
     ancd = take((nv * anc_stride + 3) / 4);    // uint8 ancestor of DOF c at depth a: ancd[c * anc_stride + a]
-    dinv = take(nv);                           // 1 / L_jj
     sup = take((K * nv + 3) / 4);              // uint8 support columns of each target, ascending
     nsup = take(K);
     total = o;
@@ -113,16 +116,45 @@ __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
 // IRLS weight w(s) of one squared residual row s (optim/kernels/{huber,cauchy,tukey}.py:
 // weight; applied as in levenberg_marquardt.py:27-44, whose sqrt(w) scales both the row
 // and its Jacobian row, so J^T J and J^T r pick up w).  Evaluated in float64.
-__device__ __forceinline__ float irls_weight(int kernel, double c, double s) {
+template <typename R>
+__device__ __forceinline__ R irls_weight(int kernel, double c, double s) {
   switch (kernel) {
-    case BR_KERNEL_HUBER: return s <= c * c ? 1.f : (float)(c / sqrt(fmax(s, 0.0) + 1e-30));
-    case BR_KERNEL_CAUCHY: return (float)(1.0 / (1.0 + s / (c * c)));
+    case BR_KERNEL_HUBER: return s <= c * c ? (R)1 : (R)(c / sqrt(fmax(s, 0.0) + 1e-30));
+    case BR_KERNEL_CAUCHY: return (R)(1.0 / (1.0 + s / (c * c)));
     case BR_KERNEL_TUKEY: {
       const double u = fmax(1.0 - s / (c * c), 0.0);
-      return (float)(u * u);
+      return (R)(u * u);
     }
-    default: return 1.f;
+    default: return (R)1;
   }
+}
+
+// Scalar helpers of the normal-equation arithmetic, for R = float (the default variant) or
+// R = double (the float64 variant: the Jacobian, J^T J, J^T r and the factorization in float64).
+__device__ __forceinline__ float rfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float rrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double rrcp(double a) { return __drcp_rn(a); }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double rmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float rsqrt_(float a) { return sqrtf(a); }
+__device__ __forceinline__ double rsqrt_(double a) { return sqrt(a); }
+
+// C(th^2) of the SO3 Jr^-1 = I + W/2 + C W^2, C = 1/th^2 - (1 + cos th) / (2 th sin th)
+// (tangents.py:122-145), in float64: its Taylor series 1/12 + th^2/720 + th^4/30240 +
+// th^6/1209600 + th^8/47900160 below th^2 = 0.1 (the next term is below 1e-15 of C there),
+// else the closed form.
+__device__ __forceinline__ double dvinv_coeff(double th2) {
+  if (th2 < 0.1) {
+    return fma(th2, fma(th2, fma(th2, fma(th2, 1.0 / 47900160.0, 1.0 / 1209600.0), 1.0 / 30240.0), 1.0 / 720.0),
+               1.0 / 12.0);
+  }
+  const double th = sqrt(th2);
+  double s, c;
+  sincos(th, &s, &c);
+  return 1.0 / th2 - (1.0 + c) / (2.0 * th * s);
 }
 
 // Lanes per problem (team size) the kernel is built for, and the DOFs one lane owns in the
@@ -191,12 +223,15 @@ __device__ __forceinline__ Pose to_f(const DPose& P) {
 // kGeneral = false compiles the plain stack (pose targets, l2 kernel, fixed / revolute /
 // prismatic / free-flyer joints) with the other branches folded away; the host launches it
 // whenever a batch needs nothing else.
-template <int T, bool kGeneral>
+// kF64 = true computes the Jacobian columns, J^T J, J^T r, the factorization and the step in
+// float64 (R = double) instead of float32.
+template <int T, bool kGeneral, bool kF64>
 __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob, float* sm, const Team<T>& tm,
                               const uint32_t*& sched_ok) {
+  using R = typename std::conditional<kF64, double, float>::type;
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv;
   const int K = P.b.max_targets;
-  const TeamLayout L(nj, nq, nv, K, T, tree.dof_entries, tree.dof_depth, tree.rounds);
+  const TeamLayout L(nj, nq, nv, K, T, tree.dof_entries, tree.dof_depth, tree.rounds, kF64 ? 2 : 1);
   int* parent = reinterpret_cast<int*>(sm + L.parent);
   int* jtype = reinterpret_cast<int*>(sm + L.jtype);
   int* idxq = reinterpret_cast<int*>(sm + L.idxq);
@@ -223,28 +258,28 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   double* tgt = reinterpret_cast<double*>(sm + L.tgt);
   int* ancA = reinterpret_cast<int*>(sm + L.ancA);
   int* ancB = reinterpret_cast<int*>(sm + L.ancB);
-  float* jri = sm + L.jri;
-  float* colw = sm + L.colw;
-  float* g = sm + L.g;
-  float* delta = sm + L.delta;
-  float* jtj = sm + L.jtj;
-  float* work = sm + L.work;
+  R* jri = reinterpret_cast<R*>(sm + L.jri);
+  R* colw = reinterpret_cast<R*>(sm + L.colw);
+  R* g = reinterpret_cast<R*>(sm + L.g);
+  R* delta = reinterpret_cast<R*>(sm + L.delta);
+  R* jtj = reinterpret_cast<R*>(sm + L.jtj);
+  R* work = reinterpret_cast<R*>(sm + L.work);
   unsigned long long* amask = reinterpret_cast<unsigned long long*>(sm + L.amask);
   signed char* dpar = reinterpret_cast<signed char*>(sm + L.dpar);
   unsigned char* ddep = reinterpret_cast<unsigned char*>(sm + L.ddep);
   unsigned short* rowoff = reinterpret_cast<unsigned short*>(sm + L.rowoff);
   unsigned char* ancd = reinterpret_cast<unsigned char*>(sm + L.ancd);
-  float* dinv = sm + L.dinv;
+  R* dinv = reinterpret_cast<R*>(sm + L.dinv);
   int* misc = reinterpret_cast<int*>(sm + L.misc);  // [0]: the tree's tables are inconsistent; [1]: 1 + max DOF depth
   unsigned char* sup = reinterpret_cast<unsigned char*>(sm + L.sup);
   int* nsup = reinterpret_cast<int*>(sm + L.nsup);
   const int tl = tm.tl;
   const br_ik_settings_t& S = P.s;
-  const float wp = S.pos_weight, wo = S.ori_weight, wl = S.limit_weight, wr = S.rest_weight;
+  const R wp = (R)S.pos_weight, wo = (R)S.ori_weight, wl = (R)S.limit_weight, wr = (R)S.rest_weight;
   const double wpd = wp, wod = wo, wld = wl, wrd = wr;
   const double kc = S.kernel_param;
   const bool irls = kGeneral && S.kernel != BR_KERNEL_L2;
-  const bool use_limits = wl > 0.f, use_rest = wr > 0.f;
+  const bool use_limits = S.limit_weight > 0.f, use_rest = S.rest_weight > 0.f;
   // packed lower-triangle pair p -> (a, b), b <= a, p = tri(a) + b
   auto decode_pair = [](int p) {
     float r;  // approximate square root: the two corrections below make the decode exact
@@ -518,40 +553,90 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // float32 J^T J (packed lower, column-major) and g = J^T r at q with world poses `pose`; returns |g|.
   // Each target's pose Jacobian diag(w) Jr^-1 blockdiag(R^T, R^T) J_lwa (pose.py:68-103) is
   // built only on its support columns and accumulated into the (support x support) block.
-  auto build_normal = [&](const double* q, const double* pose) -> float {
+  auto build_normal = [&](const double* q, const double* pose) -> R {
     for (int c = tl; c < nv; c += T) {
-      const Pose Tj = to_f(lds(pose, nj, cjoint[c]));
-      const float3 a = qrot(Tj.q, f3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
-      *reinterpret_cast<float4*>(colw + 8 * c) = make_float4(a.x, a.y, a.z, 0.f);
-      *reinterpret_cast<float4*>(colw + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
-      g[c] = 0.f;
+      if constexpr (kF64) {
+        const DPose Tj = lds(pose, nj, cjoint[c]);
+        const double3 a = dqrot(Tj.q, d3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
+        double* cw = colw + 8 * c;
+        cw[0] = a.x; cw[1] = a.y; cw[2] = a.z; cw[4] = Tj.t.x; cw[5] = Tj.t.y; cw[6] = Tj.t.z;
+      } else {
+        const Pose Tj = to_f(lds(pose, nj, cjoint[c]));
+        const float3 a = qrot(Tj.q, f3(caxis[4 * c], caxis[4 * c + 1], caxis[4 * c + 2]));
+        *reinterpret_cast<float4*>(colw + 8 * c) = make_float4(a.x, a.y, a.z, 0.f);
+        *reinterpret_cast<float4*>(colw + 8 * c + 4) = make_float4(Tj.t.x, Tj.t.y, Tj.t.z, 0.f);
+      }
+      g[c] = (R)0;
     }
     for (int t = tl; t < nt; t += T) {
       const double* e = xi + 8 * t;
-      float* o = jri + 16 * t;
+      R* o = jri + 16 * t;
       if (!kGeneral || tkind[t] == BR_TARGET_POSE) {                   // SE3 Jr^-1(xi), tangents.py:204-207
-        const JrInv J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
-        o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
-        for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
+        if constexpr (kF64) {
+          const DJrInv J = djr_inv_se3<9>(d3(e[0], e[1], e[2]), d3(e[3], e[4], e[5]));
+          o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
+          for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
+        } else {
+          const JrInv J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
+          o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
+          for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
+        }
       } else {  // orientation: SO3 Jr^-1(r) (tangents.py:122-145) as the angular block, no coupling;
                 // position: identity (its rows are replaced by J_lwa's linear rows)
         const bool ori = tkind[t] == BR_TARGET_ORIENTATION;
-        const float3 w = f3((float)e[3], (float)e[4], (float)e[5]);
-        o[0] = w.x; o[1] = w.y; o[2] = w.z;
-        o[3] = 1.f;
-        o[4] = ori ? 0.5f : 0.f;
-        o[5] = ori ? vinv_coeff(dot(w, w)) : 0.f;
-        for (int k = 0; k < 9; ++k) o[6 + k] = 0.f;
+        o[0] = (R)e[3]; o[1] = (R)e[4]; o[2] = (R)e[5];
+        o[3] = (R)1;
+        o[4] = ori ? (R)0.5 : (R)0;
+        if constexpr (kF64) {
+          o[5] = ori ? dvinv_coeff(e[3] * e[3] + e[4] * e[4] + e[5] * e[5]) : 0.0;
+        } else {
+          const float3 w = f3((float)e[3], (float)e[4], (float)e[5]);
+          o[5] = ori ? vinv_coeff(dot(w, w)) : 0.f;
+        }
+        for (int k = 0; k < 9; ++k) o[6 + k] = (R)0;
       }
     }
 #pragma unroll 1
-    for (int e = tl; e < nL; e += T) jtj[e] = 0.f;
+    for (int e = tl; e < nL; e += T) jtj[e] = (R)0;
     tm.sync();
-    float* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
+    R* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
     for (int t = 0; t < nt; ++t) {
       const int ns = nsup[t];
       const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
       const unsigned char* st = sup + t * nv;
+      if constexpr (kF64) {
+        const DPose Tee = ldd(tw + 8 * t);
+        const double* o = jri + 16 * t;
+        DJrInv J;
+        J.w = d3(o[0], o[1], o[2]);
+        J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
+        const double4 qc = dqconj(Tee.q);
+        for (int u = tl; u < ns; u += T) {
+          const int c = st[u];
+          const double* cw = colw + 8 * c;
+          const double3 a = d3(cw[0], cw[1], cw[2]);
+          double3 lin, ang;
+          if (ckind[c] == 0) {
+            lin = dcross(a, dsub(Tee.t, d3(cw[4], cw[5], cw[6])));      // jacobian.py:213-215
+            ang = a;
+          } else {
+            lin = a;
+            ang = d3(0.0, 0.0, 0.0);
+          }
+          double3 ol, oa;
+          djr_inv_apply(J, dqrot(qc, lin), dqrot(qc, ang), ol, oa);    // pose.py:91-99
+          if (kind == BR_TARGET_POSITION) {            // top rows of J_lwa (pose.py:133-141)
+            ol = lin;
+            oa = d3(0.0, 0.0, 0.0);
+          } else if (kind == BR_TARGET_ORIENTATION) {  // Jr^-1(r) R^T J_ang (pose.py:175-195)
+            ol = d3(0.0, 0.0, 0.0);
+          }
+          Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
+          Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
+        }
+      } else {
       const Pose Tee = to_f(ldd(tw + 8 * t));
       const float* o = jri + 16 * t;
       JrInv J;
@@ -583,48 +668,49 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
         Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
       }
+      }
       tm.sync();
       const double* e = xi + 8 * t;
-      float kw[6] = {1.f, 1.f, 1.f, 1.f, 1.f, 1.f};  // IRLS weight of each of the target's 6 rows
+      R kw[6] = {(R)1, (R)1, (R)1, (R)1, (R)1, (R)1};  // IRLS weight of each of the target's 6 rows
       if (irls) {
 #pragma unroll
         for (int r = 0; r < 6; ++r) {
           const double rr = (r < 3 ? wpd : wod) * e[r];
-          kw[r] = irls_weight(S.kernel, kc, rr * rr);
+          kw[r] = irls_weight<R>(S.kernel, kc, rr * rr);
         }
       }
       for (int p = tl; p < tri(ns); p += T) {
         const int uv = decode_pair(p);                        // row-major (u >= v) decode of p
         const int u = uv & 0xff, v = uv >> 8;
-        float acc = 0.f;
+        R acc = (R)0;
         if (irls) {
 #pragma unroll
-          for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u] * kw[r], Jc[r * nv + v], acc);
+          for (int r = 0; r < 6; ++r) acc = rfma(Jc[r * nv + u] * kw[r], Jc[r * nv + v], acc);
         } else {
 #pragma unroll
-          for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], Jc[r * nv + v], acc);
+          for (int r = 0; r < 6; ++r) acc = rfma(Jc[r * nv + u], Jc[r * nv + v], acc);
         }
         jtj[rowoff[st[u]] + ddep[st[v]]] += acc;  // st ascending: st[u] descends from st[v]
       }
-      const float rw[6] = {wp * (float)e[0] * kw[0], wp * (float)e[1] * kw[1], wp * (float)e[2] * kw[2],
-                           wo * (float)e[3] * kw[3], wo * (float)e[4] * kw[4], wo * (float)e[5] * kw[5]};
+      const R rw[6] = {wp * (R)e[0] * kw[0], wp * (R)e[1] * kw[1], wp * (R)e[2] * kw[2],
+                       wo * (R)e[3] * kw[3], wo * (R)e[4] * kw[4], wo * (R)e[5] * kw[5]};
       for (int u = tl; u < ns; u += T) {
-        float acc = 0.f;
+        R acc = (R)0;
 #pragma unroll
-        for (int r = 0; r < 6; ++r) acc = fmaf(Jc[r * nv + u], rw[r], acc);
+        for (int r = 0; r < 6; ++r) acc = rfma(Jc[r * nv + u], rw[r], acc);
         g[st[u]] += acc;
       }
       tm.sync();
     }
     // rest (w I, regularization.py:56-64) and limit (+-w on active rows, limits.py:64-86) terms
-    float gg = 0.f;
+    R gg = (R)0;
     for (int c = tl; c < nv; c += T) {
-      float dg = 0.f, gc = g[c];
+      R dg = (R)0, gc = g[c];
       if (use_rest) {
         const double rr = wrd * dr[c];
-        const float w = irls ? irls_weight(S.kernel, kc, rr * rr) : 1.f;
+        const R w = irls ? irls_weight<R>(S.kernel, kc, rr * rr) : (R)1;
         dg += wr * wr * w;
-        gc += wr * wr * w * (float)dr[c];
+        gc += wr * wr * w * (R)dr[c];
       }
       if (use_limits) {
         const int j = cjoint[c];
@@ -632,15 +718,15 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           const int iq = idxq[j] + (c - idxv[j]);
           if (q[iq] < (double)lower[iq]) {
             const double d = (double)lower[iq] - q[iq];
-            const float w = irls ? irls_weight(S.kernel, kc, wld * wld * d * d) : 1.f;
+            const R w = irls ? irls_weight<R>(S.kernel, kc, wld * wld * d * d) : (R)1;
             dg += wl * wl * w;
-            gc -= wl * wl * w * (float)d;
+            gc -= wl * wl * w * (R)d;
           }
           if (q[iq] > (double)upper[iq]) {
             const double d = q[iq] - (double)upper[iq];
-            const float w = irls ? irls_weight(S.kernel, kc, wld * wld * d * d) : 1.f;
+            const R w = irls ? irls_weight<R>(S.kernel, kc, wld * wld * d * d) : (R)1;
             dg += wl * wl * w;
-            gc += wl * wl * w * (float)d;
+            gc += wl * wl * w * (R)d;
           }
         }
       }
@@ -648,9 +734,10 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       g[c] = gc;
       gg += gc * gc;
     }
-    gg = tm.sum(gg);
+#pragma unroll
+    for (int o = T / 2; o > 0; o >>= 1) gg += __shfl_xor_sync(tm.mask, gg, o, T);
     tm.sync();
-    return sqrtf(gg);
+    return rsqrt_(gg);
   };
 
   // Solve (J^T J + damp I) delta = -g in float32 by an LDL^T factorization that eliminates
@@ -664,16 +751,16 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // eliminated together (tasks of the schedule, one lane each), the right-hand side
   // -g is updated in the same tasks (forward substitution), then back substitution
   // runs root first by depth: delta_i = (z_i - sum_a Lm[i][a] delta_anc(i, a)) / D_i.
-  auto solve = [&](float damp) -> bool {
-    float* Lm = work;
-    float* z = work + nL;
+  auto solve = [&](R damp) -> bool {
+    R* Lm = work;
+    R* z = work + nL;
 #pragma unroll 1
     for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
     // pivots of the leaves (final already); a non-leaf's is stored by the task that
     // finalises its diagonal (the schedule's flag)
     for (int i = tl; i < nv; i += T) {
       z[i] = -g[i];
-      dinv[i] = __frcp_rn(jtj[rowoff[i] + ddep[i]] + damp);
+      dinv[i] = rrcp(jtj[rowoff[i] + ddep[i]] + damp);
     }
     tm.sync();
     const int nlev = (int)sched[0];
@@ -688,45 +775,45 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         const uint4 tk = nx;                                   // the next pass's task is in flight
         if (p + T < t1) nx = __ldg(tasks + p + T);
         const int dst = tk.x & 0xffff;
-        float acc = fmaf(-Lm[tk.y & 0xffff] * dinv[tk.z & 0xffff], Lm[tk.y >> 16], Lm[dst]);
+        R acc = rfma(-Lm[tk.y & 0xffff] * dinv[tk.z & 0xffff], Lm[tk.y >> 16], Lm[dst]);
         int e = (int)(tk.z >> 16);
         const int e1 = e + (int)(tk.x >> 16);
         for (; e + 1 < e1; e += 2) {                           // two records in flight at once
           const uint2 ea = __ldg(extra + e), eb = __ldg(extra + e + 1);
-          const float a1 = Lm[ea.x & 0xffff] * dinv[ea.y], a2 = Lm[ea.x >> 16];
-          const float b1 = Lm[eb.x & 0xffff] * dinv[eb.y], b2 = Lm[eb.x >> 16];
-          acc = fmaf(-a1, a2, acc);
-          acc = fmaf(-b1, b2, acc);
+          const R a1 = Lm[ea.x & 0xffff] * dinv[ea.y], a2 = Lm[ea.x >> 16];
+          const R b1 = Lm[eb.x & 0xffff] * dinv[eb.y], b2 = Lm[eb.x >> 16];
+          acc = rfma(-a1, a2, acc);
+          acc = rfma(-b1, b2, acc);
         }
         if (e < e1) {
           const uint2 ex = __ldg(extra + e);
-          acc = fmaf(-Lm[ex.x & 0xffff] * dinv[ex.y], Lm[ex.x >> 16], acc);
+          acc = rfma(-Lm[ex.x & 0xffff] * dinv[ex.y], Lm[ex.x >> 16], acc);
         }
         Lm[dst] = acc;
-        if (tk.w) dinv[tk.w - 1] = __frcp_rn(acc + damp);    // DOF tk.w - 1's pivot is final
+        if (tk.w) dinv[tk.w - 1] = rrcp(acc + damp);         // DOF tk.w - 1's pivot is final
       }
       tm.sync();
     }
     bool bad = false;  // pivots are final once their level is done
     for (int i = tl; i < nv; i += T) {
-      const float piv = Lm[rowoff[i] + ddep[i]] + damp;
-      bad |= !(piv > 0.f) || !isfinite(piv);
-      dinv[i] = __frcp_rn(piv);
+      const R piv = Lm[rowoff[i] + ddep[i]] + damp;
+      bad |= !(piv > (R)0) || !isfinite(piv);
+      dinv[i] = rrcp(piv);
     }
     if (__any_sync(tm.mask, bad)) return false;
     tm.sync();
     // back substitution by depth, root first: a lane keeps its DOFs' right-hand sides in
     // registers; once the DOFs of depth dl are final, every deeper DOF subtracts the
     // term of its one ancestor at depth dl (no two lanes write the same DOF)
-    constexpr int R = lm_rows(T);
-    float zr[R], dvr[R];
-    int dr[R], ror[R];
+    constexpr int NR = lm_rows(T);
+    R zr[NR], dvr[NR];
+    int dr[NR], ror[NR];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < NR; ++r) {
       const int i = tl + T * r;
       const bool in = i < nv;
-      zr[r] = in ? z[i] : 0.f;
-      dvr[r] = in ? dinv[i] : 0.f;
+      zr[r] = in ? z[i] : (R)0;
+      dvr[r] = in ? dinv[i] : (R)0;
       dr[r] = in ? ddep[i] : -1;
       ror[r] = in ? rowoff[i] : 0;
     }
@@ -734,12 +821,12 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
 #pragma unroll 1
     for (int dl = 0; dl < ndl; ++dl) {
 #pragma unroll
-      for (int r = 0; r < R; ++r)
+      for (int r = 0; r < NR; ++r)
         if (dr[r] == dl) delta[tl + T * r] = zr[r] * dvr[r];
       tm.sync();
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-        if (dr[r] > dl) zr[r] = fmaf(-Lm[ror[r] + dl], delta[ancd[(tl + T * r) * L.anc_stride + dl]], zr[r]);
+      for (int r = 0; r < NR; ++r)
+        if (dr[r] > dl) zr[r] = rfma(-Lm[ror[r] + dl], delta[ancd[(tl + T * r) * L.anc_stride + dl]], zr[r]);
     }
     tm.sync();
     return true;
@@ -774,11 +861,11 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         // keeps the float64 exponential
         const DPose a{d3(x[iq], x[iq + 1], x[iq + 2]), make_double4(x[iq + 3], x[iq + 4], x[iq + 5], x[iq + 6])};
         DPose inc;
-        if (kGeneral) {
+        if (kGeneral || kF64) {
           inc = dse3_exp(d3(delta[iv], delta[iv + 1], delta[iv + 2]), d3(delta[iv + 3], delta[iv + 4], delta[iv + 5]));
         } else {
-          const Pose e = se3_exp_step(f3(delta[iv], delta[iv + 1], delta[iv + 2]),
-                                      f3(delta[iv + 3], delta[iv + 4], delta[iv + 5]));
+          const Pose e = se3_exp_step(f3((float)delta[iv], (float)delta[iv + 1], (float)delta[iv + 2]),
+                                      f3((float)delta[iv + 3], (float)delta[iv + 4], (float)delta[iv + 5]));
           inc = DPose{d3(e.t.x, e.t.y, e.t.z), make_double4(e.q.x, e.q.y, e.q.z, e.q.w)};
         }
         DPose n = dcompose(a, inc);
@@ -800,8 +887,8 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   // point was rejected.
   const bool gn = S.optimizer == BR_OPT_GN;
   const bool want_residual = P.r.residual && P.b.r_offset;
-  float lam = gn ? 0.f : S.lam0;
-  float gnorm = 0.f;
+  R lam = gn ? (R)0 : (R)S.lam0;
+  R gnorm = (R)0;
   double cost = 0.0;
   bool need_jac = true, started = false, final_pass = false, last_at_x = true;
   int flags = 0;
@@ -824,12 +911,12 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         for (int i = tl; i < nq; i += T) x[i] = xn[i];
         tm.sync();
         cost = cn;
-        if (!gn) lam = fmaxf(lam / S.factor, S.lam_min);
+        if (!gn) lam = rmax(lam / (R)S.factor, (R)S.lam_min);
         need_jac = true;
         last_at_x = true;
-        if (gnorm < S.tol) { status = BR_IK_CONVERGED; break; }
+        if (gnorm < (R)S.tol) { status = BR_IK_CONVERGED; break; }
       } else {
-        lam = fminf(lam * S.factor, S.lam_max);
+        lam = rmin(lam * (R)S.factor, (R)S.lam_max);
         last_at_x = false;
       }
     }
@@ -845,19 +932,19 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       gnorm = build_normal(x, pose);
       need_jac = false;
     }
-    const float damp = gn ? S.gn_eps : lam;
-    // a failed float32 factorization is retried with diagonal regularisation 1e-6 .. 1e-1
+    const R damp = gn ? (R)S.gn_eps : lam;
+    // a failed factorization is retried with diagonal regularisation 1e-6 .. 1e-1
     bool ok = false;
-    float extra = 0.f;
+    R extra = (R)0;
     for (int k = 0; k < 7; ++k) {
       ok = solve(damp + extra);
       if (ok) break;
       flags |= BR_IK_FLAG_REGULARIZED;
-      extra = k == 0 ? 1e-6f : extra * 10.f;
+      extra = k == 0 ? (R)1e-6f : extra * (R)10;
     }
     if (!ok) {
 #pragma unroll 1
-      for (int i = tl; i < nv; i += T) delta[i] = 0.f;
+      for (int i = tl; i < nv; i += T) delta[i] = (R)0;
       tm.sync();
     }
     retract();
@@ -906,7 +993,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   tm.sync();
 }
 
-template <int T, bool kGeneral>
+template <int T, bool kGeneral, bool kF64>
 __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, int count, float* wsm, int lane,
                                          const uint32_t*& sched_ok) {
   const int team = lane / T;
@@ -914,14 +1001,15 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
   tm.tl = lane % T;
   tm.mask = (T == 32) ? 0xffffffffu : (((1u << T) - 1u) << (team * T));
   const br_tree_t& tree = P.trees[cls];
-  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T, tree.dof_entries, tree.dof_depth, tree.rounds);
+  const TeamLayout L(tree.njoints, tree.nq, tree.nv, P.b.max_targets, T, tree.dof_entries, tree.dof_depth, tree.rounds,
+                     kF64 ? 2 : 1);
   if (team < count) {
     const int prob = P.b.order[first + team];
-    solve_problem<T, kGeneral>(P, tree, prob, wsm + team * L.total, tm, sched_ok);
+    solve_problem<T, kGeneral, kF64>(P, tree, prob, wsm + team * L.total, tm, sched_ok);
   }
 }
 
-template <bool kGeneral>
+template <bool kGeneral, bool kF64>
 __global__ void __maxnreg__(128) lm_solve_kernel(const LmParams P) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -937,7 +1025,7 @@ __global__ void __maxnreg__(128) lm_solve_kernel(const LmParams P) {
     // One instantiation: 32-lane teams.  8- and 16-lane teams (several small problems per
     // warp) were measured slower on the mixed batch: three copies of this kernel body
     // overflow the instruction cache, and 32 lanes are the fastest per class on their own.
-    run_item<kLmTeam, kGeneral>(P, cls, first, count, wsm, lane, sched_ok);
+    run_item<kLmTeam, kGeneral, kF64>(P, cls, first, count, wsm, lane, sched_ok);
     __syncwarp();
   }
 }
@@ -959,7 +1047,7 @@ std::mutex g_lm_mu;  // guards the two per-device caches below
 // Dynamic shared memory each lm_solve_kernel variant has been allowed on each device
 // (cudaFuncAttributeMaxDynamicSharedMemorySize only ever raised, so a launch that
 // needs less than an earlier one still fits).  Shared by every entry point below.
-int g_smem_allowed[2][64] = {};
+int g_smem_allowed[4][64] = {};  // [float64 variant * 2 + general variant][device]
 }  // namespace
 
 // Argument checks of both LM entry points: BR_OK, an error, or kLmNothing when the batch
@@ -980,6 +1068,7 @@ static int lm_check(const br_ik_batch_t* batch, const br_ik_settings_t* settings
   if (settings->kernel < BR_KERNEL_L2 || settings->kernel > BR_KERNEL_TUKEY) return BR_EINVAL;
   if (settings->kernel != BR_KERNEL_L2 && !(settings->kernel_param > 0.f)) return BR_EINVAL;
   if (warps_per_cta < 1 || warps_per_cta > 32) return BR_EINVAL;
+  if (settings->precision != BR_PREC_F32 && settings->precision != BR_PREC_F64) return BR_EINVAL;
   return BR_OK;
 }
 
@@ -991,6 +1080,7 @@ static int lm_launch(const br_ik_batch_t& b, const br_ik_settings_t& settings, c
   p.s = settings;
   p.b = b;
   p.r = result;
+  const bool f64 = settings.precision == BR_PREC_F64;
   int warp_floats = 0;
   for (int c = 0; c < b.n_classes; ++c) {
     const int st = validate_tree(&b.trees[c]);
@@ -1001,7 +1091,8 @@ static int lm_launch(const br_ik_batch_t& b, const br_ik_settings_t& settings, c
     p.trees[c] = b.trees[c];
     p.team[c] = T;
     const br_tree_t& tc = b.trees[c];
-    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth, tc.rounds).total;
+    const int f = (32 / T) * TeamLayout(tc.njoints, tc.nq, tc.nv, b.max_targets, T, tc.dof_entries, tc.dof_depth,
+                                        tc.rounds, f64 ? 2 : 1).total;
     if (f > warp_floats) warp_floats = f;
   }
   p.warp_floats = warp_floats;
@@ -1017,10 +1108,11 @@ static int lm_launch(const br_ik_batch_t& b, const br_ik_settings_t& settings, c
   if ((int64_t)bytes > dev.max_smem_optin) return BR_ETOOBIG;
   bool general = b.target_kind != nullptr || settings.kernel != BR_KERNEL_L2;
   for (int c = 0; c < b.n_classes; ++c) general |= (b.trees[c].kinds & ~kBasicKinds) != 0 || b.trees[c].kinds == 0;
-  auto kern = general ? lm_solve_kernel<true> : lm_solve_kernel<false>;
+  auto kern = f64 ? (general ? lm_solve_kernel<true, true> : lm_solve_kernel<false, true>)
+                 : (general ? lm_solve_kernel<true, false> : lm_solve_kernel<false, false>);
   {
     std::lock_guard<std::mutex> lock(g_lm_mu);
-    int& have = g_smem_allowed[general][dev.device];
+    int& have = g_smem_allowed[(f64 ? 2 : 0) + (general ? 1 : 0)][dev.device];
     if ((int)bytes > have) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
       if (e != cudaSuccess) return (int)e;

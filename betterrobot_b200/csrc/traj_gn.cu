@@ -65,32 +65,34 @@ struct TrajParams {
 
 struct TrajLayout {
   // doubles
-  int x, xn, xref, dd, dr, g, delta, bl1, bl2, bdi, vy, vu, vw, Sb, sdi, rb, Jg, Js, rg, rs, jtjg, jtjs, pA, pB;
+  int x, xn, dd, dr, g, delta, bl1, bdi, Sb, sdi, rb, zb, Jg, Js, rg, rs, jtjg, jtjs, pA, pB, red;
   int total_doubles;
-  // ints / floats (in units of doubles)
-  int parent, jtype, idxq, idxv, dofq, cjoint, ckind, axis, place, caxis, anc, lower, upper, misc;
+  // 4-byte arrays (offsets in doubles)
+  int xref, parent, jtype, idxq, idxv, dofq, cjoint, ckind, axis, place, caxis, anc, lower, upper;
   int total;
   __host__ __device__ TrajLayout(int nj, int nq, int nv, int T, bool floating) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += (n + 1) & ~1; return r; };  // 16-byte aligned
-    x = take(T * nq); xn = take(T * nq); xref = take(T * nq); g = take(T * nv); delta = take(T * nv);
+    const int nb = 2 * nv;
+    x = take(T * nq); xn = take(T * nq); g = take(T * nv); delta = take(T * nv);
     // knot differences difference(x_t, x_{t+1}) and difference(xref_t, x_t) of the last
     // evaluated trajectory (kManifold variant; the other subtracts inline)
     dd = take(floating ? T * nv : 0); dr = take(floating ? T * nv : 0);
-    // per-DOF interior bands (index p * nv + i, p = knot - 1): L[p][p-1], L[p][p-2], 1 / D[p];
-    // solutions of P_i y = r, P_i u = h0, P_i w = hT
-    bl1 = take(T * nv); bl2 = take(T * nv); bdi = take(T * nv);
-    vy = take(T * nv); vu = take(T * nv); vw = take(T * nv);
-    Sb = take(4 * nv * nv); sdi = take(2 * nv); rb = take(2 * nv);   // boundary Schur complement
-    Jg = take(6 * nv); Js = take(6 * nv); rg = take(8); rs = take(8); jtjg = take(nv * nv); jtjs = take(nv * nv);
+    // per-DOF interior band factors (index p * nv + i, p = knot - 1): L[p][p-1] and 1 / D[p]
+    // (L[p][p-2] = c^2 / D[p-2] is rebuilt from 1 / D)
+    bl1 = take(T * nv); bdi = take(T * nv);
+    Sb = take(nb * (nb + 1) / 2); sdi = take(nb); rb = take(nb); zb = take(nb);  // boundary Schur complement
+    Jg = take(6 * nv); Js = take(6 * nv); rg = take(8); rs = take(8);
+    jtjg = take(nv * (nv + 1) / 2); jtjs = take(nv * (nv + 1) / 2);              // packed lower
     pA = take(16 * nj); pB = take(16 * nj);   // FK buffers of the two pose terms (goal, start)
+    red = take(32);                           // per-warp partial sums of the block reductions
     total_doubles = o;
-    // 4-byte arrays: count in doubles (2 per double)
     auto take4 = [&](int n) { int r = o; o += ((n + 3) & ~3) / 2; return r; };
+    xref = take4(T * nq);                     // float32, as given
     parent = take4(nj); jtype = take4(nj); idxq = take4(nj); idxv = take4(nj); dofq = take4(nv);
     cjoint = take4(nv); ckind = take4(nv);
-    axis = take4(4 * nj); place = take4(8 * nj); caxis = take4(4 * nv); anc = take4(4 * nj);
-    lower = take4(nq); upper = take4(nq); misc = take4(8);
+    axis = take4(4 * nj); place = take4(8 * nj); caxis = take4(4 * nv); anc = take4(8 * nj);
+    lower = take4(nq); upper = take4(nq);
     total = o;
   }
 };
@@ -122,35 +124,43 @@ __device__ __forceinline__ double fast_rsqrt(double x) {
   return y * fma(-0.5 * x * y, y, 1.5);
 }
 
-// pair decodes of the boundary Cholesky kept in registers (p < 32 * kTrajPairRegs); larger
-// boundary blocks decode the rest on the fly
-constexpr int kTrajPairRegs = 4;
+// packed lower-triangle index p -> (a, b), b <= a, p = a (a + 1) / 2 + b: approximate square
+// root, made exact by its two integer corrections
+__device__ __forceinline__ int2 tri_decode(int p) {
+  int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
+  if ((a + 1) * (a + 2) / 2 <= p) ++a;
+  if (a * (a + 1) / 2 > p) --a;
+  return make_int2(a, p - a * (a + 1) / 2);
+}
+__device__ __forceinline__ int tri_at(int r, int c) { return r * (r + 1) / 2 + c; }  // r >= c
+
+// Threads per trajectory: the per-DOF interior chains take one thread each (nv <= 64),
+// the two pose terms one warp each, everything else strides over the block.
+constexpr int kTrajThreads = 128;
 
 // kManifold: the tree has joints whose configuration is not their tangent coordinates
 // (free-flyer, spherical, planar, unbounded revolute): knot differences and the retraction go
 // through Model.difference / Model.integrate; otherwise they are q1 - q0 and q + v.
 template <bool kManifold>
-__global__ void traj_gn_kernel(const TrajParams P) {
+__global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams P) {
   extern __shared__ __align__(16) double sm[];
   const br_tree_t& tree = P.tree;
-  const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, T = P.T, lane = threadIdx.x;
+  const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, T = P.T;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NT = kTrajThreads, NW = kTrajThreads / kWarp;
   const int64_t traj = blockIdx.x;
   if (traj >= P.n) return;
   const TrajLayout L(nj, nq, nv, T, kManifold);
   double* x = sm + L.x;
   double* xn = sm + L.xn;
-  double* xref = sm + L.xref;
   double* g = sm + L.g;
   double* delta = sm + L.delta;
   double* bl1 = sm + L.bl1;
-  double* bl2 = sm + L.bl2;
   double* bdi = sm + L.bdi;
-  double* vy = sm + L.vy;
-  double* vu = sm + L.vu;
-  double* vw = sm + L.vw;
   double* Sb = sm + L.Sb;
   double* sdi = sm + L.sdi;
   double* rb = sm + L.rb;
+  double* zb = sm + L.zb;
   double* Jg = sm + L.Jg;
   double* Js = sm + L.Js;
   double* rg = sm + L.rg;
@@ -159,6 +169,8 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   double* jtjs = sm + L.jtjs;
   double* pA = sm + L.pA;
   double* pB = sm + L.pB;
+  double* red = sm + L.red;
+  float* xref = reinterpret_cast<float*>(sm + L.xref);
   int* parent = reinterpret_cast<int*>(sm + L.parent);
   int* jtype = reinterpret_cast<int*>(sm + L.jtype);
   int* idxq = reinterpret_cast<int*>(sm + L.idxq);
@@ -181,10 +193,10 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   const double wl = S.w_limit, wr = S.w_ref, wg = S.w_goal, ws = S.w_start;
   const bool has_start = P.start != nullptr && S.w_start > 0.f;
   const bool has_goal = S.w_goal > 0.f;
-  const int n = T * nv, nqT = T * nq;
+  const int n = T * nv, nqT = T * nq, nb = 2 * nv;
   const FastDiv divj(nj > 0 ? nj : 1), divv(nv > 0 ? nv : 1), divq(nq > 0 ? nq : 1);
 
-  for (int j = lane; j < nj; j += kWarp) {
+  for (int j = tid; j < nj; j += NT) {
     parent[j] = tree.parent[j];
     jtype[j] = tree.jtype[j];
     idxq[j] = tree.idx_q[j];
@@ -192,64 +204,58 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     for (int k = 0; k < 4; ++k) axis[4 * j + k] = tree.axis[4 * j + k];
     for (int k = 0; k < 8; ++k) place[8 * j + k] = tree.placement[8 * j + k];
   }
-  for (int k = lane; k < nv; k += kWarp) {
+  for (int k = tid; k < nv; k += NT) {
     cjoint[k] = tree.col_joint[k];
     ckind[k] = tree.col_kind[k];
     for (int m = 0; m < 4; ++m) caxis[4 * k + m] = tree.col_axis[4 * k + m];
   }
-  for (int i = lane; i < nq; i += kWarp) {
+  for (int i = tid; i < nq; i += NT) {
     lower[i] = tree.lower[i];
     upper[i] = tree.upper[i];
   }
-  __syncwarp();
-  for (int j = lane; j < nj; j += kWarp) {          // limits.py:36-48: nq == nv joints only
+  __syncthreads();
+  for (int j = tid; j < nj; j += NT) {              // limits.py:36-48: nq == nv joints only
     const int jt = jtype[j];
     const bool vec = joint_is_vector(jt);
     for (int k = 0; k < joint_nv(jt); ++k) dofq[idxv[j] + k] = vec ? idxq[j] + k : -1;
   }
   const float* x0 = P.x0 + traj * (int64_t)nqT;
   const float* xr = (P.xref ? P.xref : P.x0) + traj * (int64_t)nqT;
-  for (int i = lane; i < nqT; i += kWarp) {
+  for (int i = tid; i < nqT; i += NT) {
     x[i] = x0[i];
     xref[i] = xr[i];
   }
   const int fpar = tree.frame_parent[P.frame_id];
   const Pose fpl = load_pose8(tree.frame_placement + 8 * P.frame_id);
   const unsigned long long sup = tree.support[fpar];
-  Pose tgt_goal, tgt_start;
-  {
-    const float* tp = P.goal + traj * 7;
-    tgt_goal = Pose{f3(tp[0], tp[1], tp[2]), make_float4(tp[3], tp[4], tp[5], tp[6])};
-    if (has_start) {
-      const float* sp = P.start + traj * 7;
-      tgt_start = Pose{f3(sp[0], sp[1], sp[2]), make_float4(sp[3], sp[4], sp[5], sp[6])};
-    }
-  }
-  __syncwarp();
+  __syncthreads();
 
-  // packed lower-triangle pairs of the boundary Cholesky's trailing updates: p -> (a, b),
-  // b <= a, p = a (a + 1) / 2 + b, for the lane's first kTrajPairRegs pair indices
-  int spair[kTrajPairRegs];
+  auto warp_sum = [&](double v) {
 #pragma unroll
-  for (int i = 0; i < kTrajPairRegs; ++i) {
-    const int p = lane + kWarp * i;
-    int a = (int)((sqrtf(8.f * p + 1.f) - 1.f) * 0.5f);
-    if ((a + 1) * (a + 2) / 2 <= p) ++a;
-    if (a * (a + 1) / 2 > p) --a;
-    spair[i] = a | ((p - a * (a + 1) / 2) << 8);
-  }
-  // The two pose terms (goal at knot T-1: term 0, start at knot 0: term 1) are evaluated
-  // together, one per half-warp, when the tree has at most 16 joints; otherwise one after
-  // the other by the whole warp.  Term h uses FK buffers pA / pB + 8 nj h and ancA / ancB + nj h.
-  const bool halves = nj <= 16;
-  // float64 FK of knot t of trajectory `xs` on lanes sl, sl + SL, ...; returns the world poses
-  auto fk = [&](const double* xs, int t, int h, int sl, int SL) -> double* {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+  };
+  // sum over the block; every thread gets the same value (the warps' partials are added in
+  // warp order by every thread)
+  auto block_sum = [&](double v) -> double {
+    v = warp_sum(v);
+    __syncthreads();                                  // the previous reduction's reads are done
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s += red[w];
+    return s;
+  };
+  // float64 FK of knot t of trajectory `xs` by one warp (pose term h: buffers pA / pB + 8 nj h,
+  // ancA / ancB + nj h); returns the world poses
+  auto fk = [&](const double* xs, int t, int h) -> double* {
     const double* q = xs + t * nq;
     double* A = pA + 8 * nj * h;
     double* B = pB + 8 * nj * h;
     int* aA = ancA + nj * h;
     int* aB = ancB + nj * h;
-    for (int j = sl; j < nj; j += SL) {
+    for (int j = lane; j < nj; j += kWarp) {
       const Pose Pj = load_pose8(place + 8 * j);
       const DPose Lj = dlocal_transform(jtype[j], DPose{d3(Pj.t.x, Pj.t.y, Pj.t.z),
                                                         make_double4(Pj.q.x, Pj.q.y, Pj.q.z, Pj.q.w)},
@@ -259,7 +265,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     __syncwarp();
     for (int r = 0; r < tree.rounds; ++r) {
-      for (int j = sl; j < nj; j += SL) {
+      for (int j = lane; j < nj; j += kWarp) {
         const int a = aA[j];
         if (a >= 0) {
           std8d(B + 8 * j, dcompose(ldd8(A + 8 * a), ldd8(A + 8 * j)));
@@ -275,54 +281,49 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
     return A;
   };
-  // both pose terms at xs: xi (double, into rg / rs); with want_J also
-  // J = Jr^-1 blockdiag(R^T,R^T) J_lwa (6 x nv, into Jg / Js).  A term that is not in the
-  // problem (weight 0 or no start pose) is evaluated but not stored.
+  // both pose terms at xs, warp 0 the goal (knot T-1), warp 1 the start (knot 0): xi (into
+  // rg / rs); with want_J also J = Jr^-1 blockdiag(R^T,R^T) J_lwa (6 x nv, into Jg / Js).
+  // A term that is not in the problem (weight 0 or no start pose) is skipped.
   auto pose_terms = [&](const double* xs, bool want_J) __attribute__((always_inline)) {
-    const int npass = halves ? 1 : 2;
-    for (int pass = 0; pass < npass; ++pass) {
-      const int h = halves ? (lane >> 4) : pass;
-      const int sl = halves ? (lane & 15) : lane, SL = halves ? 16 : kWarp;
+    if (warp < 2) {
+      const int h = warp;
       const bool active = h == 0 ? has_goal : has_start;
-      const Pose& target = h == 0 ? tgt_goal : tgt_start;
-      double* r = h == 0 ? rg : rs;
-      double* J = h == 0 ? Jg : Js;
-      double* pose = fk(xs, h == 0 ? T - 1 : 0, halves ? h : 0, sl, SL);
-      const DPose Tee = dcompose(ldd8(pose + 8 * fpar),
-                                 DPose{d3(fpl.t.x, fpl.t.y, fpl.t.z), make_double4(fpl.q.x, fpl.q.y, fpl.q.z, fpl.q.w)});
-      double3 v, w;
-      dse3_log(dcompose(dinverse(DPose{d3(target.t.x, target.t.y, target.t.z),
-                                       make_double4(target.q.x, target.q.y, target.q.z, target.q.w)}), Tee), v, w);
-      if (active && sl == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
-      if (want_J && active) {
-        const DJrInv Jr = djr_inv_se3<9>(v, w);
-        const double4 qc = dqconj(Tee.q);
-        for (int k = sl; k < nv; k += SL) {
-          double3 ol = d3(0, 0, 0), oa = d3(0, 0, 0);
-          if ((sup >> cjoint[k]) & 1ull) {
-            const DPose Tj = ldd8(pose + 8 * cjoint[k]);
-            const double3 a = dqrot(Tj.q, d3(caxis[4 * k], caxis[4 * k + 1], caxis[4 * k + 2]));
-            double3 lin, ang;
-            if (ckind[k] == 0) {
-              lin = dcross(a, dsub(Tee.t, Tj.t));
-              ang = a;
-            } else {
-              lin = a;
-              ang = d3(0, 0, 0);
+      if (active) {
+        const float* tp = (h == 0 ? P.goal : P.start) + traj * 7;   // the term's target pose
+        const DPose target{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])};
+        double* r = h == 0 ? rg : rs;
+        double* J = h == 0 ? Jg : Js;
+        double* pose = fk(xs, h == 0 ? T - 1 : 0, h);
+        const DPose Tee = dcompose(ldd8(pose + 8 * fpar), DPose{d3(fpl.t.x, fpl.t.y, fpl.t.z),
+                                                                make_double4(fpl.q.x, fpl.q.y, fpl.q.z, fpl.q.w)});
+        double3 v, w;
+        dse3_log(dcompose(dinverse(target), Tee), v, w);
+        if (lane == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
+        if (want_J) {
+          const DJrInv Jr = djr_inv_se3<9>(v, w);
+          const double4 qc = dqconj(Tee.q);
+          for (int k = lane; k < nv; k += kWarp) {
+            double3 ol = d3(0, 0, 0), oa = d3(0, 0, 0);
+            if ((sup >> cjoint[k]) & 1ull) {
+              const DPose Tj = ldd8(pose + 8 * cjoint[k]);
+              const double3 a = dqrot(Tj.q, d3(caxis[4 * k], caxis[4 * k + 1], caxis[4 * k + 2]));
+              double3 lin, ang;
+              if (ckind[k] == 0) {
+                lin = dcross(a, dsub(Tee.t, Tj.t));
+                ang = a;
+              } else {
+                lin = a;
+                ang = d3(0, 0, 0);
+              }
+              djr_inv_apply(Jr, dqrot(qc, lin), dqrot(qc, ang), ol, oa);
             }
-            djr_inv_apply(Jr, dqrot(qc, lin), dqrot(qc, ang), ol, oa);
+            J[0 * nv + k] = ol.x; J[1 * nv + k] = ol.y; J[2 * nv + k] = ol.z;
+            J[3 * nv + k] = oa.x; J[4 * nv + k] = oa.y; J[5 * nv + k] = oa.z;
           }
-          J[0 * nv + k] = ol.x; J[1 * nv + k] = ol.y; J[2 * nv + k] = ol.z;
-          J[3 * nv + k] = oa.x; J[4 * nv + k] = oa.y; J[5 * nv + k] = oa.z;
         }
       }
-      __syncwarp();
     }
-  };
-  auto warp_sum = [&](double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+    __syncthreads();
   };
   // dd[t] = difference(xs_t, xs_{t+1}) (t < T-1) and dr[t] = difference(xref_t, xs_t)
   // (model.py:176-190): free-flyer log(q_a^-1 q_b) (free_flyer.py:53-57), spherical
@@ -330,46 +331,46 @@ __global__ void traj_gn_kernel(const TrajParams P) {
   // unbounded revolute and planar joints (revolute.py:233-237, planar.py:70-76)
   auto knot_differences = [&](const double* xs) {
     const int npair = 2 * T - 1;
-    for (int e = lane; e < npair * nj; e += kWarp) {
+    for (int e = tid; e < npair * nj; e += NT) {
       const int pi = divj.div(e), j = e - pi * nj;
       const int jt = jtype[j], nvj = joint_nv(jt);
       if (nvj == 0) continue;
-      const double* qa;
-      const double* qb;
-      double* out;
-      if (pi < T - 1) {
-        qa = xs + pi * nq; qb = xs + (pi + 1) * nq; out = dd + pi * nv;
-      } else {
-        const int t = pi - (T - 1);
-        qa = xref + t * nq; qb = xs + t * nq; out = dr + t * nv;
-      }
       const int iq = idxq[j], iv = idxv[j];
+      // configurations a -> b of the pair: (x_t, x_{t+1}) or (xref_t, x_t)
+      const bool ref = pi >= T - 1;
+      const int t = ref ? pi - (T - 1) : pi;
+      const double* qbp = xs + (ref ? t : t + 1) * nq + iq;
+      const double* qap = xs + t * nq + iq;
+      const float* qrp = xref + t * nq + iq;
+      auto qa = [&](int k) -> double { return ref ? (double)qrp[k] : qap[k]; };
+      auto qb = [&](int k) -> double { return qbp[k]; };
+      double* out = (ref ? dr : dd) + t * nv;
       if (jt == BR_JOINT_FREE_FLYER) {
-        const DPose a{d3(qa[iq], qa[iq + 1], qa[iq + 2]), make_double4(qa[iq + 3], qa[iq + 4], qa[iq + 5], qa[iq + 6])};
-        const DPose b{d3(qb[iq], qb[iq + 1], qb[iq + 2]), make_double4(qb[iq + 3], qb[iq + 4], qb[iq + 5], qb[iq + 6])};
+        const DPose a{d3(qa(0), qa(1), qa(2)), make_double4(qa(3), qa(4), qa(5), qa(6))};
+        const DPose b{d3(qb(0), qb(1), qb(2)), make_double4(qb(3), qb(4), qb(5), qb(6))};
         double3 v, w;
         dse3_log(dcompose(dinverse(a), b), v, w);
         out[iv] = v.x; out[iv + 1] = v.y; out[iv + 2] = v.z;
         out[iv + 3] = w.x; out[iv + 4] = w.y; out[iv + 5] = w.z;
       } else if (jt == BR_JOINT_SPHERICAL) {
-        const double3 w = dso3_log(dqnormalize(dqmul(dqconj(make_double4(qa[iq], qa[iq + 1], qa[iq + 2], qa[iq + 3])),
-                                                     make_double4(qb[iq], qb[iq + 1], qb[iq + 2], qb[iq + 3]))));
+        const double3 w = dso3_log(dqnormalize(dqmul(dqconj(make_double4(qa(0), qa(1), qa(2), qa(3))),
+                                                     make_double4(qb(0), qb(1), qb(2), qb(3)))));
         out[iv] = w.x; out[iv + 1] = w.y; out[iv + 2] = w.z;
       } else if (jt == BR_JOINT_PLANAR || jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
         const int k = jt == BR_JOINT_PLANAR ? 2 : 0;
-        if (k) { out[iv] = qb[iq] - qa[iq]; out[iv + 1] = qb[iq + 1] - qa[iq + 1]; }
-        out[iv + k] = atan2(qb[iq + k + 1], qb[iq + k]) - atan2(qa[iq + k + 1], qa[iq + k]);
+        if (k) { out[iv] = qb(0) - qa(0); out[iv + 1] = qb(1) - qa(1); }
+        out[iv + k] = atan2(qb(k + 1), qb(k)) - atan2(qa(k + 1), qa(k));
       } else {
-        for (int k = 0; k < nvj; ++k) out[iv + k] = qb[iq + k] - qa[iq + k];
+        for (int k = 0; k < nvj; ++k) out[iv + k] = qb(k) - qa(k);
       }
     }
-    __syncwarp();
+    __syncthreads();
   };
   // xn_t = integrate(x_t, delta_t) per knot (model.py:160-174): free-flyer normalize(q . exp(v))
   // (free_flyer.py:47-51), spherical normalize(q . exp(w)) (spherical.py:52-56), unbounded
   // revolute / planar angle atan2(s, c) + v as (cos, sin) (revolute.py:223-231, planar.py:61-68)
   auto retract_knots = [&]() {
-    for (int e = lane; e < T * nj; e += kWarp) {
+    for (int e = tid; e < T * nj; e += NT) {
       const int t = divj.div(e), j = e - t * nj;
       const int jt = jtype[j], nvj = joint_nv(jt);
       if (nvj == 0) continue;
@@ -404,49 +405,49 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     double acc = 0.0;
     pose_terms(xs, false);
     if (kManifold) knot_differences(xs);
-    for (int e = lane; e < (T - 2) * nv; e += kWarp) {          // smoothness.py:118-125
+    for (int e = tid; e < (T - 2) * nv; e += NT) {              // smoothness.py:118-125
       const double a = kManifold ? c * (dd[e + nv] - dd[e]) : c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
       acc += a * a;
     }
     if (kManifold) {
-      for (int e = lane; e < nqT; e += kWarp) {                 // limits.py:56-62
+      for (int e = tid; e < nqT; e += NT) {                     // limits.py:56-62
         const int i = divq.mod(e);
         const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
         acc += wl * wl * (lo * lo + hi * hi);
       }
-      for (int e = lane; e < n; e += kWarp) acc += wr * wr * dr[e] * dr[e];   // regularization.py:143-152
+      for (int e = tid; e < n; e += NT) acc += wr * wr * dr[e] * dr[e];   // regularization.py:143-152
     } else {                                                    // nq == nv: one pass for both
-      for (int e = lane; e < n; e += kWarp) {
+      for (int e = tid; e < n; e += NT) {
         const int i = divv.mod(e);
         const double lo = fmax((double)lower[i] - xs[e], 0.0), hi = fmax(xs[e] - (double)upper[i], 0.0);
-        const double d = xs[e] - xref[e];
+        const double d = xs[e] - (double)xref[e];
         acc += wl * wl * (lo * lo + hi * hi) + wr * wr * d * d;
       }
     }
-    acc = warp_sum(acc);
+    acc = block_sum(acc);
     double pc = 0.0;
     for (int k = 0; k < 6; ++k) {
       if (has_goal) pc += wg * wg * rg[k] * rg[k];
       if (has_start) pc += ws * ws * rs[k] * rs[k];
     }
-    __syncwarp();
     return 0.5 * (acc + pc);
   };
-  // J^T J of the pose terms and g = J^T r at x; returns |g|
+  // J^T J of the pose terms (packed lower) and g = J^T r at x; returns |g|
   auto build = [&]() -> double {
     pose_terms(x, true);
-    for (int e = lane; e < nv * nv; e += kWarp) {
-      const int i = divv.div(e), j = e - i * nv;
+    const int npk = nv * (nv + 1) / 2;
+    for (int e = tid; e < npk; e += NT) {
+      const int2 ab = tri_decode(e);
       double a = 0.0, b = 0.0;
       for (int r = 0; r < 6; ++r) {
-        if (has_goal) a += Jg[r * nv + i] * Jg[r * nv + j];
-        if (has_start) b += Js[r * nv + i] * Js[r * nv + j];
+        if (has_goal) a += Jg[r * nv + ab.x] * Jg[r * nv + ab.y];
+        if (has_start) b += Js[r * nv + ab.x] * Js[r * nv + ab.y];
       }
       jtjg[e] = wg * wg * a;
       jtjs[e] = ws * ws * b;
     }
     double gg = 0.0;
-    for (int e = lane; e < n; e += kWarp) {
+    for (int e = tid; e < n; e += NT) {
       const int t = divv.div(e), i = e - t * nv;
       double acc = 0.0;
       // acceleration rows s = t, t-1, t-2 with coefficients +1, -2, +1 at knot t (the
@@ -464,7 +465,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         if (xq < (double)lower[iq]) acc -= wl * wl * ((double)lower[iq] - xq);
         if (xq > (double)upper[iq]) acc += wl * wl * (xq - (double)upper[iq]);
       }
-      acc += wr * wr * (kManifold ? dr[e] : x[e] - xref[e]);
+      acc += wr * wr * (kManifold ? dr[e] : x[e] - (double)xref[e]);
       if (has_goal && t == T - 1)
         for (int r = 0; r < 6; ++r) acc += wg * wg * Jg[r * nv + i] * rg[r];
       if (has_start && t == 0)
@@ -472,8 +473,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       g[e] = acc;
       gg += acc * acc;
     }
-    gg = warp_sum(gg);
-    __syncwarp();
+    gg = block_sum(gg);
     return sqrt(gg);
   };
   // bands of J^T J + damp I at x (DOF i): diagonal at knot t, H[(t+1,i),(t,i)], and
@@ -499,149 +499,144 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     if (t - 1 >= 0 && t <= T - 2) b += -2.0;
     return c2 * b;
   };
-  // solve (J^T J + damp I) delta = -g; false when a pivot is not positive
+  // interior columns of the boundary knots: h0 = H[(t, i), (0, i)], hT = H[(t, i), (T-1, i)]
+  auto h0_at = [&](int t) -> double { return t == 1 ? hoff1(0) : (t == 2 ? c2 : 0.0); };
+  auto hT_at = [&](int t) -> double { return t == T - 2 ? hoff1(T - 2) : (t == T - 3 ? c2 : 0.0); };
+  // solve (J^T J + damp I) delta = -g; false when a pivot is not positive.
+  // Interior knots 1..T-2 of DOF i form the pentadiagonal P_i = L D L^T (thread i).  With
+  // z = L^-1 v, the Schur complement terms are h^T P_i^-1 k = sum_p z_h[p] z_k[p] / D[p], so
+  // one forward pass gives S = H_bb - H_bI P^-1 H_Ib and rb = -g_b - H_bI P^-1 (-g_I) without
+  // storing P^-1 h0 and P^-1 hT; after the boundary solve, the interior step is one more
+  // banded solve with right-hand side -g_I - h0 delta_0 - hT delta_{T-1}.
   auto newton_solve = [&](double damp) -> bool {
-    const int m = T - 2, nb = 2 * nv;
+    const int m = T - 2;
     bool good = true;
-    // interior diagonals H[(p+1, i), (p+1, i)] by all lanes first (vy is free until the
-    // forward solve); the off-diagonal H[(p+1), (p)] of the interior is -4 c2
-    for (int e = lane; e < m * nv; e += kWarp) {
-      const int pp = divv.div(e);
-      vy[e] = hdiag(pp + 1, e - pp * nv, damp);
-    }
-    __syncwarp();
-    const double h1 = -4.0 * c2;
-    if (lane < nv) {
-      const int i = lane;
-      // banded LDL^T of the interior of DOF i: L[p][p-2] = c2 / D[p-2],
-      // L[p][p-1] = (H[p][p-1] - c2 L[p-1][p-2]) / D[p-1], D[p] = H[p][p] - L[p][p-1]^2 D[p-1] - L[p][p-2] c2
+    double suu = 0.0, suw = 0.0, sww = 0.0, suy = 0.0, swy = 0.0;
+    const double h1 = -4.0 * c2;                    // H[(p+1), (p)] inside the interior
+    if (tid < nv) {
+      const int i = tid;
       double d1 = 0.0, di1 = 0.0, di2 = 0.0, l1p = 0.0;
+      double y1 = 0, y2 = 0, u1 = 0, u2 = 0, w1 = 0, w2 = 0;
       for (int p = 0; p < m; ++p) {
+        const int t = p + 1;
         const double l2 = (p >= 2) ? c2 * di2 : 0.0;
         const double l1 = (p >= 1) ? (h1 - c2 * l1p) * di1 : 0.0;
-        const double dp = vy[p * nv + i] - l1 * l1 * d1 - l2 * c2;
+        const double dp = hdiag(t, i, damp) - l1 * l1 * d1 - l2 * c2;
         if (!(dp > 0.0)) { good = false; break; }
         const double dip = fast_rcp(dp);
-        bl1[p * nv + i] = l1; bl2[p * nv + i] = l2; bdi[p * nv + i] = dip;
+        bl1[p * nv + i] = l1; bdi[p * nv + i] = dip;
+        const double y = -g[t * nv + i] - l1 * y1 - l2 * y2;
+        const double u = h0_at(t) - l1 * u1 - l2 * u2;
+        const double w = hT_at(t) - l1 * w1 - l2 * w2;
+        suu += u * u * dip; suw += u * w * dip; sww += w * w * dip;
+        suy += u * y * dip; swy += w * y * dip;
         di2 = di1; di1 = dip; d1 = dp; l1p = l1;
-      }
-      if (good) {
-        // forward L z = (r, h0, hT), r = -g on the interior; h0 / hT: the columns of knots 0 / T-1
-        double y1 = 0, y2 = 0, u1 = 0, u2 = 0, w1 = 0, w2 = 0;
-#pragma unroll 2
-        for (int p = 0; p < m; ++p) {
-          const int t = p + 1;
-          const double l1 = bl1[p * nv + i], l2 = bl2[p * nv + i];
-          const double h0 = (t == 1) ? hoff1(0) : (t == 2 ? c2 : 0.0);
-          const double hT = (t == T - 2) ? hoff1(T - 2) : (t == T - 3 ? c2 : 0.0);
-          const double y = -g[t * nv + i] - l1 * y1 - l2 * y2;
-          const double u = h0 - l1 * u1 - l2 * u2;
-          const double w = hT - l1 * w1 - l2 * w2;
-          vy[p * nv + i] = y; vu[p * nv + i] = u; vw[p * nv + i] = w;
-          y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
-        }
-        // backward D L^T v = z
-        y1 = y2 = u1 = u2 = w1 = w2 = 0;
-#pragma unroll 2
-        for (int p = m - 1; p >= 0; --p) {
-          const double di = bdi[p * nv + i];
-          const double l1n = (p + 1 < m) ? bl1[(p + 1) * nv + i] : 0.0;   // L[p+1][p]
-          const double l2n = (p + 2 < m) ? bl2[(p + 2) * nv + i] : 0.0;   // L[p+2][p]
-          const double y = vy[p * nv + i] * di - l1n * y1 - l2n * y2;
-          const double u = vu[p * nv + i] * di - l1n * u1 - l2n * u2;
-          const double w = vw[p * nv + i] * di - l1n * w1 - l2n * w2;
-          vy[p * nv + i] = y; vu[p * nv + i] = u; vw[p * nv + i] = w;
-          y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
-        }
+        y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
       }
     }
-    if (!__all_sync(0xffffffffu, good)) return false;
-    // boundary block H_bb: b = i for (knot 0, DOF i), nv + i for (knot T-1, DOF i)
-    const bool two = nb <= 16;                                     // two rows per pass, else one
-    for (int r0 = 0; r0 < nb; r0 += two ? 2 : 1) {
-      const int r = r0 + (two ? (lane >> 4) : 0), cc = two ? (lane & 15) : lane;
-      if (r >= nb || cc >= nb) continue;
+    if (__syncthreads_or(!good)) return false;
+    // boundary block H_bb, packed lower: b = i for (knot 0, DOF i), nv + i for (knot T-1, DOF i)
+    const int nbp = nb * (nb + 1) / 2;
+    for (int e = tid; e < nbp; e += NT) {
+      const int2 rc = tri_decode(e);
+      const int r = rc.x, cc = rc.y;
       const int kr = r >= nv, kc = cc >= nv, ir = r - kr * nv, ic = cc - kc * nv;
       double h = 0.0;
       if (kr == kc) {
-        if (kr == 0 && has_start) h = jtjs[ir * nv + ic];
-        if (kr == 1 && has_goal) h = jtjg[ir * nv + ic];
+        const int pe = ir >= ic ? tri_at(ir, ic) : tri_at(ic, ir);
+        if (kr == 0 && has_start) h = jtjs[pe];
+        if (kr == 1 && has_goal) h = jtjg[pe];
         if (ir == ic) h += hdiag(kr ? T - 1 : 0, ir, damp);
       } else if (ir == ic && T == 3) {
         h = c2;                                                    // row 0 couples knots 0 and 2
       }
-      Sb[r * nb + cc] = h;
+      Sb[e] = h;
     }
-    __syncwarp();
-    if (lane < nv) {
-      // S = H_bb - H_bI P^-1 H_Ib and rb = -g_b - H_bI y: h0 is nonzero at interior p = 0, 1,
-      // hT at p = m-1, m-2
-      const int i = lane;
-      const double a0 = hoff1(0), a1 = (m >= 2) ? c2 : 0.0;           // h0[0], h0[1]
-      const double b0 = hoff1(T - 2), b1 = (m >= 2) ? c2 : 0.0;       // hT[m-1], hT[m-2]
-      auto at = [&](const double* v, int p) { return v[p * nv + i]; };
-      const double h0u = a0 * at(vu, 0) + (m >= 2 ? a1 * at(vu, 1) : 0.0);
-      const double h0w = a0 * at(vw, 0) + (m >= 2 ? a1 * at(vw, 1) : 0.0);
-      const double hTw = b0 * at(vw, m - 1) + (m >= 2 ? b1 * at(vw, m - 2) : 0.0);
-      const double h0y = a0 * at(vy, 0) + (m >= 2 ? a1 * at(vy, 1) : 0.0);
-      const double hTy = b0 * at(vy, m - 1) + (m >= 2 ? b1 * at(vy, m - 2) : 0.0);
-      Sb[i * nb + i] -= h0u;
-      Sb[i * nb + nv + i] -= h0w;
-      Sb[(nv + i) * nb + i] -= h0w;
-      Sb[(nv + i) * nb + nv + i] -= hTw;
-      rb[i] = -g[i] - h0y;
-      rb[nv + i] = -g[(T - 1) * nv + i] - hTy;
+    __syncthreads();
+    if (tid < nv) {
+      const int i = tid;
+      Sb[tri_at(i, i)] -= suu;
+      Sb[tri_at(nv + i, i)] -= suw;
+      Sb[tri_at(nv + i, nv + i)] -= sww;
+      rb[i] = -g[i] - suy;
+      rb[nv + i] = -g[(T - 1) * nv + i] - swy;
     }
-    __syncwarp();
+    __syncthreads();
     for (int k = 0; k < nb; ++k) {                                  // chol(S), lower, in place
-      const double dkk = Sb[k * nb + k];
-      if (!(dkk > 0.0)) return false;
+      const double dkk = Sb[tri_at(k, k)];
+      if (!(dkk > 0.0)) return false;                               // every thread read the same value
       const double inv = fast_rsqrt(dkk);
-      const double sk = dkk * inv;
-      __syncwarp();
-      if (lane > k && lane < nb) Sb[lane * nb + k] *= inv;
-      if (lane == k) { Sb[k * nb + k] = sk; sdi[k] = inv; }
-      __syncwarp();
+      __syncthreads();
+      for (int r = k + 1 + tid; r < nb; r += NT) Sb[tri_at(r, k)] *= inv;
+      if (tid == 0) { Sb[tri_at(k, k)] = dkk * inv; sdi[k] = inv; }
+      __syncthreads();
       // trailing update S[r][cc] -= L[r][k] L[cc][k], k < cc <= r < nb, as packed pairs
-      // (r - k - 1, cc - k - 1) = pair p of the lane (decoded once, p = lane + 32 i)
       const int np = (nb - k - 1) * (nb - k) / 2;
-#pragma unroll
-      for (int i = 0; i < kTrajPairRegs; ++i) {
-        if (lane + kWarp * i < np) {
-          const int r = (spair[i] & 0xff) + k + 1, cc = (spair[i] >> 8) + k + 1;
-          Sb[r * nb + cc] -= Sb[r * nb + k] * Sb[cc * nb + k];
+      for (int pp = tid; pp < np; pp += NT) {
+        const int2 ab = tri_decode(pp);
+        const int r = ab.x + k + 1, cc = ab.y + k + 1;
+        Sb[tri_at(r, cc)] -= Sb[tri_at(r, k)] * Sb[tri_at(cc, k)];
+      }
+      __syncthreads();
+    }
+    // z = S^-1 rb
+    if (nb <= kWarp) {
+      if (warp == 0) {                      // lane b owns entry b; one finished entry broadcast per step
+        double v = (lane < nb) ? rb[lane] : 0.0;
+        for (int j = 0; j < nb; ++j) {
+          const double zj = __shfl_sync(0xffffffffu, v, j) * sdi[j];
+          if (lane == j) v = zj;
+          else if (lane > j && lane < nb) v -= Sb[tri_at(lane, j)] * zj;
         }
+        for (int j = nb - 1; j >= 0; --j) {
+          const double zj = __shfl_sync(0xffffffffu, v, j) * sdi[j];
+          if (lane == j) v = zj;
+          else if (lane < j) v -= Sb[tri_at(j, lane)] * zj;
+        }
+        if (lane < nb) zb[lane] = v;
       }
-      for (int pp = lane + kWarp * kTrajPairRegs; pp < np; pp += kWarp) {   // nb > 17 only
-        int a = (int)((sqrtf(8.f * pp + 1.f) - 1.f) * 0.5f);
-        if ((a + 1) * (a + 2) / 2 <= pp) ++a;
-        if (a * (a + 1) / 2 > pp) --a;
-        const int r = a + k + 1, cc = pp - a * (a + 1) / 2 + k + 1;
-        Sb[r * nb + cc] -= Sb[r * nb + k] * Sb[cc * nb + k];
+    } else {                                // column-oriented substitutions over the block
+      for (int j = 0; j < nb; ++j) {        // L y = rb (rb overwritten by the partial sums)
+        const double yj = rb[j] * sdi[j];
+        for (int r = j + 1 + tid; r < nb; r += NT) rb[r] -= Sb[tri_at(r, j)] * yj;
+        if (tid == 0) zb[j] = yj;
+        __syncthreads();
       }
-      __syncwarp();
+      for (int j = nb - 1; j >= 0; --j) {   // L^T z = y (zb overwritten in place)
+        const double zj = zb[j] * sdi[j];
+        __syncthreads();
+        for (int r = tid; r < j; r += NT) zb[r] -= Sb[tri_at(j, r)] * zj;
+        if (tid == 0) zb[j] = zj;
+        __syncthreads();
+      }
     }
-    // z = S^-1 rb: lane b owns entry b; one finished entry broadcast per step
-    double v = (lane < nb) ? rb[lane] : 0.0;
-    for (int j = 0; j < nb; ++j) {
-      const double zj = __shfl_sync(0xffffffffu, v, j) * sdi[j];
-      if (lane == j) v = zj;
-      else if (lane > j && lane < nb) v -= Sb[lane * nb + j] * zj;
+    __syncthreads();
+    // interior step of DOF i: P_i d = -g_I - h0 z(knot 0) - hT z(knot T-1); forward into delta,
+    // then backward in place
+    if (tid < nv) {
+      const int i = tid;
+      const double z0 = zb[i], zT = zb[nv + i];
+      delta[i] = z0;
+      delta[(T - 1) * nv + i] = zT;
+      double y1 = 0, y2 = 0;
+      for (int p = 0; p < m; ++p) {
+        const int t = p + 1;
+        const double l1 = bl1[p * nv + i], l2 = (p >= 2) ? c2 * bdi[(p - 2) * nv + i] : 0.0;
+        const double y = -g[t * nv + i] - h0_at(t) * z0 - hT_at(t) * zT - l1 * y1 - l2 * y2;
+        delta[t * nv + i] = y;
+        y2 = y1; y1 = y;
+      }
+      y1 = y2 = 0;
+      for (int p = m - 1; p >= 0; --p) {
+        const double di = bdi[p * nv + i];
+        const double l1n = (p + 1 < m) ? bl1[(p + 1) * nv + i] : 0.0;   // L[p+1][p]
+        const double l2n = (p + 2 < m) ? c2 * di : 0.0;                  // L[p+2][p] = c2 / D[p]
+        const double y = delta[(p + 1) * nv + i] * di - l1n * y1 - l2n * y2;
+        delta[(p + 1) * nv + i] = y;
+        y2 = y1; y1 = y;
+      }
     }
-    for (int j = nb - 1; j >= 0; --j) {
-      const double zj = __shfl_sync(0xffffffffu, v, j) * sdi[j];
-      if (lane == j) v = zj;
-      else if (lane < j) v -= Sb[j * nb + lane] * zj;
-    }
-    if (lane < nv) delta[lane] = v;
-    else if (lane < nb) delta[(T - 1) * nv + lane - nv] = v;
-    __syncwarp();
-    // interior: y - u z(knot 0) - w z(knot T-1)
-    for (int e = lane; e < m * nv; e += kWarp) {
-      const int i = divv.mod(e);
-      delta[nv + e] = vy[e] - vu[e] * delta[i] - vw[e] * delta[(T - 1) * nv + i];
-    }
-    __syncwarp();
+    __syncthreads();
     return true;
   };
 
@@ -662,22 +657,22 @@ __global__ void traj_gn_kernel(const TrajParams P) {
         ok = newton_solve((lm ? lam : (double)S.gn_eps) + extra);
       }
       if (!ok) {
-        for (int e = lane; e < n; e += kWarp) delta[e] = 0.0;
-        __syncwarp();
+        for (int e = tid; e < n; e += NT) delta[e] = 0.0;
+        __syncthreads();
       }
     }
     if (kManifold) {                                               // Model.integrate per knot (trajopt.py:159-169)
       retract_knots();
     } else {
-      for (int e = lane; e < n; e += kWarp) xn[e] = x[e] + delta[e];
+      for (int e = tid; e < n; e += NT) xn[e] = x[e] + delta[e];
     }
-    __syncwarp();
+    __syncthreads();
     const double cn = cost_of(xn);
     if (!isfinite(cn)) flags |= BR_IK_FLAG_NONFINITE;
     bool accept = !lm || cn < cost;
     if (accept) {
-      for (int e = lane; e < nqT; e += kWarp) x[e] = xn[e];
-      __syncwarp();
+      for (int e = tid; e < nqT; e += NT) x[e] = xn[e];
+      __syncthreads();
       cost = cn;
       need = true;
       if (lm) lam = fmax(lam / S.factor, (double)S.lam_min);
@@ -687,10 +682,10 @@ __global__ void traj_gn_kernel(const TrajParams P) {
     }
   }
   float* xo = P.x + traj * (int64_t)nqT;
-  for (int e = lane; e < nqT; e += kWarp) xo[e] = (float)x[e];
+  for (int e = tid; e < nqT; e += NT) xo[e] = (float)x[e];
   if (P.goal_grad && has_goal) {
     pose_terms(x, false);
-    if (lane == 0) {
+    if (tid == 0) {
       const double3 v = d3(rg[0], rg[1], rg[2]);
       const double3 w = d3(rg[3], rg[4], rg[5]);
       const DJrInv Jl = djr_inv_se3<20>(dscale(v, -1.0), dscale(w, -1.0));   // Jl^-1(xi) = Jr^-1(-xi)
@@ -702,7 +697,7 @@ __global__ void traj_gn_kernel(const TrajParams P) {
       o[3] = (float)(k * ga.x); o[4] = (float)(k * ga.y); o[5] = (float)(k * ga.z);
     }
   }
-  if (lane == 0) {
+  if (tid == 0) {
     P.iters[traj] = it;
     P.status[traj] = status | (flags << 8);
     P.cost[traj] = (float)cost;
@@ -754,6 +749,6 @@ extern "C" int br_trajopt_solve(const br_tree_t* tree, int32_t frame_id, int64_t
     conf = (int)bytes;
   }
   if (n_traj > 0x7fffffff) return BR_ETOOBIG;
-  kern<<<(unsigned)n_traj, kWarp, bytes, (cudaStream_t)stream>>>(p);
+  kern<<<(unsigned)n_traj, kTrajThreads, bytes, (cudaStream_t)stream>>>(p);
   return (int)cudaGetLastError();
 }

@@ -65,6 +65,12 @@ class OptimizerConfig:
     lam_max: float = 1e8
     gn_eps: float = 1e-8
     kernel_param: float | None = None  # None: the kernel class's default (Huber 1.0, Cauchy 1.0, Tukey 4.685)
+    # arithmetic of the Jacobian, J^T J, J^T r and the factorization ("f32": fastest; "f64": the
+    # float64 reference's iterates); the iterate, FK, residual and cost are float64 in both
+    precision: Literal["f32", "f64"] = "f32"
+
+
+PRECISIONS = {"f32": 0, "f64": 1}  # BR_PREC_*
 
 
 # OptimizerConfig.kernel -> BR_KERNEL_*, and the default parameter of each kernel class
@@ -129,6 +135,9 @@ def settings_from(cost_cfg: IKCostConfig, opt: OptimizerConfig) -> IKSettings:
         raise ValueError(f"Unknown kernel {opt.kernel!r}; expected one of {sorted(KERNELS)}")
     s.kernel = KERNELS[opt.kernel]
     s.kernel_param = KERNEL_DEFAULTS.get(opt.kernel, 0.0) if opt.kernel_param is None else float(opt.kernel_param)
+    if opt.precision not in PRECISIONS:
+        raise ValueError(f"Unknown precision {opt.precision!r}; expected 'f32' or 'f64'")
+    s.precision = PRECISIONS[opt.precision]
     return s
 
 

@@ -176,7 +176,7 @@ BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joi
 #define BR_IK_CONVERGED 0       /* status & 0xff                                   */
 #define BR_IK_MAXITER 1
 #define BR_IK_FLAG_NONFINITE 1  /* (status >> 8) bits: a non-finite cost was seen   */
-#define BR_IK_FLAG_REGULARIZED 2 /* float32 LDL^T needed extra diagonal damping     */
+#define BR_IK_FLAG_REGULARIZED 2 /* the LDL^T needed extra diagonal damping          */
 #define BR_IK_FLAG_BADTREE 4    /* tree's dof_entries / dof_depth below its DOF tree: not solved */
 
 /* Solver settings: LevenbergMarquardt(lam0, factor, tol) with Adaptive damping
@@ -190,7 +190,12 @@ typedef struct br_ik_settings {
     int32_t optimizer;          /* BR_OPT_LM or BR_OPT_GN                          */
     int32_t kernel;             /* BR_KERNEL_*: IRLS row weights (levenberg_marquardt.py:27-44) */
     float kernel_param;         /* Huber delta / Cauchy c / Tukey c (optim/kernels/*.py)      */
+    int32_t precision;          /* BR_PREC_*: arithmetic of the Jacobian, J^T J, J^T r and the
+                                   factorization (the iterate, FK, residual and cost are float64
+                                   in both)                                                   */
 } br_ik_settings_t;
+#define BR_PREC_F32 0           /* float32 normal equations (the default, fastest)            */
+#define BR_PREC_F64 1           /* float64 normal equations: the float64 reference's iterates */
 
 /* A packed batch of independent IK problems over up to 8 robot classes. */
 typedef struct br_ik_batch {
@@ -251,8 +256,9 @@ BR_API int br_lm_solve(const br_ik_batch_t* batch, const br_ik_settings_t* setti
 BR_API int br_lm_solve_noalloc(const br_ik_batch_t* batch, const br_ik_settings_t* settings,
                                br_ik_result_t* result, int32_t warps_per_cta, void* stream);
 
-/* Shared-memory floats one problem of `tree` with `max_targets` targets needs
- * (for choosing team sizes and warps per CTA). No reference counterpart. */
+/* Shared-memory floats one problem of `tree` with `max_targets` targets needs in the
+ * float32 variant (BR_PREC_F32; the float64 variant needs more, and the solve entry
+ * points size their launches themselves). No reference counterpart. */
 BR_API int64_t br_lm_team_floats(const br_tree_t* tree, int32_t max_targets);
 
 /* ==== pose loss through FK and its adjoint ================================ */
@@ -283,7 +289,7 @@ BR_API int br_pose_loss_backward(const br_tree_t* tree, const float* q, const fl
 
 /* ==== batched trajectory optimisation (Gauss-Newton / LM) ================ */
 #define BR_MAX_TRAJ_KNOTS 128
-#define BR_MAX_TRAJ_NV 16
+#define BR_MAX_TRAJ_NV 64
 
 /* Cost stack weights (CostStack item weights) and solver settings.  Terms with
  * weight 0 are left out. */
@@ -299,14 +305,16 @@ typedef struct br_traj_settings {
 } br_traj_settings_t;
 
 /*
- * Solve n_traj independent trajectories of `knots` configurations each, one warp
- * per trajectory, with the Newton step in nested-dissection order (per-DOF
- * pentadiagonal interior, dense Schur complement on the end knots).  x0 / x_ref / x
+ * Solve n_traj independent trajectories of `knots` configurations each, one CTA
+ * of 128 threads per trajectory, with the Newton step in nested-dissection order
+ * (per-DOF pentadiagonal interior, dense Schur complement on the end knots).  x0 / x_ref / x
  * are [n_traj, knots, nq] (x_ref NULL = x0), goal / start are [n_traj, 7] poses of
  * frame `frame_id` (start may be NULL).  goal_grad (NULL or [n_traj, 6]) receives
  * d(final cost)/d(eps) for the goal perturbed as T_goal * exp(eps).  Every joint kind
  * (knot differences and the retraction through Model.difference / Model.integrate);
- * nv <= BR_MAX_TRAJ_NV.
+ * nv <= BR_MAX_TRAJ_NV; BR_ETOOBIG when one trajectory's working set (about
+ * 8 (7 knots nv + 2 knots nq + 2 nv^2) bytes) exceeds the device's shared memory per
+ * CTA (e.g. the 36-DOF humanoid fits up to 64 knots).
  * Replaces solve_trajopt with the knot parameterisation and its dense LM / GN
  * (src/better_robot/tasks/trajopt.py:84-230) on the goal / start / acceleration /
  * limit / reference-trajectory stack.

@@ -313,7 +313,7 @@ def make_adjoint(spec, B, seed, out):
 
 
 def make_trajopt(spec, N, T, seed, out, dt=0.05, w_goal=1.0, w_start=1.0, w_accel=1e-2, w_limit=0.1,
-                 w_ref=1e-3, tol=1e-6, max_iter=30, spread=1.0):
+                 w_ref=1e-3, tol=1e-6, max_iter=30, spread=1.0, frame="ee"):
     """Reference solve_trajopt (knots, GaussNewton) on the config-4 stack, float64."""
     from better_robot.costs.stack import CostStack
     from better_robot.kinematics.forward import forward_kinematics
@@ -325,7 +325,7 @@ def make_trajopt(spec, N, T, seed, out, dt=0.05, w_goal=1.0, w_start=1.0, w_acce
     m = reference_model(spec)
     mine = syn.model_from_spec(spec, dtype=D)
     q_start, q_goal = syn.trajopt_endpoints(mine, N, seed, spread)
-    fid = m.frame_id("ee")
+    fid = m.frame_id(frame)
     res = {"X": [], "iters": [], "converged": [], "residual": []}
     goals, starts = [], []
     for n in range(N):
@@ -351,7 +351,8 @@ def make_trajopt(spec, N, T, seed, out, dt=0.05, w_goal=1.0, w_start=1.0, w_acce
     np.savez_compressed(out, q_start=q_start.numpy(), q_goal=q_goal.numpy(), goal=np.stack(goals),
                         start=np.stack(starts), X=np.stack(res["X"]), iters=np.array(res["iters"]),
                         converged=np.array(res["converged"]), residual=np.stack(res["residual"]),
-                        settings=np.array([T, dt, w_goal, w_start, w_accel, w_limit, w_ref, tol, max_iter]))
+                        settings=np.array([T, dt, w_goal, w_start, w_accel, w_limit, w_ref, tol, max_iter]),
+                        frame=np.array(frame))
 
 
 def main():
@@ -371,6 +372,10 @@ def main():
         return
     if only == ["trajopt_mixed"]:
         make_trajopt(syn.mixed_spec(), 3, 12, 45, os.path.join(HERE, "trajopt_mixed.npz"), spread=0.3)
+        return
+    if only == ["trajopt_humanoid"]:
+        make_trajopt(syn.humanoid_spec(), 2, 10, 49, os.path.join(HERE, "trajopt_humanoid.npz"), spread=0.3,
+                     frame="track0")
         return
     make_lie(os.path.join(HERE, "lie.npz"))
     make_lie_ops(os.path.join(HERE, "lie_ops.npz"))
@@ -396,6 +401,8 @@ def main():
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))
     make_trajopt(syn.floating_chain_spec(), 3, 12, 43, os.path.join(HERE, "trajopt_floating.npz"))
     make_trajopt(syn.mixed_spec(), 3, 12, 45, os.path.join(HERE, "trajopt_mixed.npz"), spread=0.3)
+    make_trajopt(syn.humanoid_spec(), 2, 10, 49, os.path.join(HERE, "trajopt_humanoid.npz"), spread=0.3,
+                 frame="track0")
 
 
 if __name__ == "__main__":

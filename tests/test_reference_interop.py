@@ -106,3 +106,35 @@ def test_reference_except_clauses_catch_errors_raised_here():
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "caught" in r.stdout
+
+
+def test_solve_trajopt_reads_reference_cost_stack():
+    """The solve_trajopt facade reads a CostStack built from BetterRobot's own residual classes
+    (the stack of ``tasks/trajopt.py``'s docstring and of the golden solves) into the kernel's
+    weights and targets."""
+    import torch as _t
+    from better_robot.costs.stack import CostStack
+    from better_robot.optim.optimizers.gauss_newton import GaussNewton
+    from better_robot.residuals import AccelerationResidual, JointPositionLimit, PoseResidual, TimeIndexedResidual
+    from better_robot.residuals.regularization import ReferenceTrajectoryResidual
+    from make_golden import reference_model
+    from betterrobot_b200.trajopt import _stack_to_config
+    m = reference_model(SPECS["chain7"])
+    T = 8
+    X0 = _t.zeros(T, m.nq, dtype=_t.float64)
+    Tg = _t.tensor([0.1, 0.2, 0.3, 0.0, 0.0, 0.0, 1.0], dtype=_t.float64)
+    Ts = _t.tensor([0.0, 0.2, 0.3, 0.0, 0.0, 0.0, 1.0], dtype=_t.float64)
+    fid = m.frame_id("ee")
+    st = CostStack()
+    st.add("goal", TimeIndexedResidual(PoseResidual(frame_id=fid, target=Tg), t_idx=T - 1), weight=2.0)
+    st.add("start", TimeIndexedResidual(PoseResidual(frame_id=fid, target=Ts), t_idx=0), weight=0.5)
+    st.add("accel", AccelerationResidual(m, dt=0.1), weight=1e-2)
+    for t in range(T):
+        st.add(f"limits_t{t}", TimeIndexedResidual(JointPositionLimit(m), t_idx=t, name=f"limits_t{t}"), weight=0.1)
+    st.add("ref", ReferenceTrajectoryResidual(m, X0.clone()), weight=1e-3)
+    cfg, f, goal, start, q_ref = _stack_to_config(m, st, T, GaussNewton(tol=1e-7), 40)
+    assert f == fid and _t.equal(goal, Tg) and _t.equal(start, Ts) and _t.equal(q_ref, X0)
+    assert (cfg.w_goal, cfg.w_start, cfg.w_accel, cfg.w_limit, cfg.w_ref) == (2.0, 0.5, 1e-2, 0.1, 1e-3)
+    assert (cfg.dt, cfg.optimizer, cfg.tol, cfg.max_iter) == (0.1, "gn", 1e-7, 40)
+    st.set_active("ref", False)
+    assert _stack_to_config(m, st, T, GaussNewton(), 40)[0].w_ref == 0.0

@@ -49,18 +49,20 @@ def _gpu(m, fid, goal, start, X0, cfg):
                                      start=torch.from_numpy(start).float().cuda(), cfg=cfg)
 
 
-@pytest.mark.parametrize("fixture", ["trajopt_chain7.npz", "trajopt_floating.npz", "trajopt_mixed.npz"])
+@pytest.mark.parametrize("fixture", ["trajopt_chain7.npz", "trajopt_floating.npz", "trajopt_mixed.npz",
+                                     "trajopt_humanoid.npz"])
 def test_reference_solve_trajopt_golden(fixture):
-    """The reference's float64 solve_trajopt: the 7-DOF chain, a floating-base chain, and the
+    """The reference's float64 solve_trajopt: the 7-DOF chain, a floating-base chain, the
     robot with planar, translation, spherical and unbounded-revolute joints (knots moved by
-    Model.integrate, acceleration and reference residuals through Model.difference)."""
+    Model.integrate, acceleration and reference residuals through Model.difference), and the
+    36-DOF free-flyer humanoid (a 72 x 72 boundary system over four warps)."""
     g = np.load(os.path.join(GOLDEN, fixture))
     T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
     spec = {"trajopt_chain7.npz": syn.chain_spec(), "trajopt_floating.npz": syn.floating_chain_spec(),
-            "trajopt_mixed.npz": syn.mixed_spec()}[fixture]
+            "trajopt_mixed.npz": syn.mixed_spec(), "trajopt_humanoid.npz": syn.humanoid_spec()}[fixture]
     m = syn.model_from_spec(spec)
     m64 = syn.model_from_spec(spec, dtype=torch.float64)
-    fid = m.frame_id("ee")
+    fid = m.frame_id(str(g["frame"]) if "frame" in g else "ee")
     X0 = np.repeat(g["q_start"][:, None, :], int(T), 1)
     cfg = btr.TrajOptConfig(dt=float(dt), w_goal=float(wg), w_start=float(ws), w_accel=float(wa), w_limit=float(wl),
                             w_ref=float(wr), tol=float(tol), max_iter=int(mi))
@@ -134,12 +136,12 @@ def test_goal_gradient_envelope_vs_resolved_cost():
     assert (rel[ok] <= 2e-2).all(), rel
 
 
-def _vs_oracle(spec, N, T, seed):
+def _vs_oracle(spec, N, T, seed, frame="ee", spread=0.5):
     """N trajectories of T knots on ``spec`` against the float64 oracle (same verdicts on >= 90%,
     trajectories within 1e-4 and costs within 1e-6 + 1e-4 relative where both converged)."""
     m, m64 = syn.model_from_spec(spec), syn.model_from_spec(spec, dtype=torch.float64)
-    fid = m.frame_id("ee")
-    qs, qg = syn.trajopt_endpoints(m64, N, seed, 0.5)
+    fid = m.frame_id(frame)
+    qs, qg = syn.trajopt_endpoints(m64, N, seed, spread)
     oMi, _ = K.forward_kinematics(m64, qg.numpy())
     goal = K.frame_placements(m64, oMi, [fid])[:, 0]
     oMi, _ = K.forward_kinematics(m64, qs.numpy())
@@ -165,19 +167,80 @@ def test_floating_base_vs_oracle():
     _vs_oracle(syn.floating_chain_spec(), 16, 24, 47)
 
 
+def test_humanoid_vs_oracle():
+    """The 36-DOF free-flyer humanoid (the FK + Jacobian robot), 6 trajectories x 16 knots
+    (576 variables each), against the float64 oracle."""
+    _vs_oracle(syn.humanoid_spec(), 6, 16, 57, frame="track0", spread=0.3)
+
+
 @pytest.mark.parametrize("spec,N,T", [(syn.chain_spec(seed=11, n=16, name="chain16"), 16, 16),
-                                      (syn.chain_spec(), 8, 128)], ids=["nv16", "knots128"])
+                                      (syn.chain_spec(seed=13, n=62, name="chain62"), 3, 12),
+                                      (syn.chain_spec(), 8, 128)], ids=["nv16", "nv62", "knots128"])
 def test_size_limits_vs_oracle(spec, N, T):
-    """The trajectory limits: nv = 16 = BR_MAX_TRAJ_NV (18 joints: pose terms on the whole
-    warp, a 32 x 32 boundary system) and T = 128 = BR_MAX_TRAJ_KNOTS knots."""
+    """The trajectory limits: nv = 16 (a 32 x 32 boundary system: one warp's substitutions),
+    nv = 62 (64 joints, the tree table's limit: a 124 x 124 boundary system over the whole
+    CTA) and T = 128 = BR_MAX_TRAJ_KNOTS knots."""
     _vs_oracle(spec, N, T, 53)
 
 
 def test_trajopt_rejects_oversized_trees_and_bad_shapes():
-    m = syn.model_from_spec(syn.humanoid_spec())     # nv = 36 > BR_MAX_TRAJ_NV
-    X0 = torch.zeros(2, 8, m.nq, device="cuda")
+    m = syn.model_from_spec(syn.humanoid_spec())     # 128 knots of 36 DOFs: above shared memory
+    X0 = torch.zeros(2, 128, m.nq, device="cuda")
+    X0[..., 6] = 1.0
     with pytest.raises(Exception):
-        btr.solve_trajopt_batched(m, 0, torch.zeros(2, 7, device="cuda"), X0)
+        btr.solve_trajopt_batched(m, m.frame_id("track0"), torch.zeros(2, 7, device="cuda"), X0)
     mc = syn.model_from_spec(syn.chain_spec())
     with pytest.raises(btr.ShapeError):
         btr.solve_trajopt_batched(mc, 0, torch.zeros(3, 7, device="cuda"), torch.zeros(2, 8, mc.nq, device="cuda"))
+
+
+class _Item:
+    def __init__(self, residual, weight):
+        self.residual, self.weight, self.active = residual, weight, True
+
+
+class _Stack:
+    """The shape of BetterRobot's CostStack that solve_trajopt reads (``items``: name -> item)."""
+
+    def __init__(self):
+        self.items = {}
+
+    def add(self, name, residual, weight=1.0):
+        self.items[name] = _Item(residual, weight)
+
+
+def _ref_like(name, **attrs):
+    """An object whose class is named like a BetterRobot residual / optimizer, with its attributes."""
+    return type(name, (), {})() if not attrs else type(name, (), dict(attrs))()
+
+
+def test_solve_trajopt_facade_matches_reference_golden():
+    """``solve_trajopt(model, horizon=, dt=, initial_q_traj=, cost_stack=, optimizer=)`` with the
+    stack the reference's golden solves used (objects shaped like BetterRobot's, the reference
+    itself not being importable here) returns the reference's trajectories."""
+    g = np.load(os.path.join(GOLDEN, "trajopt_chain7.npz"))
+    T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
+    T = int(T)
+    m = syn.model_from_spec(syn.chain_spec())
+    fid = m.frame_id("ee")
+    for n in range(len(g["X"])):
+        X0 = torch.from_numpy(np.repeat(g["q_start"][n][None], T, 0))
+        st = _Stack()
+        pose = lambda target: _ref_like("PoseResidual", frame_id=fid, target=torch.from_numpy(target),  # noqa: E731
+                                        pos_weight=1.0, ori_weight=1.0)
+        st.add("goal", _ref_like("TimeIndexedResidual", inner=pose(g["goal"][n]), t_idx=T - 1), float(wg))
+        st.add("start", _ref_like("TimeIndexedResidual", inner=pose(g["start"][n]), t_idx=0), float(ws))
+        st.add("accel", _ref_like("AccelerationResidual", dt=float(dt), weight=1.0), float(wa))
+        for t in range(T):
+            st.add(f"limits_t{t}", _ref_like("TimeIndexedResidual", inner=_ref_like("JointPositionLimit", weight=1.0),
+                                             t_idx=t), float(wl))
+        st.add("ref", _ref_like("ReferenceTrajectoryResidual", q_ref=X0.clone(), weight=1.0), float(wr))
+        r = btr.solve_trajopt(m, horizon=T, dt=float(dt), initial_q_traj=X0.cuda(), cost_stack=st,
+                              optimizer=_ref_like("GaussNewton", tol=float(tol), eps=1e-8), max_iter=int(mi))
+        assert r.converged == bool(g["converged"][n])
+        assert r.trajectory.q.shape == (1, T, m.nq)
+        assert np.abs(r.trajectory.q[0].cpu().double().numpy() - g["X"][n]).max() <= 1e-4
+    with pytest.raises(NotImplementedError):
+        st.add("other", _ref_like("CollisionResidual"), 1.0)
+        btr.solve_trajopt(m, horizon=T, dt=float(dt), initial_q_traj=X0.cuda(), cost_stack=st,
+                          optimizer=_ref_like("GaussNewton", tol=1e-6, eps=1e-8))
