@@ -547,12 +547,13 @@ def _cpu_worker(args):
     return reached, time.perf_counter() - t0, len(idx)
 
 
-def cpu_baseline(seed: int, per_class=(12, 9, 9), cores: int | None = None, pool=None):
-    """Serial float64 LM (one problem per call, like solve_ik) on a stratified sample, all host cores."""
+def cpu_baseline(seed: int, per_class=(77, 77, 102), cores: int | None = None, pool=None, draw: int = 0):
+    """Serial float64 LM (one problem per call, like solve_ik) on a stratified sample, all host cores.
+    ``draw`` picks another stratified sample of the same workload."""
     cores = cores or len(os.sched_getaffinity(0))
     names = [n for n, _ in class_specs()]
     frac = {"humanoid": 0.3, "dual_arm": 0.3, "chain7": 0.4}
-    rng = np.random.default_rng(seed + 5)
+    rng = np.random.default_rng(seed + 5 + 1000 * draw)
     wl = {c["name"]: c for c in make_workload(N_PROBLEMS, seed)}
     tasks, weights = [], {}
     for name, n in zip(names, per_class):
@@ -587,6 +588,83 @@ def cpu_baseline(seed: int, per_class=(12, 9, 9), cores: int | None = None, pool
 
 
 # ---------------------------------------------------------------------------
+# CPU: the float64 oracle ports of configs 1, 2 and 4 on host cores
+# ---------------------------------------------------------------------------
+CPU_FKJ_SAMPLE = 2048      # configurations per process and repetition
+CPU_ADJ_SAMPLE = 2048
+CPU_TRAJ_KNOTS = 64
+
+
+def _cpu_leg_worker(args):
+    """One process of a CPU leg: returns (units done, seconds)."""
+    import torch
+    torch.set_num_threads(1)
+    os.environ["OMP_NUM_THREADS"] = "1"
+    from betterrobot_b200 import synthetic as syn
+    from oracle import adjoint as A, kinematics as K, trajopt as ot
+    leg, seed, reps = args
+    if leg == "trajopt":
+        mc = syn.model_from_spec(syn.chain_spec(), dtype=torch.float64)
+        fid = mc.frame_id("ee")
+        qs, qg = syn.trajopt_endpoints(mc, 1, 81 + seed, spread=0.5)
+        oMi, _ = K.forward_kinematics(mc, qg.numpy())
+        goal = K.frame_placements(mc, oMi, [fid])[:, 0]
+        oMi, _ = K.forward_kinematics(mc, qs.numpy())
+        start = K.frame_placements(mc, oMi, [fid])[:, 0]
+        X0 = np.repeat(qs.numpy()[:, None, :], CPU_TRAJ_KNOTS, 1)
+        t0 = time.perf_counter()
+        ot.solve(mc, X0, fid, goal, start, ot.TrajSettings(max_iter=30))
+        return 1, time.perf_counter() - t0
+    m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
+    fids = syn.op_frame_ids(m64)
+    B = CPU_FKJ_SAMPLE if leg == "fkj" else CPU_ADJ_SAMPLE
+    q = syn.random_q(m64, B, seed, rev_range=2.5, base_translation=1.0).numpy()
+    tg = syn.random_targets(B, len(fids), seed + 1).double().numpy()
+    w = np.random.default_rng(seed + 2).uniform(0.5, 2.0, size=len(fids))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        if leg == "fkj":      # forward_kinematics(compute_frames=True) + 12 x get_frame_jacobian (LWA)
+            oMi, _ = K.forward_kinematics(m64, q)
+            K.frame_placements(m64, oMi, fids)
+            for f in fids:
+                K.frame_jacobian(m64, oMi, q, f)
+        else:                 # the pose loss and its gradient w.r.t. q (what autograd returns)
+            A.pose_loss(m64, q, fids, tg, w)
+            A.pose_loss_grad(m64, q, fids, tg, w)
+    return B * reps, time.perf_counter() - t0
+
+
+def cpu_legs(pool, cores: int) -> dict:
+    """Configs 1, 2, 4 through the float64 oracle ports on the host: all cores (one process per
+    core) and, for configs 1 and 2, one thread."""
+    out = {}
+    for leg, reps, unit in (("fkj", 4, "configs/s"), ("adjoint", 2, "configs/s")):
+        n1, s1 = pool.apply(_cpu_leg_worker, ((leg, 100, reps),))
+        # all cores: the workers compute concurrently; the rate is the units of all of them over the
+        # slowest one's compute time (process start-up and imports excluded)
+        res = pool.map(_cpu_leg_worker, [(leg, 200 + i, reps) for i in range(cores)], chunksize=1)
+        n = sum(r[0] for r in res)
+        d = {"value": n / max(r[1] for r in res), "unit": unit, "cores": cores, "value_1thread": n1 / s1,
+             "kind": "port"}
+        if leg == "fkj":
+            d["gbs"] = d["value"] * FKJ_BYTES_PER_CONFIG / 1e9
+            d["sample"] = (f"humanoid FK + 12 frame Jacobians (local_world_aligned), float64 numpy oracle, "
+                           f"{CPU_FKJ_SAMPLE} configurations x {reps} per process")
+        else:
+            d["sample"] = (f"humanoid 12-frame pose loss + its gradient w.r.t. q, float64 numpy oracle "
+                           f"(reverse sweep pinned to the reference's autograd), {CPU_ADJ_SAMPLE} configurations x "
+                           f"{reps} per process")
+        out[leg] = d
+    res = pool.map(_cpu_leg_worker, [("trajopt", i, 1) for i in range(cores)], chunksize=1)
+    out["trajopt"] = {"value": sum(r[0] for r in res) / max(r[1] for r in res), "unit": "trajectories/s",
+                      "cores": cores,
+                      "kind": "port", "sample": f"{cores} chain7 trajectories x {CPU_TRAJ_KNOTS} knots, one per "
+                      "process, float64 oracle GN with the dense (T nv)^2 normal equations of solve_trajopt, "
+                      "<= 30 iterations"}
+    return out
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -618,11 +696,12 @@ def main():
         steps = []
         cb = None
         cores = len(os.sched_getaffinity(0))
-        n = max(cores, 10)  # at least one problem per host core, in the mix's proportions
+        n = max(2 * cores, 96)  # per step: >= 2 problems per host core, in the mix's proportions
         per_class = (round(0.3 * n), round(0.3 * n), n - 2 * round(0.3 * n))  # humanoid, dual_arm, chain7
         with mp.get_context("spawn").Pool(cores) as pool:
             for i in range(warmup + args.steps):
-                cb = cpu_baseline(seed=7, per_class=per_class, cores=cores, pool=pool)
+                # every step draws another stratified sample of the 8,192-problem mix
+                cb = cpu_baseline(seed=7, per_class=per_class, cores=cores, pool=pool, draw=i)
                 if i >= warmup:
                     steps.append(cb)
         v = float(np.mean([s["value"] for s in steps]))
@@ -654,9 +733,13 @@ def main():
             r = bench_adjoint(args.steps, warmup)
         print(json.dumps({"section": args.only, **r}), flush=True)
         return
-    cpu = None
+    cpu = legs = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(seed=7)  # before any CUDA work in this process (spawned workers)
+        # before any CUDA work in this process (spawned workers)
+        cores = len(os.sched_getaffinity(0))
+        with mp.get_context("spawn").Pool(cores) as pool:
+            cpu = cpu_baseline(seed=7, cores=cores, pool=pool)
+            legs = cpu_legs(pool, cores)
     import torch
     world, rank, local = dist_setup()
     peak, peak_kind = _peaks()
@@ -701,6 +784,7 @@ def main():
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": "solves/s", "cores": cpu["cores"], "kind": "port",
                                 "sample": cpu["sample"]}
+        line["cpu_baselines_other_configs"] = legs
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -39,6 +39,16 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
 // Wait for every cp.async this thread issued (the data is then visible to this thread;
 // other threads see it after a barrier).
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// One 4-byte global -> shared copy (both addresses 4-byte aligned).
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gsrc) : "memory");
+}
+// Close the group of this thread's cp.async issued since the last commit.
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most N of this thread's committed groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_groups() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 
 // Warp-cooperative copy of `n` floats from shared to global (fallback when the
 // destination block is not 16-byte aligned or its size is not a multiple of 16).

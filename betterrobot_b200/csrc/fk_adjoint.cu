@@ -46,7 +46,7 @@ struct LossParams {
 struct LossLayout {
   int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, fparent, fplace, fmask;
   int cta_floats;
-  int q, poseT, poseQ, anc, F, gv, stage;
+  int in0, in1, poseT, poseQ, anc, F, gv, stage;
   int warp_floats;
   __host__ __device__ LossLayout(int nj, int nq, int nv, int nf) {
     int o = 0;
@@ -56,7 +56,10 @@ struct LossLayout {
     fparent = take(nf); fplace = take(8 * nf); fmask = take(2 * nf);
     cta_floats = o;
     o = 0;
-    q = take(nq); poseT = take(4 * nj); poseQ = take(4 * nj); anc = take(nj);
+    // the inputs of one configuration (q, stored oMi, targets), double buffered: the next
+    // configuration's are copied in (cp.async) while this one is computed
+    in0 = take(nq + 7 * nj + 7 * nf); in1 = take(nq + 7 * nj + 7 * nf);
+    poseT = take(4 * nj); poseQ = take(4 * nj); anc = take(nj);
     F = take(8 * nf);     // world wrench per frame (f.xyz, pad, tau.xyz, pad)
     gv = take(nv);        // dL/dv
     stage = take(nj * 7); // oMi staging (store mode)
@@ -113,7 +116,6 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
   __syncthreads();
 
   float* w = smem + L.cta_floats + warp * L.warp_floats;
-  float* wq = w + L.q;
   float* wpT = w + L.poseT;
   float* wpQ = w + L.poseQ;
   int* wanc = reinterpret_cast<int*>(w + L.anc);
@@ -121,16 +123,41 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
   float* wg = w + L.gv;
   float* wst = w + L.stage;
   const int64_t stride = (int64_t)gridDim.x * wpc;
-  for (int64_t b = (int64_t)blockIdx.x * wpc + warp; b < p.batch; b += stride) {
-    const float* qb = p.q + b * nq;
-    for (int i = lane; i < nq; i += kWarp) wq[i] = __ldg(qb + i);
+  const bool stored = kBackward && p.oMi_in;
+  const int o_pose = nq, o_tgt = nq + (stored ? 7 * nj : 0);   // offsets in an input buffer
+  // queue the copies of configuration bb's inputs into `dst` (one commit group per call,
+  // empty past the end of the batch): 4-byte cp.async, the rows are 4-byte aligned only
+  auto prefetch = [&](int64_t bb, float* dst) {
+    if (bb < p.batch) {
+      const float* qb = p.q + bb * nq;
+      for (int i = lane; i < nq; i += kWarp) cp_async4(dst + i, qb + i);
+      if (stored) {
+        const float* ob = p.oMi_in + bb * (int64_t)nj * 7;
+        for (int i = lane; i < nj * 7; i += kWarp) cp_async4(dst + o_pose + i, ob + i);
+      }
+      const float* tb = p.targets + bb * (int64_t)nf * 7;
+      for (int i = lane; i < nf * 7; i += kWarp) cp_async4(dst + o_tgt + i, tb + i);
+    }
+    cp_async_commit();
+  };
+  float* cur = w + L.in0;                  // this configuration's inputs; the other buffer: the next's
+  float* nxt = w + L.in1;
+  int64_t b = (int64_t)blockIdx.x * wpc + warp;
+  prefetch(b, cur);
+  for (; b < p.batch; b += stride) {
+    __syncwarp();                          // every lane is done with the buffer refilled next
+    prefetch(b + stride, nxt);
+    cp_async_wait_groups<1>();             // this configuration's copies (all but the newest group)
     __syncwarp();
-    if (kBackward && p.oMi_in) {
-      const float* ob = p.oMi_in + b * (int64_t)nj * 7;
+    const float* wq = cur;
+    const float* wtg = cur + o_tgt;
+    float* t = cur; cur = nxt; nxt = t;
+    if (stored) {
+      const float* ob = wq + o_pose;
       for (int i = lane; i < nj * 7; i += kWarp) {
         const int j = i / 7, c = i - 7 * j;
-        if (c < 3) wpT[4 * j + c] = __ldg(ob + i);
-        else wpQ[4 * j + c - 3] = __ldg(ob + i);
+        if (c < 3) wpT[4 * j + c] = ob[i];
+        else wpQ[4 * j + c - 3] = ob[i];
       }
       __syncwarp();
     } else {
@@ -175,9 +202,8 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
     float acc = 0.f;
     for (int f = lane; f < nf; f += kWarp) {
       const Pose Tf = compose(load_split(wpT, wpQ, s_fparent[f]), load_pose8(s_fplace + 8 * f));
-      const float* tp = p.targets + (b * nf + f) * 7;
-      const Pose Tt{f3(__ldg(tp), __ldg(tp + 1), __ldg(tp + 2)),
-                    make_float4(__ldg(tp + 3), __ldg(tp + 4), __ldg(tp + 5), __ldg(tp + 6))};
+      const float* tp = wtg + 7 * f;
+      const Pose Tt{f3(tp[0], tp[1], tp[2]), make_float4(tp[3], tp[4], tp[5], tp[6])};
       float3 v, om;
       se3_log(compose(inverse(Tt), Tf), v, om);
       const float wf = __ldg(p.weights + (p.weights_per_config ? b * nf + f : f));
@@ -275,6 +301,7 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
     }
     __syncwarp();
   }
+  cp_async_wait_groups<0>();               // the (empty) last group
 }
 
 template <bool kBackward>

@@ -183,7 +183,8 @@ def make_kin(name, spec, batch, seed, base_t, out):
 
 
 def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, factor=10.0, pos_w=1.0, ori_w=1.0,
-                 limit_w=0.1, rest_w=0.01, optimizer="lm", kernel="l2", kinds=None):
+                 limit_w=0.1, rest_w=0.01, optimizer="lm", kernel="l2", kinds=None, damping="adaptive",
+                 gn_eps=1e-8):
     """One float64 solve through the reference's own stack (``tasks/ik.py:191-258``)."""
     from better_robot.costs.stack import CostStack
     from better_robot.kinematics.forward import forward_kinematics
@@ -192,6 +193,7 @@ def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, facto
     from better_robot.optim.problem import LeastSquaresProblem
     from better_robot.optim.solvers.cholesky import Cholesky
     from better_robot.optim.strategies.adaptive import Adaptive
+    from better_robot.optim.strategies.constant import Constant
     from better_robot.residuals.base import ResidualState
     from better_robot.residuals.limits import JointPositionLimit
     from better_robot.residuals.pose import PoseResidual
@@ -222,10 +224,12 @@ def reference_lm(m, frame_names, targets, q0, *, tol, max_iter, lam0=1e-3, facto
     from better_robot.tasks.ik import _make_robust_kernel
     k = _make_robust_kernel(kernel)   # solve_ik's own factory: None for "l2"
     if optimizer == "lm":
+        # solve_ik's OptimizerConfig.damping (tasks/ik.py:136-147): Adaptive, or Constant (lambda fixed)
+        strat = Constant(lam=lam0) if damping == "constant" else Adaptive(lam0=lam0, factor=factor)
         st = LevenbergMarquardt(lam0=lam0, factor=factor, tol=tol).minimize(
-            prob, max_iter=max_iter, linear_solver=Cholesky(), kernel=k, strategy=Adaptive(lam0=lam0, factor=factor))
+            prob, max_iter=max_iter, linear_solver=Cholesky(), kernel=k, strategy=strat)
     else:
-        st = GaussNewton(tol=tol).minimize(prob, max_iter=max_iter, linear_solver=Cholesky(), kernel=k)
+        st = GaussNewton(tol=tol, eps=gn_eps).minimize(prob, max_iter=max_iter, linear_solver=Cholesky(), kernel=k)
     return st
 
 
@@ -256,7 +260,8 @@ def make_ik(case, spec, frame_names, P, seed, start, out, **kw):
                         settings=np.array([kw.get("lam0", 0), kw.get("factor", 0), kw["tol"], kw["max_iter"],
                                            kw.get("limit_w", 0.1), kw.get("rest_w", 0.01)]),
                         optimizer=np.array(kw.get("optimizer", "lm")), kernel=np.array(kw.get("kernel", "l2")),
-                        kinds=np.array(kw.get("kinds") or ["pose"] * len(frame_names)))
+                        kinds=np.array(kw.get("kinds") or ["pose"] * len(frame_names)),
+                        damping=np.array(kw.get("damping", "adaptive")), gn_eps=np.array(kw.get("gn_eps", 1e-8)))
 
 
 def make_ik_kernels(chain, dual, hum, lm):
@@ -289,6 +294,18 @@ def make_ik_kinds(chain, dual, hum, lm):
     make_ik("humanoid_mixed", hum, ["track0", "track2", "track4"], 4, 31, "noisy",
             os.path.join(HERE, "ik_humanoid_mixed.npz"), max_iter=100, rest_w=1e-3,
             kinds=["pose", "position", "orientation"], **lm)
+
+
+def make_ik_damping_and_singular(chain, dual):
+    """LM with Constant damping (solve_ik's damping="constant": Constant() keeps lambda = 1e-4,
+    optim/strategies/constant.py:9-25); and GN without damping (eps = 0) on the dual-arm with one
+    left-arm target and no limit / rest terms: the right arm's Jacobian columns are zero, so
+    J^T J is exactly singular, torch.linalg.cholesky fails and Cholesky.solve falls back to
+    lstsq (optim/solvers/cholesky.py:14-20) in every iteration."""
+    make_ik("chain7_constant", chain, ["ee"], 8, 33, "noisy", os.path.join(HERE, "ik_chain7_constant.npz"),
+            max_iter=60, tol=1e-6, lam0=1e-4, factor=2.0, damping="constant")
+    make_ik("dual_arm_gn_singular", dual, ["ee_l"], 6, 34, "noisy", os.path.join(HERE, "ik_dual_arm_gn_singular.npz"),
+            max_iter=30, tol=1e-6, optimizer="gn", gn_eps=0.0, limit_w=0.0, rest_w=0.0)
 
 
 def make_adjoint(spec, B, seed, out):
@@ -373,6 +390,9 @@ def main():
     if only == ["trajopt_mixed"]:
         make_trajopt(syn.mixed_spec(), 3, 12, 45, os.path.join(HERE, "trajopt_mixed.npz"), spread=0.3)
         return
+    if only == ["ik_damping"]:
+        make_ik_damping_and_singular(syn.chain_spec(), syn.dual_arm_spec())
+        return
     if only == ["trajopt_humanoid"]:
         make_trajopt(syn.humanoid_spec(), 2, 10, 49, os.path.join(HERE, "trajopt_humanoid.npz"), spread=0.3,
                      frame="track0")
@@ -396,6 +416,7 @@ def main():
     make_ik_kernels(chain, dual, hum, lm)
     make_ik_kinds(chain, dual, hum, lm)
     make_ik_mixed()
+    make_ik_damping_and_singular(chain, dual)
     make_adjoint(hum, 4, 31, os.path.join(HERE, "adjoint.npz"))
     make_adjoint(syn.mixed_spec(), 8, 33, os.path.join(HERE, "adjoint_mixed.npz"))
     make_trajopt(chain, 3, 24, 41, os.path.join(HERE, "trajopt_chain7.npz"))

@@ -8,6 +8,8 @@ on the same problems: ``ik_mix_reach.npz`` with, per problem,
 * ``margin``: the oracle's smallest ``|cost_new - cost|`` in units of the cost's float64
   spacing over the accept tests that decide convergence (``oracle.ik.IKOutcome.margin``);
   a verdict with a margin of a few units is decided by the rounding of a float64 sum;
+* ``q_final`` (packed per problem in class order, ``q_offset``), ``cost``: the oracle's final
+  configuration and ``0.5 |r|^2``;
 * ``ref_converged``, ``ref_iters``: the verdict and iteration count of BetterRobot's
   ``LevenbergMarquardt`` run in float64 through its own cost stack (the solve of
   ``make_golden.reference_lm``, built as ``solve_ik`` builds it).
@@ -62,7 +64,8 @@ def _chunk(args):
         st = reference_lm(mref, names, Tref, c["q0"][p].double(), tol=s.tol, max_iter=s.max_iter, lam0=s.lam0,
                           factor=s.factor, limit_w=s.limit_weight, rest_w=s.rest_weight)
         rows.append((ci, p, int(pe[0] <= bench.REACH_TOL and re[0] <= bench.REACH_TOL), int(r.converged[0]),
-                     int(r.iters[0]), float(r.margin[0]), int(st.status == "converged"), int(st.iters)))
+                     int(r.iters[0]), float(r.margin[0]), int(st.status == "converged"), int(st.iters),
+                     r.q[0].copy(), float(r.cost[0])))
     return rows
 
 
@@ -75,10 +78,13 @@ def main():
             for lo in range(0, len(c["n_targets"]), 32)]
     jobs.sort(key=lambda j: j[0])  # humanoid chunks (the slowest) first
     with mp.get_context("spawn").Pool(int(os.environ.get("PROCS", "8"))) as pool:
-        rows = sorted(r for chunk in pool.imap_unordered(_chunk, jobs) for r in chunk)
+        rows = sorted((r for chunk in pool.imap_unordered(_chunk, jobs) for r in chunk), key=lambda r: (r[0], r[1]))
     a = np.array([r[:5] for r in rows], np.int16)
+    qf = [r[8] for r in rows]
+    q_offset = np.concatenate([[0], np.cumsum([len(x) for x in qf])[:-1]]).astype(np.int64)
     np.savez_compressed(os.path.join(HERE, "ik_mix_reach.npz"), cls=a[:, 0], index=a[:, 1], reached=a[:, 2],
                         converged=a[:, 3], iters=a[:, 4], margin=np.array([r[5] for r in rows], np.float32),
+                        q_final=np.concatenate(qf), q_offset=q_offset, cost=np.array([r[9] for r in rows]),
                         ref_converged=np.array([r[6] for r in rows], np.int8),
                         ref_iters=np.array([r[7] for r in rows], np.int16),
                         classes=np.array([c["name"] for c in wl]))

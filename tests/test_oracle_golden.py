@@ -67,12 +67,16 @@ def test_lie_matches_reference():
                                         ("chain7_huber", "chain7"), ("chain7_gn_cauchy", "chain7"),
                                         ("dual_arm_cauchy", "dual_arm"), ("humanoid_tukey", "humanoid"),
                                         ("chain7_position", "chain7"), ("dual_arm_mixed", "dual_arm"),
-                                        ("humanoid_mixed", "humanoid"), ("mixed", "mixed")])
+                                        ("humanoid_mixed", "humanoid"), ("mixed", "mixed"),
+                                        ("chain7_constant", "chain7")])
 def test_lm_gn_match_reference_solver(case, robot):
+    """The oracle's LM / GN reproduces the reference's solves; Constant damping
+    (optim/strategies/constant.py:9-25) is Adaptive's update with factor 1."""
     g = _load(f"ik_{case}.npz")
     m = syn.model_from_spec(SPECS[robot], dtype=torch.float64)
     st = g["settings"]
-    s = ik.IKSettings(lam0=st[0], factor=st[1], tol=st[2], max_iter=int(st[3]), limit_weight=st[4],
+    constant = "damping" in g and str(g["damping"]) == "constant"
+    s = ik.IKSettings(lam0=st[0], factor=1.0 if constant else st[1], tol=st[2], max_iter=int(st[3]), limit_weight=st[4],
                       rest_weight=st[5], optimizer=str(g["optimizer"]),
                       kernel=str(g["kernel"]) if "kernel" in g else "l2")
     kinds = [str(k) for k in g["kinds"]] if "kinds" in g else None
@@ -131,19 +135,20 @@ def test_known_answers_one_joint_arm():
 
 
 @pytest.mark.parametrize("fixture,spec", [("trajopt_chain7.npz", "chain7"), ("trajopt_floating.npz", "floating"),
-                                          ("trajopt_mixed.npz", "mixed")])
+                                          ("trajopt_mixed.npz", "mixed"), ("trajopt_humanoid.npz", "humanoid")])
 def test_trajopt_matches_reference_solve_trajopt(fixture, spec):
     """GN trajectory optimisation (goal/start pose, acceleration, per-knot limits, reference
-    trajectory), on the fixed-base chain, a floating-base chain (free-flyer knots) and the
-    robot with planar, translation, spherical and unbounded-revolute joints."""
+    trajectory), on the fixed-base chain, a floating-base chain (free-flyer knots), the
+    robot with planar, translation, spherical and unbounded-revolute joints and the 36-DOF
+    humanoid."""
     from oracle import trajopt as ot
     g = _load(fixture)
     T, dt, wg, ws, wa, wl, wr, tol, mi = g["settings"]
     m = syn.model_from_spec({"chain7": SPECS["chain7"], "floating": syn.floating_chain_spec(),
-                             "mixed": syn.mixed_spec()}[spec], dtype=torch.float64)
+                             "mixed": syn.mixed_spec(), "humanoid": syn.humanoid_spec()}[spec], dtype=torch.float64)
     s = ot.TrajSettings(dt=dt, w_goal=wg, w_start=ws, w_accel=wa, w_limit=wl, w_ref=wr, tol=tol, max_iter=int(mi))
     X0 = np.repeat(g["q_start"][:, None, :], int(T), 1)
-    fid = m.frame_id("ee")
+    fid = m.frame_id(str(g["frame"]) if "frame" in g else "ee")
     out = ot.solve(m, X0, fid, g["goal"], g["start"], s)
     np.testing.assert_array_equal(out.iters, g["iters"])
     np.testing.assert_array_equal(out.converged, g["converged"])
@@ -167,3 +172,17 @@ def test_lie_ops_match_reference():
     }
     for k, v in checks.items():
         np.testing.assert_allclose(v, g[k], atol=1e-12, rtol=0, err_msg=k)
+
+
+@pytest.mark.parametrize("fixture,spec", [("adjoint.npz", syn.humanoid_spec()), ("adjoint_mixed.npz", syn.mixed_spec())],
+                         ids=["humanoid", "mixed"])
+def test_oracle_pose_loss_gradient_matches_reference_autograd(fixture, spec):
+    """The oracle's reverse sweep (oracle/adjoint.py) against BetterRobot's float64 autograd
+    through its own FK (the humanoid, and the robot with every multi-slot joint kind)."""
+    from oracle import adjoint as A
+    g = np.load(os.path.join(GOLDEN, fixture))
+    m64 = syn.model_from_spec(spec, dtype=torch.float64)
+    L = A.pose_loss(m64, g["q"], g["frame_ids"], g["targets"], g["weights"])
+    G = A.pose_loss_grad(m64, g["q"], g["frame_ids"], g["targets"], g["weights"])
+    np.testing.assert_allclose(L, g["loss"], rtol=1e-12, atol=1e-12)
+    assert np.abs(G - g["grad"]).max() <= 1e-12 * np.abs(g["grad"]).max()
