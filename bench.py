@@ -128,6 +128,52 @@ def gpu_reach_flags(wl, q_list):
 
 
 # ---------------------------------------------------------------------------
+# LM compute roofline: algorithmic floating-point operations of one iteration of the
+# reference's dense method (levenberg_marquardt.py:89-110 with the IK stack of tasks/ik.py),
+# an FMA counted as 2
+# ---------------------------------------------------------------------------
+SE3_COMPOSE_FLOPS = 61        # quaternion product (28) + rotate (30) + add (3)
+SE3_LOG_FLOPS = 60            # quaternion log + V^-1 v
+JR_INV_FLOPS = 9 * 2 * 6 ** 3 + 2 * 6 ** 3   # 9-term ad series of 6x6 products + 6x6 inverse
+# B200 FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 flops x 1.965 GHz (nominal; the kernel issues
+# FP32 and FP64 instructions, FP64 at half this rate)
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def lm_iteration_flops(model, frame_ids) -> int:
+    """Flops of one LM iteration on ``model`` with pose targets on ``frame_ids``: trial FK (one SE3
+    compose per joint), the residual (frame pose, error pose, log per target; limit and rest rows),
+    the Jacobian (per target Jr^-1, its frame Jacobian by the support loop, one 6x6 Ad product per
+    supporting column, and Jr^-1 R^T J_lwa), the dense J^T J and J^T r over the stacked rows,
+    the Cholesky factorization and two triangular solves, and the retraction."""
+    nj, nq, nv = model.njoints, model.nq, model.nv
+    k = len(frame_ids)
+    dim = 6 * k + 2 * nq + nv
+    f = nj * SE3_COMPOSE_FLOPS
+    f += k * (2 * SE3_COMPOSE_FLOPS + SE3_LOG_FLOPS) + 4 * nq + 3 * nv
+    for fid in frame_ids:
+        depth = sum(int(model.nvs[j]) for j in model.supports[model.frames[fid].parent_joint])
+        f += JR_INV_FLOPS + depth * 2 * 36 + 2 * 2 * 36 * nv
+    f += 2 * dim * nv * nv + 2 * dim * nv
+    f += 2 * nv ** 3 // 3 + 2 * 2 * nv * nv
+    f += 2 * nq
+    return f
+
+
+def lm_launch_flops(wl, iters) -> float:
+    """Flops of one solve of the packed mix: per problem, its iterations x its class's iteration
+    flops for its own targets."""
+    total, off = 0.0, 0
+    for c in wl:
+        m = c["model"]
+        for p in range(len(c["n_targets"])):
+            k = int(c["n_targets"][p])
+            total += float(iters[off + p]) * lm_iteration_flops(m, [int(x) for x in c["frames"][p, :k]])
+        off += len(c["n_targets"])
+    return total
+
+
+# ---------------------------------------------------------------------------
 # helpers
 # ---------------------------------------------------------------------------
 def _peaks():
@@ -256,15 +302,21 @@ def reduce(x: float, world: int, op: str) -> float:
 # ---------------------------------------------------------------------------
 # fused LM-IK (headline)
 # ---------------------------------------------------------------------------
-def bench_ik(steps: int, warmup: int, seed: int, pinned=None):
+def ik_settings(precision: str = "f32"):
+    from betterrobot_b200 import ik as bik
+    return bik.settings_from(
+        bik.IKCostConfig(rest_weight=SETTINGS["rest_weight"], limit_weight=SETTINGS["limit_weight"]),
+        bik.OptimizerConfig(max_iter=MAX_ITER, lam0=SETTINGS["lam0"], factor=SETTINGS["factor"], tol=SETTINGS["tol"],
+                            precision=precision))
+
+
+def bench_ik(steps: int, warmup: int, seed: int, pinned=None, precision: str = "f32", e2e: bool = True):
     """``pinned = (team_sizes, warps_per_cta)`` skips the autotuner (used to profile one known launch shape)."""
     import torch
     from betterrobot_b200 import ik as bik
     wl = make_workload(N_PROBLEMS, seed)
     gpu_targets(wl)
-    settings = bik.settings_from(
-        bik.IKCostConfig(rest_weight=SETTINGS["rest_weight"], limit_weight=SETTINGS["limit_weight"]),
-        bik.OptimizerConfig(max_iter=MAX_ITER, lam0=SETTINGS["lam0"], factor=SETTINGS["factor"], tol=SETTINGS["tol"]))
+    settings = ik_settings(precision)
     from betterrobot_b200 import autotune
     tg_dev = [c["targets"] for c in wl]
     q0_dev = [c["q0"].float().cuda() for c in wl]
@@ -300,6 +352,10 @@ def bench_ik(steps: int, warmup: int, seed: int, pinned=None):
     reached = gpu_reach(wl, [pk.q_of(c).clone() for c in range(len(wl))])
     conv = int(((pk.status & 0xFF) == 0).sum())
     iters = pk.iters.float()
+    flops = lm_launch_flops(wl, pk.iters.cpu().numpy())
+    if not e2e:
+        return {"ms": ms, "reached": reached, "converged": conv, "problems": pk.P, "flops": flops,
+                "iters_mean": float(iters.mean()), "team_sizes": teams, "warps_per_cta": warps}
     # e2e: pinned host inputs -> solve -> pinned host outputs, every step
     h_tg = [t.cpu().pin_memory() for t in tg_dev]
     h_q0 = [q.cpu().pin_memory() for q in q0_dev]
@@ -342,6 +398,7 @@ def bench_ik(steps: int, warmup: int, seed: int, pinned=None):
     torch.cuda.synchronize()
     gt = [a.elapsed_time(b) for a, b in evs]
     return {"ms": ms, "reached": reached, "converged": conv, "problems": pk.P, "iters_mean": float(iters.mean()),
+            "flops": flops,
             "e2e_ms": float(np.mean(et)), "h2d": h2d, "d2h": d2h, "launches": steps, "wl": wl,
             "graph_ms": float(np.mean(gt)), "team_sizes": teams, "warps_per_cta": warps}
 
@@ -449,6 +506,57 @@ def bench_joint_ops(steps: int, warmup: int):
         ms = e0.elapsed_time(e1) / steps
         out[name] = {"ms_per_launch": ms, "gbs": B * 440 / (ms * 1e-3) / 1e9, "batch": B}
     return out
+
+
+def _time_launches(fn, steps: int, warmup: int) -> float:
+    """Mean ms per call of ``fn`` over ``steps`` calls enqueued back to back (CUDA events)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_lie(steps: int, warmup: int, n: int = 1 << 23):
+    """Batched LieOps (``lie_ops_kernel``) on 8.4 M elements: se3_compose (reads 2 poses, writes one:
+    84 B per element), se3_log (28 B in, 24 B out), se3_exp (24 B in, 28 B out); inputs > L2."""
+    import torch
+    from betterrobot_b200 import lie
+    g = torch.Generator("cuda").manual_seed(5)
+    def poses():
+        t = torch.randn(n, 7, device="cuda", generator=g)
+        t[:, 3:] = t[:, 3:] / t[:, 3:].norm(dim=1, keepdim=True)
+        return t
+    a, b = poses(), poses()
+    xi = torch.randn(n, 6, device="cuda", generator=g) * 0.5
+    out = {}
+    for name, fn, bytes_per in (("se3_compose", lambda: lie.se3_compose(a, b), 84),
+                                ("se3_log", lambda: lie.se3_log(a), 52), ("se3_exp", lambda: lie.se3_exp(xi), 52)):
+        ms = _time_launches(fn, steps, warmup)
+        out[name] = {"ms_per_launch": ms, "gbs": n * bytes_per / (ms * 1e-3) / 1e9, "elements": n}
+    return out
+
+
+def bench_joint_jacobians(steps: int, warmup: int, B: int = 16384):
+    """``compute_joint_jacobians`` on the humanoid from stored joint placements (``fk_jac_kernel``
+    in its from-poses mode): reads oMi (B x 32 x 7 floats), writes J (B x 32 x 6 x 36 floats)."""
+    import torch
+    import betterrobot_b200 as br
+    from betterrobot_b200 import synthetic as syn
+    m = syn.model_from_spec(syn.humanoid_spec())
+    m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
+    q = syn.random_q(m64, B, 3, rev_range=2.5, base_translation=1.0).float().cuda()
+    data = br.forward_kinematics(m, q)
+    ms = _time_launches(lambda: br.compute_joint_jacobians(m, data), steps, warmup)
+    nbytes = B * m.njoints * (7 + 6 * m.nv) * 4
+    return {"ms_per_launch": ms, "gbs": nbytes / (ms * 1e-3) / 1e9, "batch": B, "bytes_per_launch": nbytes}
 
 
 # ---------------------------------------------------------------------------
@@ -674,11 +782,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-op PyTorch arm")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
-    ap.add_argument("--only", choices=["ik", "fkj", "adjoint", "trajopt", "joint_ops"], default=None,
+    ap.add_argument("--only", choices=["ik", "fkj", "adjoint", "trajopt", "joint_ops", "lie", "joint_jac"],
+                    default=None,
                     help="run one section and print its raw timings (for profiling)")
     ap.add_argument("--ik-teams", default=None,
                     help="comma-separated lanes per problem for humanoid,dual_arm,chain7 (skips the autotuner)")
     ap.add_argument("--ik-warps", type=int, default=4, help="warps per CTA with --ik-teams")
+    ap.add_argument("--ik-precision", choices=["f32", "f64"], default="f32",
+                    help="normal-equation arithmetic of the LM kernel (--only ik)")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         # not started by torchrun: launch the N replicas here, one process per GPU
@@ -721,14 +832,18 @@ def main():
             pinned = None
             if args.ik_teams:
                 pinned = ([int(t) for t in args.ik_teams.split(",")], args.ik_warps)
-            r = bench_ik(args.steps, warmup, seed=7, pinned=pinned)
-            r.pop("wl")
+            r = bench_ik(args.steps, warmup, seed=7, pinned=pinned, precision=args.ik_precision)
+            r.pop("wl", None)
         elif args.only == "joint_ops":
             r = bench_joint_ops(args.steps, warmup)
         elif args.only == "fkj":
             r = bench_fkj(args.steps, warmup)
         elif args.only == "trajopt":
             r = bench_trajopt(args.steps, warmup)
+        elif args.only == "lie":
+            r = bench_lie(args.steps, warmup)
+        elif args.only == "joint_jac":
+            r = bench_joint_jacobians(args.steps, warmup)
         else:
             r = bench_adjoint(args.steps, warmup)
         print(json.dumps({"section": args.only, **r}), flush=True)
@@ -749,6 +864,7 @@ def main():
         ik = bench_ik(args.steps, warmup, seed=shard_seed(rank))
         barrier(world)
     clocks = clk.summary()
+    ik64 = bench_ik(args.steps, warmup, seed=shard_seed(rank), precision="f64", e2e=False)
     fkj = bench_fkj(args.steps, warmup)
     adj = bench_adjoint(args.steps, warmup) if not args.no_adjoint else None
     trj = bench_trajopt(args.steps, warmup) if not args.no_adjoint else None
@@ -767,11 +883,23 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "fk_jac_kernel (humanoid B=65536, 12 frames, J + oMf)",
                      "achieved": fkj["gbs"], "peak": peak, "unit": "GB/s", "frac": fkj["gbs"] / peak,
                      "traffic": FKJ_TRAFFIC_BYTES, "peak_kind": peak_kind, "ms_per_launch": fkj["ms_per_launch"]},
+        "roofline_lm": {"bound": "latency / issue (FP32 + FP64 CUDA cores, no tensor cores)",
+                        "kernel": "lm_solve_kernel (the whole mix, one launch)",
+                        "achieved": ik["flops"] / (ik["ms"] * 1e-3) / 1e12, "peak": FP32_PEAK_TFLOPS,
+                        "unit": "TFLOP/s", "frac": ik["flops"] / (ik["ms"] * 1e-3) / 1e12 / FP32_PEAK_TFLOPS,
+                        "peak_kind": "nominal FP32 CUDA-core peak (148 SMs x 128 x 2 x 1.965 GHz)",
+                        "flops_per_launch": ik["flops"],
+                        "flops_basis": "reference's dense LM iteration per problem x its iterations"},
         "ik": {"problems": ik["problems"] * world, "reached_1e-4": reached, "converged": ik["converged"],
                "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1,
                "graph_replay_ms": ik["graph_ms"], "autotuned": {"team_sizes": ik["team_sizes"],
                                                                 "warps_per_cta": ik["warps_per_cta"]}},
         "clocks": clocks, "gpu_launches": ik["launches"],
+        "ik_f64_normal_equations": {
+            "value": ik64["reached"] / (ik64["ms"] * 1e-3), "unit": "solves/s", "ms_per_step": ik64["ms"],
+            "reached_1e-4": ik64["reached"], "converged": ik64["converged"],
+            "note": "the same mix with precision='f64' (Jacobian, J^T J, J^T r and factorization in float64): "
+                    "every determinate converged verdict equals the float64 reference's"},
     }
     if adj is not None:
         line["adjoint"] = adj

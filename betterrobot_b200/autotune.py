@@ -33,7 +33,7 @@ def tune(make_packed, settings, warps=(2, 4, 8), reps: int = 3, max_candidates: 
     ``make_packed(team_sizes, warps_per_cta)`` builds a ``PackedIK`` with its inputs set.
     """
     base = make_packed(None, 4)
-    key = signature(base)
+    key = signature(base) + (int(getattr(settings, "precision", 0)),)
     if key in _CACHE:
         return _CACHE[key]
     choices = [_team_choices(m.nv) for m in base.models]

@@ -215,21 +215,73 @@ __device__ __forceinline__ void apply_op(const float* x, const float* y, float* 
   }
 }
 
+// Copy `len` floats between a warp's shared-memory tile and global memory, coalesced: 16-byte
+// accesses while both sides allow them (`vec`: the global slab starts on a 16-byte boundary;
+// tiles start on one), then single floats for the remainder.
+__device__ __forceinline__ void warp_load(float* __restrict__ s, const float* __restrict__ g, int len, int lane,
+                                          bool vec) {
+  int k0 = 0;
+  if (vec) {
+    const int n4 = len >> 2;
+    for (int k = lane; k < n4; k += kWarp)
+      reinterpret_cast<float4*>(s)[k] = __ldg(reinterpret_cast<const float4*>(g) + k);
+    k0 = n4 << 2;
+  }
+  for (int k = k0 + lane; k < len; k += kWarp) s[k] = __ldg(g + k);
+}
+__device__ __forceinline__ void warp_store(float* __restrict__ g, const float* __restrict__ s, int len, int lane,
+                                           bool vec) {
+  int k0 = 0;
+  if (vec) {
+    const int n4 = len >> 2;
+    for (int k = lane; k < n4; k += kWarp) reinterpret_cast<float4*>(g)[k] = reinterpret_cast<const float4*>(s)[k];
+    k0 = n4 << 2;
+  }
+  for (int k = k0 + lane; k < len; k += kWarp) g[k] = s[k];
+}
+
+constexpr int kLieWarps = 8;  // warps per CTA
+
+// One warp per tile of 32 consecutive elements: the tile's operand records (contiguous slabs
+// of 32 * floats-per-record) are copied into the warp's shared memory with coalesced loads,
+// each lane applies the op to its element, and the output slab leaves the same way.  A
+// broadcast operand (one record for every element) is read in place.
 template <int OP>
-__global__ void lie_ops_kernel(const float* __restrict__ a, const float* __restrict__ b, int64_t n, int a_bcast,
-                               int b_bcast, float* __restrict__ out) {
+__global__ void __launch_bounds__(kLieWarps * kWarp) lie_ops_kernel(const float* __restrict__ a,
+                                                                   const float* __restrict__ b, int64_t n,
+                                                                   int a_bcast, int b_bcast, float* __restrict__ out) {
   constexpr LieOpSpec sp = lie_spec(OP);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float* x = a + (a_bcast ? 0 : i * sp.a);
-    const float* y = sp.b ? b + (b_bcast ? 0 : i * sp.b) : nullptr;
-    apply_op<OP>(x, y, out + i * sp.out);
+  constexpr int A = sp.a, Bn = sp.b, O = sp.out;
+  constexpr int TILE = kWarp * (A + Bn + O);    // floats per warp (a multiple of 4: 16-byte tiles)
+  __shared__ __align__(16) float smem[kLieWarps * TILE];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float* sa = smem + w * TILE;
+  float* sb = sa + kWarp * A;
+  float* so = sb + kWarp * Bn;
+  const bool va = ((reinterpret_cast<uintptr_t>(a) & 15u) == 0), vb = ((reinterpret_cast<uintptr_t>(b) & 15u) == 0),
+             vo = ((reinterpret_cast<uintptr_t>(out) & 15u) == 0);
+  const int64_t ntiles = (n + kWarp - 1) / kWarp;
+  for (int64_t t = (int64_t)blockIdx.x * kLieWarps + w; t < ntiles; t += (int64_t)gridDim.x * kLieWarps) {
+    const int64_t i0 = t * kWarp;
+    const int cnt = (int)((n - i0) < kWarp ? (n - i0) : kWarp);
+    if (!a_bcast) warp_load(sa, a + i0 * A, cnt * A, lane, va);
+    if (Bn && !b_bcast) warp_load(sb, b + i0 * Bn, cnt * Bn, lane, vb);
+    __syncwarp();
+    if (lane < cnt) {
+      const float* x = a_bcast ? a : sa + lane * A;
+      const float* y = Bn ? (b_bcast ? b : sb + lane * Bn) : nullptr;
+      apply_op<OP>(x, y, so + lane * O);
+    }
+    __syncwarp();
+    warp_store(out + i0 * O, so, cnt * O, lane, vo);
+    __syncwarp();
   }
 }
 
 template <int OP>
 static void launch_op(unsigned blocks, cudaStream_t s, const float* a, const float* b, int64_t n, int ab, int bb,
                       float* out) {
-  lie_ops_kernel<OP><<<blocks, 256, 0, s>>>(a, b, n, ab, bb, out);
+  lie_ops_kernel<OP><<<blocks, kLieWarps * kWarp, 0, s>>>(a, b, n, ab, bb, out);
 }
 
 }  // namespace br
@@ -254,8 +306,8 @@ extern "C" int br_lie_op(int32_t op, const float* a, int64_t na, const float* b,
   if (sp.b && (!b || (nb != n && nb != 1))) return BR_EINVAL;
   if (!aligned4(a) || !aligned4(out) || (sp.b && !aligned4(b))) return BR_EALIGN;
   const DeviceInfo& d = device_info();
-  int64_t blocks = (n + 255) / 256;
-  const int64_t cap = (int64_t)d.sms * 8;  // grid-stride beyond 8 CTAs of 256 threads per SM
+  int64_t blocks = (n + kLieWarps * kWarp - 1) / (kLieWarps * kWarp);   // one 32-element tile per warp
+  const int64_t cap = (int64_t)d.sms * 8;  // grid-stride beyond 8 CTAs of 8 warps per SM (64 warps: the SM's limit)
   if (blocks > cap) blocks = cap;
   const cudaStream_t s = (cudaStream_t)stream;
   const unsigned g = (unsigned)blocks;

@@ -1010,7 +1010,7 @@ __device__ __forceinline__ void run_item(const LmParams& P, int cls, int first, 
 }
 
 template <bool kGeneral, bool kF64>
-__global__ void __maxnreg__(128) lm_solve_kernel(const LmParams P) {
+__global__ void __maxnreg__(kF64 ? 168 : 128) lm_solve_kernel(const LmParams P) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;

@@ -217,13 +217,16 @@ class PackedIK:
         rdim = np.concatenate(dims)
         self.r_offset_np = np.concatenate([[0], np.cumsum(rdim)[:-1]]).astype(np.int64)
         self.r_dim = rdim
-        # work items: heaviest classes first (LPT), 32/T problems per item
+        # work items: heaviest classes first, and inside a class the problems with the fewest
+        # targets first (they run the most iterations: a less constrained problem's rest term
+        # settles slowly), so the longest solves start early and the launch's tail is short
         cost = [m.nv ** 2 * (1 + self.K) for m in models]
         order, items = [], []
         slot = 0
         for c in sorted(range(self.C), key=lambda k: -cost[k]):
             per = 32 // self.team[c]
-            idx = np.arange(self.class_start[c], self.class_start[c] + self.counts[c])
+            s0 = int(self.class_start[c])
+            idx = s0 + np.argsort(nt_all[s0:s0 + self.counts[c]], kind="stable")
             order.append(idx)
             for s in range(0, self.counts[c], per):
                 items.append((slot + s, min(per, self.counts[c] - s), c))

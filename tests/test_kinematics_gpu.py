@@ -100,6 +100,24 @@ def test_frame_jacobians_match_oracle(robot, reference, B):
     assert_jac(J, Jref)
 
 
+@pytest.mark.parametrize("reference", ["world", "local_world_aligned", "local"])
+def test_large_jacobian_blocks_match_oracle(reference):
+    """Every frame of the humanoid (44: a 38 KB Jacobian block per configuration, which leaves
+    room for four warps per CTA), and all 32 joints from stored placements
+    (compute_joint_jacobians), against the oracle; B = 129 leaves partial CTAs."""
+    m = syn.model_from_spec(SPECS["humanoid"])
+    m64 = syn.model_from_spec(SPECS["humanoid"], dtype=torch.float64)
+    q = syn.random_q(m64, 129, 91, rev_range=2.5, base_translation=1.0)
+    fids = list(range(m.nframes))
+    T, J = br.frame_jacobians(m, q.float().cuda(), fids, reference=reference)
+    oMi, _ = K.forward_kinematics(m64, q.numpy())
+    assert_poses(T, K.frame_placements(m64, oMi, fids))
+    assert_jac(J, np.stack([K.frame_jacobian(m64, oMi, q.numpy(), f, reference) for f in fids], -3))
+    if reference == "world":
+        data = br.compute_joint_jacobians(m, br.forward_kinematics(m, q.float().cuda()))
+        assert_jac(data.joint_jacobians, K.compute_joint_jacobians(m64, oMi, q.numpy()))
+
+
 def test_unaligned_output_fallback_chain():
     """chain7 with one frame: a J block is 168 B (not a multiple of 16) -> cooperative stores."""
     m = syn.model_from_spec(SPECS["chain7"])
