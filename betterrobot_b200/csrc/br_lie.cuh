@@ -319,6 +319,43 @@ __device__ __forceinline__ JrInv jr_inv_se3(float3 v, float3 w) {
   return J;
 }
 
+// One column of jr_inv_se3<N>: column c of B (returned) and A^-1's coefficients b0, b1, b2.
+// The columns of the series are independent given the scalar recursion of A, so three lanes can
+// share one target's series; each column's arithmetic is jr_inv_se3's, in the same order.
+template <int N>
+__device__ __forceinline__ float3 jr_inv_se3_col(float3 v, float3 w, int c, float& b0, float& b1, float& b2) {
+  float ck[N + 1];
+  {
+    float f = 1.f;
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+      f /= (float)(k + 1);
+      ck[k] = (k & 1) ? -f : f;
+    }
+  }
+  const float th2 = dot(w, w);
+  float a0 = ck[N], a1 = 0.f, a2 = 0.f;
+  float3 bc = f3(0.f, 0.f, 0.f);
+  const float3 e = f3(c == 0 ? 1.f : 0.f, c == 1 ? 1.f : 0.f, c == 2 ? 1.f : 0.f);
+#pragma unroll
+  for (int k = N - 1; k >= 0; --k) {
+    const float3 ac = apply_poly(w, a0, a1, a2, e);     // column c of A
+    bc = add(cross(w, bc), cross(v, ac));               // W B_c + V A_c
+    const float na1 = fmaf(-th2, a2, a0);
+    a2 = a1;
+    a1 = na1;
+    a0 = ck[k];
+  }
+  b0 = 1.f / a0;
+  const float m = fmaf(-th2, a2, a0);
+  const float r0 = -a1 * b0, r1 = -a2 * b0;
+  const float det = fmaf(m, m, th2 * a1 * a1);
+  const float idet = 1.f / det;
+  b1 = (r0 * m + th2 * a1 * r1) * idet;
+  b2 = (m * r1 - a1 * r0) * idet;
+  return bc;
+}
+
 // out = Jr^-1 [x_lin; x_ang] = [A^-1 (x_lin - B A^-1 x_ang); A^-1 x_ang]
 __device__ __forceinline__ void jr_inv_apply(const JrInv& J, float3 xl, float3 xa, float3& ol, float3& oa) {
   oa = apply_poly(J.w, J.b0, J.b1, J.b2, xa);
@@ -510,6 +547,40 @@ __device__ __forceinline__ DJrInv djr_inv_se3(double3 v, double3 w) {
 #pragma unroll
   for (int i = 0; i < 9; ++i) J.B[i] = B[i];
   return J;
+}
+
+// One column of djr_inv_se3<N> (see jr_inv_se3_col).
+template <int N>
+__device__ __forceinline__ double3 djr_inv_se3_col(double3 v, double3 w, int c, double& b0, double& b1, double& b2) {
+  double ck[N + 1];
+  {
+    double f = 1.0;
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+      f /= (double)(k + 1);
+      ck[k] = (k & 1) ? -f : f;
+    }
+  }
+  const double th2 = ddot(w, w);
+  double a0 = ck[N], a1 = 0.0, a2 = 0.0;
+  double3 bc = d3(0.0, 0.0, 0.0);
+  const double3 e = d3(c == 0 ? 1.0 : 0.0, c == 1 ? 1.0 : 0.0, c == 2 ? 1.0 : 0.0);
+#pragma unroll
+  for (int k = N - 1; k >= 0; --k) {
+    const double3 ac = dapply_poly(w, a0, a1, a2, e);
+    bc = dadd(dcross(w, bc), dcross(v, ac));
+    const double na1 = a0 - th2 * a2;
+    a2 = a1;
+    a1 = na1;
+    a0 = ck[k];
+  }
+  b0 = 1.0 / a0;
+  const double m = a0 - th2 * a2;
+  const double r0 = -a1 * b0, r1 = -a2 * b0;
+  const double idet = 1.0 / (m * m + th2 * a1 * a1);
+  b1 = (r0 * m + th2 * a1 * r1) * idet;
+  b2 = (m * r1 - a1 * r0) * idet;
+  return bc;
 }
 
 __device__ __forceinline__ void djr_inv_apply(const DJrInv& J, double3 xl, double3 xa, double3& ol, double3& oa) {

@@ -113,6 +113,7 @@ struct TeamLayout {
 
 __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
 
+
 // IRLS weight w(s) of one squared residual row s (optim/kernels/{huber,cauchy,tukey}.py:
 // weight; applied as in levenberg_marquardt.py:27-44, whose sqrt(w) scales both the row
 // and its Jacobian row, so J^T J and J^T r pick up w).  Evaluated in float64.
@@ -568,21 +569,26 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       }
       g[c] = (R)0;
     }
-    for (int t = tl; t < nt; t += T) {
+    // Jr^-1 of each target: its three B columns on three lanes (job = 3 t + c)
+    for (int job = tl; job < 3 * nt; job += T) {
+      const int t = job / 3, c = job - 3 * t;
       const double* e = xi + 8 * t;
       R* o = jri + 16 * t;
       if (!kGeneral || tkind[t] == BR_TARGET_POSE) {                   // SE3 Jr^-1(xi), tangents.py:204-207
         if constexpr (kF64) {
-          const DJrInv J = djr_inv_se3<9>(d3(e[0], e[1], e[2]), d3(e[3], e[4], e[5]));
-          o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
-          for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
+          double b0, b1, b2;
+          const double3 bc = djr_inv_se3_col<9>(d3(e[0], e[1], e[2]), d3(e[3], e[4], e[5]), c, b0, b1, b2);
+          if (c == 0) { o[0] = e[3]; o[1] = e[4]; o[2] = e[5]; o[3] = b0; o[4] = b1; o[5] = b2; }
+          o[6 + c] = bc.x; o[9 + c] = bc.y; o[12 + c] = bc.z;
         } else {
-          const JrInv J = jr_inv_se3<9>(f3((float)e[0], (float)e[1], (float)e[2]), f3((float)e[3], (float)e[4], (float)e[5]));
-          o[0] = J.w.x; o[1] = J.w.y; o[2] = J.w.z; o[3] = J.b0; o[4] = J.b1; o[5] = J.b2;
-          for (int k = 0; k < 9; ++k) o[6 + k] = J.B[k];
+          float b0, b1, b2;
+          const float3 w = f3((float)e[3], (float)e[4], (float)e[5]);
+          const float3 bc = jr_inv_se3_col<9>(f3((float)e[0], (float)e[1], (float)e[2]), w, c, b0, b1, b2);
+          if (c == 0) { o[0] = w.x; o[1] = w.y; o[2] = w.z; o[3] = b0; o[4] = b1; o[5] = b2; }
+          o[6 + c] = bc.x; o[9 + c] = bc.y; o[12 + c] = bc.z;
         }
-      } else {  // orientation: SO3 Jr^-1(r) (tangents.py:122-145) as the angular block, no coupling;
-                // position: identity (its rows are replaced by J_lwa's linear rows)
+      } else if (c == 0) {  // orientation: SO3 Jr^-1(r) (tangents.py:122-145) as the angular block, no coupling;
+                            // position: identity (its rows are replaced by J_lwa's linear rows)
         const bool ori = tkind[t] == BR_TARGET_ORIENTATION;
         o[0] = (R)e[3]; o[1] = (R)e[4]; o[2] = (R)e[5];
         o[3] = (R)1;
