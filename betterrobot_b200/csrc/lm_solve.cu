@@ -92,10 +92,10 @@ struct TeamLayout {
     n_ent = (ent > 0 && ent < ntri) ? ent : ntri;
     anc_stride = (dep > 0 && dep < nv) ? dep : (nv > 0 ? nv : 1);
     jtj = take(n_ent * rs);                    // J^T J, one row per DOF over its ancestors
-    // one target's J columns (build) / the factor and its right-hand-side slots (solve):
+    // two targets' J columns (build) / the factor and its right-hand-side slots (solve):
     // in the pose buffer that FK does not return (poseA after an odd number of rounds, else
     // poseB), dead while the normal equations are built and solved, when it is large enough
-    const int wneed = (6 * nv > n_ent + nv ? 6 * nv : n_ent + nv) * rs;
+    const int wneed = (12 * nv > n_ent + nv ? 12 * nv : n_ent + nv) * rs;
     work = wneed <= 14 * nj ? ((rounds & 1) ? poseA : poseB) : take(wneed);
     dinv = take(nv * rs);                      // 1 / L_jj
     ancA = take(nj); ancB = take(nj);
@@ -605,22 +605,28 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
 #pragma unroll 1
     for (int e = tl; e < nL; e += T) jtj[e] = (R)0;
     tm.sync();
-    R* Jc = work;  // [6][nv]: row r of the current target's J on its support columns
-    for (int t = 0; t < nt; ++t) {
-      const int ns = nsup[t];
-      const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
-      const unsigned char* st = sup + t * nv;
-      if constexpr (kF64) {
-        const DPose Tee = ldd(tw + 8 * t);
-        const double* o = jri + 16 * t;
-        DJrInv J;
-        J.w = d3(o[0], o[1], o[2]);
-        J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
+    // Jacobian columns of two targets per pass (blocks Jc_h = work + 6 nv h, h = 0, 1: row r of
+    // target t0 + h's J on its support columns), then each target's J^T J and J^T r in target
+    // order, so the accumulation order (and rounding) does not depend on the pairing
+    for (int t0 = 0; t0 < nt; t0 += 2) {
+      const int npair = t0 + 1 < nt ? 2 : 1;
+      const int ns0 = nsup[t0];
+      const int njob = ns0 + (npair == 2 ? nsup[t0 + 1] : 0);
+      for (int job = tl; job < njob; job += T) {
+        const int h = job >= ns0 ? 1 : 0;
+        const int t = t0 + h, u = job - (h ? ns0 : 0);
+        const int kind = kGeneral ? tkind[t] : BR_TARGET_POSE;
+        const int c = sup[t * nv + u];
+        R* Jc = work + 6 * nv * h;
+        if constexpr (kF64) {
+          const DPose Tee = ldd(tw + 8 * t);
+          const double* o = jri + 16 * t;
+          DJrInv J;
+          J.w = d3(o[0], o[1], o[2]);
+          J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
-        const double4 qc = dqconj(Tee.q);
-        for (int u = tl; u < ns; u += T) {
-          const int c = st[u];
+          for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
+          const double4 qc = dqconj(Tee.q);
           const double* cw = colw + 8 * c;
           const double3 a = d3(cw[0], cw[1], cw[2]);
           double3 lin, ang;
@@ -641,41 +647,43 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           }
           Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
           Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
-        }
-      } else {
-      const Pose Tee = to_f(ldd(tw + 8 * t));
-      const float* o = jri + 16 * t;
-      JrInv J;
-      J.w = f3(o[0], o[1], o[2]);
-      J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
-      for (int u = tl; u < ns; u += T) {
-        const int c = st[u];
-        const float4 a4 = *reinterpret_cast<const float4*>(colw + 8 * c);
-        const float3 a = f3(a4.x, a4.y, a4.z);
-        float3 lin, ang;
-        if (ckind[c] == 0) {
-          const float4 o4 = *reinterpret_cast<const float4*>(colw + 8 * c + 4);
-          lin = cross(a, sub(Tee.t, f3(o4.x, o4.y, o4.z)));             // jacobian.py:213-215
-          ang = a;
         } else {
-          lin = a;
-          ang = f3(0.f, 0.f, 0.f);
+          const Pose Tee = to_f(ldd(tw + 8 * t));
+          const float* o = jri + 16 * t;
+          JrInv J;
+          J.w = f3(o[0], o[1], o[2]);
+          J.b0 = o[3]; J.b1 = o[4]; J.b2 = o[5];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) J.B[k] = o[6 + k];
+          const float4 a4 = *reinterpret_cast<const float4*>(colw + 8 * c);
+          const float3 a = f3(a4.x, a4.y, a4.z);
+          float3 lin, ang;
+          if (ckind[c] == 0) {
+            const float4 o4 = *reinterpret_cast<const float4*>(colw + 8 * c + 4);
+            lin = cross(a, sub(Tee.t, f3(o4.x, o4.y, o4.z)));             // jacobian.py:213-215
+            ang = a;
+          } else {
+            lin = a;
+            ang = f3(0.f, 0.f, 0.f);
+          }
+          float3 ol, oa;
+          jr_inv_apply(J, qrot_inv(Tee.q, lin), qrot_inv(Tee.q, ang), ol, oa);  // pose.py:91-99
+          if (kind == BR_TARGET_POSITION) {            // top rows of J_lwa (pose.py:133-141)
+            ol = lin;
+            oa = f3(0.f, 0.f, 0.f);
+          } else if (kind == BR_TARGET_ORIENTATION) {  // Jr^-1(r) R^T J_ang (pose.py:175-195)
+            ol = f3(0.f, 0.f, 0.f);
+          }
+          Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
+          Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
         }
-        float3 ol, oa;
-        jr_inv_apply(J, qrot_inv(Tee.q, lin), qrot_inv(Tee.q, ang), ol, oa);  // pose.py:91-99
-        if (kind == BR_TARGET_POSITION) {            // top rows of J_lwa (pose.py:133-141)
-          ol = lin;
-          oa = f3(0.f, 0.f, 0.f);
-        } else if (kind == BR_TARGET_ORIENTATION) {  // Jr^-1(r) R^T J_ang (pose.py:175-195)
-          ol = f3(0.f, 0.f, 0.f);
-        }
-        Jc[u] = wp * ol.x; Jc[nv + u] = wp * ol.y; Jc[2 * nv + u] = wp * ol.z;
-        Jc[3 * nv + u] = wo * oa.x; Jc[4 * nv + u] = wo * oa.y; Jc[5 * nv + u] = wo * oa.z;
-      }
       }
       tm.sync();
+      for (int h = 0; h < npair; ++h) {
+      const int t = t0 + h;
+      const int ns = nsup[t];
+      const unsigned char* st = sup + t * nv;
+      const R* Jc = work + 6 * nv * h;
       const double* e = xi + 8 * t;
       R kw[6] = {(R)1, (R)1, (R)1, (R)1, (R)1, (R)1};  // IRLS weight of each of the target's 6 rows
       if (irls) {
@@ -707,6 +715,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
         g[st[u]] += acc;
       }
       tm.sync();
+      }
     }
     // rest (w I, regularization.py:56-64) and limit (+-w on active rows, limits.py:64-86) terms
     R gg = (R)0;
