@@ -769,13 +769,25 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   auto solve = [&](R damp) -> bool {
     R* Lm = work;
     R* z = work + nL;
+    {  // Lm = J^T J, 16-byte vectors (both regions start on a 16-byte boundary)
+      using V = typename std::conditional<kF64, double2, float4>::type;
+      constexpr int VW = 16 / (int)sizeof(R);
+      const int nvec = nL / VW;
 #pragma unroll 1
-    for (int e = tl; e < nL; e += T) Lm[e] = jtj[e];
+      for (int e = tl; e < nvec; e += T) reinterpret_cast<V*>(Lm)[e] = reinterpret_cast<const V*>(jtj)[e];
+      for (int e = nvec * VW + tl; e < nL; e += T) Lm[e] = jtj[e];
+    }
     // pivots of the leaves (final already); a non-leaf's is stored by the task that
-    // finalises its diagonal (the schedule's flag)
+    // finalises its diagonal (the schedule's flag).  A pivot is tested where it becomes
+    // final: in its flagged task for a non-leaf, and here for every DOF (while the pivots
+    // below a non-leaf are positive its pivot only decreases from this value, so the test
+    // here fails for it only when the final one would: the outcome of one test at the end).
+    bool bad = false;
     for (int i = tl; i < nv; i += T) {
       z[i] = -g[i];
-      dinv[i] = rrcp(jtj[rowoff[i] + ddep[i]] + damp);
+      const R piv = jtj[rowoff[i] + ddep[i]] + damp;
+      bad |= !(piv > (R)0) || !isfinite(piv);
+      dinv[i] = rrcp(piv);
     }
     tm.sync();
     const int nlev = (int)sched[0];
@@ -805,18 +817,15 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
           acc = rfma(-Lm[ex.x & 0xffff] * dinv[ex.y], Lm[ex.x >> 16], acc);
         }
         Lm[dst] = acc;
-        if (tk.w) dinv[tk.w - 1] = rrcp(acc + damp);         // DOF tk.w - 1's pivot is final
+        if (tk.w) {                                            // DOF tk.w - 1's pivot is final
+          const R piv = acc + damp;
+          bad |= !(piv > (R)0) || !isfinite(piv);
+          dinv[tk.w - 1] = rrcp(piv);
+        }
       }
       tm.sync();
     }
-    bool bad = false;  // pivots are final once their level is done
-    for (int i = tl; i < nv; i += T) {
-      const R piv = Lm[rowoff[i] + ddep[i]] + damp;
-      bad |= !(piv > (R)0) || !isfinite(piv);
-      dinv[i] = rrcp(piv);
-    }
     if (__any_sync(tm.mask, bad)) return false;
-    tm.sync();
     // back substitution by depth, root first: a lane keeps its DOFs' right-hand sides in
     // registers; once the DOFs of depth dl are final, every deeper DOF subtracts the
     // term of its one ancestor at depth dl (no two lanes write the same DOF)

@@ -78,6 +78,12 @@ def test_full_mix_verdicts_and_reach(precision):
         agree_all.append(agree)
         assert agree.mean() >= 0.98, (c["name"], agree.mean())
         a_det = (mine == ref_conv)[det].mean()
+        # one line per class for the parity summary (shown with pytest -s)
+        print(f"\n[parity] {precision} {c['name']}: n {n} determinate {int(det.sum())} "
+              f"verdict(det) vs oracle {a_det:.4f} vs BetterRobot {(mine == br_conv)[det].mean():.4f} "
+              f"verdict(rounding) vs oracle {(mine == ref_conv)[~det].mean():.4f} "
+              f"(BetterRobot vs oracle {(br_conv == ref_conv)[~det].mean():.4f}) reach {agree.mean():.4f} "
+              f"converged {int(mine.sum())}/{int(ref_conv.sum())}/{int(br_conv.sum())} (gpu/oracle/BetterRobot)")
         if precision == "f64":
             assert a_det >= 0.999, (c["name"], a_det)
             assert (mine == br_conv)[det].mean() >= 0.999, c["name"]
