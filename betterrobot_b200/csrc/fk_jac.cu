@@ -17,7 +17,11 @@
 //   * every output block of the configuration (J: n_targets*6*nv floats,
 //     poses: n*7 floats) is assembled in shared memory and written with one
 //     cp.async.bulk store (TMA bulk copy, full 128-B lines), so HBM sees only
-//     the algorithmic bytes.
+//     the algorithmic bytes.  A J block above 16 KB (all 32 joints of a humanoid:
+//     27.6 KB) goes out in pieces of a few targets through two alternating
+//     buffers, so that its size does not cap the warps per SM;
+//   * in from-poses mode (compute_joint_jacobians) the next configuration's
+//     placements are loaded into registers while the current one is written.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,6 +44,7 @@ struct FkParams {
   int32_t nt;
   uint32_t outputs;      // OUT_* bits
   uint32_t bulk;         // OUT_* bits whose blocks are 16-byte aligned -> TMA bulk store
+  int32_t chunk;         // targets per staged piece of the J block (>= nt: the whole block)
   int32_t targets[BR_MAX_TARGETS];
 };
 
@@ -51,7 +56,11 @@ struct Layout {
   // per-warp regions
   int q, poseT, poseQ, anc, colA, colO, tgt, sJ, sT, sOMi, sLiMi;
   int warp_floats;
-  __host__ __device__ Layout(int nj, int nq, int nv, int nt, uint32_t outputs) {
+  // chunk: targets per staged piece of a configuration's J block.  chunk >= nt stages the
+  // whole block in one buffer; a smaller (even) chunk stages it piece by piece in two
+  // alternating buffers, so a large block (all joints of a humanoid: 27.6 KB) does not
+  // limit the warps per SM.
+  __host__ __device__ Layout(int nj, int nq, int nv, int nt, uint32_t outputs, int chunk) {
     int o = 0;
     parent = o; o += round4(nj);
     jtype = o; o += round4(nj);
@@ -76,7 +85,7 @@ struct Layout {
     colA = o; o += 4 * nv;                                       // world column axis
     colO = o; o += 4 * nv;                                       // world column origin
     tgt = o; o += 8 * nt;
-    sJ = o; o += (outputs & OUT_JAC) ? round4(nt * 6 * nv) : 0;
+    sJ = o; o += (outputs & OUT_JAC) ? (chunk < nt ? 2 * round4(chunk * 6 * nv) : round4(nt * 6 * nv)) : 0;
     sT = o; o += (outputs & OUT_TPOSE) ? round4(nt * 7) : 0;
     sOMi = o; o += (outputs & OUT_OMI) ? round4(nj * 7) : 0;
     sLiMi = o; o += (outputs & OUT_LIMI) ? round4(nj * 7) : 0;
@@ -89,7 +98,8 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
   extern __shared__ __align__(16) float smem[];
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, nt = p.nt;
   const bool want_jac = (p.outputs & OUT_JAC) != 0;
-  const Layout L(nj, nq, nv, nt, p.outputs);
+  const Layout L(nj, nq, nv, nt, p.outputs, p.chunk);
+  const bool chunked = want_jac && p.chunk < nt;
   float* cta = smem;
   int* s_parent = reinterpret_cast<int*>(cta + L.parent);
   int* s_jtype = reinterpret_cast<int*>(cta + L.jtype);
@@ -178,7 +188,8 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
   float* sT = w + L.sT;
   float* sOMi = w + L.sOMi;
   float* sLiMi = w + L.sLiMi;
-  if (want_jac) {
+  const int cfl = chunked ? round4(p.chunk * 6 * nv) : 0;  // floats per chunk buffer
+  if (want_jac && !chunked) {  // the chunked staging buffers are cleared before each piece
     const int n = round4(nt * 6 * nv) / 4;
     for (int i = lane; i < n; i += kWarp) reinterpret_cast<float4*>(sJ)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
@@ -198,6 +209,18 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
       qn[k] = i < nq ? __ldg(p.q + b0 * nq + i) : 0.f;
     }
   }
+  // likewise the next configuration's joint placements in from-poses mode
+  // (nj * 7 <= BR_MAX_JOINTS * 7 = 448 floats: at most 14 values per lane)
+  constexpr int kPoseRegs = (BR_MAX_JOINTS * 7 + kWarp - 1) / kWarp;
+  float on[kPoseRegs];
+  if (!kFromQ && b0 < p.batch) {
+#pragma unroll
+    for (int k = 0; k < kPoseRegs; ++k) {
+      const int i = lane + kWarp * k;
+      on[k] = i < nj * 7 ? __ldg(p.oMi_in + b0 * nj * 7 + i) : 0.f;
+    }
+  }
+  uint32_t gc = 0;  // staged J pieces so far: piece gc uses buffer gc & 1
   for (int64_t b = b0; b < p.batch; b += stride) {
     // ---- world joint placements --------------------------------------
     if (kFromQ) {
@@ -269,13 +292,23 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
         }
       }
     } else {
-      const float* ob = p.oMi_in + b * (int64_t)nj * 7;
-      if (lane == 0) bulk_wait_read_all();
-      __syncwarp();
-      for (int i = lane; i < nj * 7; i += kWarp) {
-        const int j = i / 7, c = i - 7 * j;
-        if (c < 3) wpT[4 * j + c] = __ldg(ob + i);
-        else wpQ[4 * j + c - 3] = __ldg(ob + i);
+      if (!chunked && lane == 0) bulk_wait_read_all();  // the whole-block buffer is free again
+#pragma unroll
+      for (int k = 0; k < kPoseRegs; ++k) {
+        const int i = lane + kWarp * k;
+        if (i < nj * 7) {
+          const int j = i / 7, c = i - 7 * j;
+          if (c < 3) wpT[4 * j + c] = on[k];
+          else wpQ[4 * j + c - 3] = on[k];
+        }
+      }
+      const int64_t bn = b + stride;
+      if (bn < p.batch) {
+#pragma unroll
+        for (int k = 0; k < kPoseRegs; ++k) {
+          const int i = lane + kWarp * k;
+          on[k] = i < nj * 7 ? __ldg(p.oMi_in + bn * nj * 7 + i) : 0.f;
+        }
       }
       __syncwarp();
     }
@@ -296,35 +329,72 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
     }
     __syncwarp();
 
-    if (want_jac) {
+    // the six entries of J column c for target s, rows nv floats apart from dst
+    auto jac_pair = [&](int s, int c, float* dst) {
+      const float4 a4 = *reinterpret_cast<const float4*>(wcA + 4 * c);
+      const float3 a = f3(a4.x, a4.y, a4.z);
+      float3 lin, ang;
+      if (s_ckind[c] == 0) {
+        const float4 o4 = *reinterpret_cast<const float4*>(wcO + 4 * c);
+        const float3 o = f3(o4.x, o4.y, o4.z);
+        if (kRef == BR_REF_WORLD) {
+          lin = cross(o, a);                                   // hat(p_j) R S_ang  (jacobian.py:290-296)
+        } else {
+          const float4 pt = *reinterpret_cast<const float4*>(wtgt + 8 * s);
+          lin = cross(a, sub(f3(pt.x, pt.y, pt.z), o));        // J_lin - hat(p_f) J_ang (jacobian.py:213-215)
+        }
+        ang = a;
+      } else {
+        lin = a;
+        ang = f3(0.f, 0.f, 0.f);
+      }
+      if (kRef == BR_REF_LOCAL) {                              // R_f^T rows (jacobian.py:219-225)
+        const float4 qt = *reinterpret_cast<const float4*>(wtgt + 8 * s + 4);
+        lin = qrot_inv(qt, lin);
+        ang = qrot_inv(qt, ang);
+      }
+      dst[0] = lin.x; dst[nv] = lin.y; dst[2 * nv] = lin.z;
+      dst[3 * nv] = ang.x; dst[4 * nv] = ang.y; dst[5 * nv] = ang.z;
+    };
+    if (want_jac && !chunked) {
       for (int idx = lane; idx < npairs; idx += kWarp) {
         const int pr = s_pairs[idx];
         const int s = pr >> 8, c = pr & 255;
-        const float4 a4 = *reinterpret_cast<const float4*>(wcA + 4 * c);
-        const float3 a = f3(a4.x, a4.y, a4.z);
-        float3 lin, ang;
-        if (s_ckind[c] == 0) {
-          const float4 o4 = *reinterpret_cast<const float4*>(wcO + 4 * c);
-          const float3 o = f3(o4.x, o4.y, o4.z);
-          if (kRef == BR_REF_WORLD) {
-            lin = cross(o, a);                                   // hat(p_j) R S_ang  (jacobian.py:290-296)
-          } else {
-            const float4 pt = *reinterpret_cast<const float4*>(wtgt + 8 * s);
-            lin = cross(a, sub(f3(pt.x, pt.y, pt.z), o));        // J_lin - hat(p_f) J_ang (jacobian.py:213-215)
+        jac_pair(s, c, sJ + s * 6 * nv + c);
+      }
+    }
+    if (chunked) {
+      // targets [t0, t1) at a time: clear a buffer, fill the piece's (target, column) pairs,
+      // store it; the other buffer's store is still reading while this one is filled
+      const bool bulkJ = (p.bulk & OUT_JAC) != 0;
+      float* gJ = p.jac + b * (int64_t)nt * 6 * nv;
+      for (int t0 = 0; t0 < nt; t0 += p.chunk) {
+        const int t1 = t0 + p.chunk < nt ? t0 + p.chunk : nt;
+        float* buf = sJ + (int)(gc & 1u) * cfl;
+        ++gc;
+        if (bulkJ && lane == 0) bulk_wait_read<1>();         // the store two pieces back has read buf
+        __syncwarp();
+        for (int i = lane; i < cfl / 4; i += kWarp) reinterpret_cast<float4*>(buf)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+        const int e1 = t1 < nt ? s_pairoff[t1] : npairs;
+        for (int idx = s_pairoff[t0] + lane; idx < e1; idx += kWarp) {
+          const int pr = s_pairs[idx];
+          const int s = pr >> 8, c = pr & 255;
+          jac_pair(s, c, buf + (s - t0) * 6 * nv + c);
+        }
+        const int n = (t1 - t0) * 6 * nv;
+        if (bulkJ) {
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            bulk_store(gJ + (int64_t)t0 * 6 * nv, buf, (uint32_t)n * 4u);
+            bulk_commit();
           }
-          ang = a;
         } else {
-          lin = a;
-          ang = f3(0.f, 0.f, 0.f);
+          __syncwarp();
+          warp_copy(gJ + (int64_t)t0 * 6 * nv, buf, n, lane);
         }
-        if (kRef == BR_REF_LOCAL) {                              // R_f^T rows (jacobian.py:219-225)
-          const float4 qt = *reinterpret_cast<const float4*>(wtgt + 8 * s + 4);
-          lin = qrot_inv(qt, lin);
-          ang = qrot_inv(qt, ang);
-        }
-        float* dst = sJ + s * 6 * nv + c;
-        dst[0] = lin.x; dst[nv] = lin.y; dst[2 * nv] = lin.z;
-        dst[3 * nv] = ang.x; dst[4 * nv] = ang.y; dst[5 * nv] = ang.z;
+        __syncwarp();
       }
     }
 
@@ -340,7 +410,7 @@ __global__ void fk_jac_kernel(const br_tree_t tree, const FkParams p) {
     bool issued = false;
 #pragma unroll
     for (int o = 0; o < 4; ++o) {
-      if (!(p.outputs & outs[o].bit) || outs[o].n == 0) continue;
+      if (!(p.outputs & outs[o].bit) || outs[o].n == 0 || (chunked && outs[o].bit == OUT_JAC)) continue;
       if (p.bulk & outs[o].bit) {
         if (lane == 0) bulk_store(outs[o].g, outs[o].s, (uint32_t)outs[o].n * 4u);
         issued = true;
@@ -385,10 +455,21 @@ int validate_tree(const br_tree_t* t) {
 
 static int g_warps_per_cta = 8;
 
+// A configuration's J block above kWholeBlockBytes is staged in pieces of about
+// kPieceBytes (an even number of targets, so that every piece starts and ends on a
+// 16-byte boundary of a 16-byte aligned block).
+constexpr int kWholeBlockBytes = 16384, kPieceBytes = 4096;
+
 template <int kRef, bool kFromQ>
-static int launch_fk(const br_tree_t& tree, const FkParams& p, cudaStream_t stream) {
+static int launch_fk(const br_tree_t& tree, FkParams p, cudaStream_t stream) {
   if (p.batch == 0) return BR_OK;
-  const Layout L(tree.njoints, tree.nq, tree.nv, p.nt, p.outputs);
+  p.chunk = p.nt;
+  const int64_t jbytes = (int64_t)p.nt * 6 * tree.nv * 4;
+  if ((p.outputs & OUT_JAC) && tree.nv > 0 && jbytes > kWholeBlockBytes) {
+    int ch = (kPieceBytes / (6 * tree.nv * 4)) & ~1;
+    p.chunk = ch < 2 ? 2 : ch;
+  }
+  const Layout L(tree.njoints, tree.nq, tree.nv, p.nt, p.outputs, p.chunk);
   const DeviceInfo& dev = device_info();
   int wpc = g_warps_per_cta;
   size_t bytes = 0;

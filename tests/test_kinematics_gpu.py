@@ -102,9 +102,9 @@ def test_frame_jacobians_match_oracle(robot, reference, B):
 
 @pytest.mark.parametrize("reference", ["world", "local_world_aligned", "local"])
 def test_large_jacobian_blocks_match_oracle(reference):
-    """Every frame of the humanoid (44: a 38 KB Jacobian block per configuration, which leaves
-    room for four warps per CTA), and all 32 joints from stored placements
-    (compute_joint_jacobians), against the oracle; B = 129 leaves partial CTAs."""
+    """Every frame of the humanoid (44: a 38 KB Jacobian block per configuration, staged and
+    stored in pieces of four targets), and all 32 joints from stored placements
+    (compute_joint_jacobians, 27.6 KB blocks), against the oracle; B = 129 leaves partial CTAs."""
     m = syn.model_from_spec(SPECS["humanoid"])
     m64 = syn.model_from_spec(SPECS["humanoid"], dtype=torch.float64)
     q = syn.random_q(m64, 129, 91, rev_range=2.5, base_translation=1.0)
@@ -116,6 +116,23 @@ def test_large_jacobian_blocks_match_oracle(reference):
     if reference == "world":
         data = br.compute_joint_jacobians(m, br.forward_kinematics(m, q.float().cuda()))
         assert_jac(data.joint_jacobians, K.compute_joint_jacobians(m64, oMi, q.numpy()))
+
+
+@pytest.mark.parametrize("reference", ["world", "local_world_aligned", "local"])
+def test_large_unaligned_jacobian_blocks_in_pieces(reference):
+    """A 33-DOF chain with 21 body frames: a 16.6 KB J block per configuration, staged in pieces
+    of four targets, whose 3,168 B pieces and 16,632 B block are stored lane by lane (21 x 33 is
+    odd: the block is not a multiple of 16 bytes); B = 70 leaves partial CTAs."""
+    spec = syn.chain_spec(seed=12, n=33, name="chain33")
+    m = syn.model_from_spec(spec)
+    m64 = syn.model_from_spec(spec, dtype=torch.float64)
+    fids = [m.frame_id(f"body_link{i}") for i in (*range(3, 34, 3), *range(1, 31, 3))]
+    assert len(fids) == 21
+    q = syn.random_q(m64, 70, 17)
+    T, J = br.frame_jacobians(m, q.float().cuda(), fids, reference=reference)
+    oMi, _ = K.forward_kinematics(m64, q.numpy())
+    assert_poses(T, K.frame_placements(m64, oMi, fids))
+    assert_jac(J, np.stack([K.frame_jacobian(m64, oMi, q.numpy(), f, reference) for f in fids], -3))
 
 
 def test_unaligned_output_fallback_chain():
