@@ -215,20 +215,22 @@ __device__ __forceinline__ void apply_op(const float* x, const float* y, float* 
   }
 }
 
-// Copy `len` floats between a warp's shared-memory tile and global memory, coalesced: 16-byte
-// accesses while both sides allow them (`vec`: the global slab starts on a 16-byte boundary;
-// tiles start on one), then single floats for the remainder.
-__device__ __forceinline__ void warp_load(float* __restrict__ s, const float* __restrict__ g, int len, int lane,
-                                          bool vec) {
+// Start copying `len` floats of a global slab into a warp's shared-memory tile without passing
+// through registers: 16-byte cp.async while both sides allow it (`vec`: the slab starts on a
+// 16-byte boundary; tiles start on one), then 4-byte copies for the remainder.  The caller
+// commits the group and waits for it.
+__device__ __forceinline__ void warp_load_async(float* __restrict__ s, const float* __restrict__ g, int len,
+                                                int lane, bool vec) {
   int k0 = 0;
   if (vec) {
     const int n4 = len >> 2;
-    for (int k = lane; k < n4; k += kWarp)
-      reinterpret_cast<float4*>(s)[k] = __ldg(reinterpret_cast<const float4*>(g) + k);
+    for (int k = lane; k < n4; k += kWarp) cp_async16(s + 4 * k, g + 4 * k);
     k0 = n4 << 2;
   }
-  for (int k = k0 + lane; k < len; k += kWarp) s[k] = __ldg(g + k);
+  for (int k = k0 + lane; k < len; k += kWarp) cp_async4(s + k, g + k);
 }
+// Copy `len` floats of a warp's output tile to global memory, coalesced (16-byte stores while
+// the destination allows them).
 __device__ __forceinline__ void warp_store(float* __restrict__ g, const float* __restrict__ s, int len, int lane,
                                            bool vec) {
   int k0 = 0;
@@ -243,39 +245,58 @@ __device__ __forceinline__ void warp_store(float* __restrict__ g, const float* _
 constexpr int kLieWarps = 8;  // warps per CTA
 
 // One warp per tile of 32 consecutive elements: the tile's operand records (contiguous slabs
-// of 32 * floats-per-record) are copied into the warp's shared memory with coalesced loads,
-// each lane applies the op to its element, and the output slab leaves the same way.  A
-// broadcast operand (one record for every element) is read in place.
+// of 32 * floats-per-record) are copied into the warp's shared memory by cp.async, the NEXT
+// tile's into a second buffer while this one is computed where shared memory allows (so a
+// warp keeps a whole tile of loads in flight), each lane applies the op to its element, and the output slab leaves with
+// coalesced stores.  A broadcast operand (one record for every element) is read in place.
 template <int OP>
 __global__ void __launch_bounds__(kLieWarps * kWarp) lie_ops_kernel(const float* __restrict__ a,
                                                                    const float* __restrict__ b, int64_t n,
                                                                    int a_bcast, int b_bcast, float* __restrict__ out) {
   constexpr LieOpSpec sp = lie_spec(OP);
   constexpr int A = sp.a, Bn = sp.b, O = sp.out;
-  constexpr int TILE = kWarp * (A + Bn + O);    // floats per warp (a multiple of 4: 16-byte tiles)
+  constexpr int IN = kWarp * (A + Bn);         // input floats per tile (a multiple of 4: 16-byte tiles)
+  // two input buffers and the output tile per warp, while the CTA's static shared memory allows
+  // (the 36-float outputs of the adjoint and Jr ops leave room for one input buffer only)
+  constexpr int NB = kLieWarps * (2 * IN + kWarp * O) * 4 <= 48 * 1024 ? 2 : 1;
+  constexpr int TILE = NB * IN + kWarp * O;
   __shared__ __align__(16) float smem[kLieWarps * TILE];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float* sa = smem + w * TILE;
-  float* sb = sa + kWarp * A;
-  float* so = sb + kWarp * Bn;
+  float* sbuf = smem + w * TILE;
+  float* so = sbuf + 2 * IN;
   const bool va = ((reinterpret_cast<uintptr_t>(a) & 15u) == 0), vb = ((reinterpret_cast<uintptr_t>(b) & 15u) == 0),
              vo = ((reinterpret_cast<uintptr_t>(out) & 15u) == 0);
   const int64_t ntiles = (n + kWarp - 1) / kWarp;
-  for (int64_t t = (int64_t)blockIdx.x * kLieWarps + w; t < ntiles; t += (int64_t)gridDim.x * kLieWarps) {
+  const int64_t step = (int64_t)gridDim.x * kLieWarps;
+  auto fetch = [&](int64_t t, float* buf) {  // issue tile t's operand copies into buf
     const int64_t i0 = t * kWarp;
     const int cnt = (int)((n - i0) < kWarp ? (n - i0) : kWarp);
-    if (!a_bcast) warp_load(sa, a + i0 * A, cnt * A, lane, va);
-    if (Bn && !b_bcast) warp_load(sb, b + i0 * Bn, cnt * Bn, lane, vb);
+    if (!a_bcast) warp_load_async(buf, a + i0 * A, cnt * A, lane, va);
+    if (Bn && !b_bcast) warp_load_async(buf + kWarp * A, b + i0 * Bn, cnt * Bn, lane, vb);
+  };
+  int64_t t = (int64_t)blockIdx.x * kLieWarps + w;
+  if (NB == 2 && t < ntiles) fetch(t, sbuf);
+  cp_async_commit();
+  for (int k = 0; t < ntiles; t += step, ++k) {
+    float* cur = sbuf + (NB == 2 ? (k & 1) * IN : 0);
+    if (NB == 1) fetch(t, cur);
+    else if (t + step < ntiles) fetch(t + step, sbuf + ((k + 1) & 1) * IN);
+    cp_async_commit();
+    if (NB == 2) cp_async_wait_groups<1>();    // this tile's copies are done (the next one's may fly)
+    else cp_async_wait_groups<0>();
     __syncwarp();
+    const int64_t i0 = t * kWarp;
+    const int cnt = (int)((n - i0) < kWarp ? (n - i0) : kWarp);
     if (lane < cnt) {
-      const float* x = a_bcast ? a : sa + lane * A;
-      const float* y = Bn ? (b_bcast ? b : sb + lane * Bn) : nullptr;
+      const float* x = a_bcast ? a : cur + lane * A;
+      const float* y = Bn ? (b_bcast ? b : cur + kWarp * A + lane * Bn) : nullptr;
       apply_op<OP>(x, y, so + lane * O);
     }
     __syncwarp();
     warp_store(out + i0 * O, so, cnt * O, lane, vo);
-    __syncwarp();
+    __syncwarp();                              // cur and so are free for the next tiles
   }
+  cp_async_wait_all();
 }
 
 template <int OP>
