@@ -16,7 +16,15 @@ A step solves the whole batch once.
            targets and q0 host->device, solves, copies q / status / iterations back;
   plain_gpu = the same method as plain per-op PyTorch on the same GPU;
   roofline  = the fused FK + frame-Jacobian kernel on the free-flyer humanoid
-           (B = 65,536, 12 frames) against the measured HBM copy bandwidth.
+           (B = 65,536, 12 frames) against the measured HBM copy bandwidth;
+  roofline_lm = the LM launch's throughput in the reference's dense-iteration FLOPs
+           against the nominal FP32 CUDA-core peak;
+  ik_f64_normal_equations, adjoint, trajopt, lie_ops, joint_jacobians = the other
+           kernels of the path (float64 normal equations on the same mix; pose-loss
+           forward + backward; 256 x 64-knot trajectories; SE3 compose / log / exp on
+           8.4 M elements; all 32 joint Jacobians of the humanoid at B = 16,384), the
+           HBM-bound ones with their fraction of the measured copy bandwidth;
+  cpu_baseline(s) = the reference algorithm (float64 port) on the host cores.
 
 Multi-GPU: problems are independent, so N GPUs run N replicas on disjoint
 problem sets with no data-path collective (weak scaling); time is the max over
@@ -868,6 +876,8 @@ def main():
     fkj = bench_fkj(args.steps, warmup)
     adj = bench_adjoint(args.steps, warmup) if not args.no_adjoint else None
     trj = bench_trajopt(args.steps, warmup) if not args.no_adjoint else None
+    lie_r = bench_lie(args.steps, warmup)
+    jj = bench_joint_jacobians(args.steps, warmup)
     plain = bench_plain_gpu(ik["wl"]) if (rank == 0 and not args.no_plain) else None
     ms = reduce(ik["ms"], world, "max")
     reached = reduce(ik["reached"], world, "sum")
@@ -905,6 +915,9 @@ def main():
         line["adjoint"] = adj
     if trj is not None:
         line["trajopt"] = trj
+    line["lie_ops"] = {k: {**v, "frac_of_peak": v["gbs"] / peak} for k, v in lie_r.items()}
+    line["joint_jacobians"] = {**jj, "frac_of_peak": jj["gbs"] / peak,
+                               "kernel": "fk_jac_kernel (from poses: humanoid, all 32 joints, world)"}
     if plain is not None:
         line["plain_gpu"] = {"value": plain["reached"] / plain["sec"], "unit": "solves/s", "sec_per_step": plain["sec"],
                              "reached_1e-4": plain["reached"], "speedup_fused_over_plain":
