@@ -146,11 +146,31 @@ __device__ __forceinline__ void jr_inv_T_xi(float3 v, float3 w, float3& gl, floa
   ga = sub(w, vinv(q));
 }
 
-// SE3 log -> (v, w)   (se3_log, _torch_native_backend.py:289-310)
+// SE3 log -> (v, w)   (se3_log, _torch_native_backend.py:289-310).  The rotation part as
+// so3_log; the V^-1 coefficient c = 1/th^2 - cot(th/2) / (2 th) takes cot(th/2) = |q_w| / s
+// from the quaternion itself (th / 2 = atan2(s, |q_w|)), so no trigonometric call is needed
+// beyond the atan2 (the series of vinv_coeff below th = 1, where the closed form cancels).
 __device__ __forceinline__ void se3_log(const Pose& T, float3& v, float3& w) {
-  w = so3_log(T.q);
+  float4 q = T.q;
+  if (q.w < 0.f) q = make_float4(-q.x, -q.y, -q.z, -q.w);
+  const float s2 = q.x * q.x + q.y * q.y + q.z * q.z;
+  const float s = sqrtf(s2);
+  const float qw = fminf(fmaxf(q.w, -1.f), 1.f);
+  float factor;
+  if (s2 < 0.25e-8f) {
+    factor = 2.f + s2 * (2.f / 3.f);
+  } else {
+    factor = 2.f * atan2f(s, qw) / s;
+  }
+  w = f3(factor * q.x, factor * q.y, factor * q.z);
   const float th2 = dot(w, w);
-  const float c = vinv_coeff(th2);
+  float c;
+  if (th2 < 1.f) {
+    c = vinv_coeff(th2);
+  } else {
+    const float th = sqrtf(th2);
+    c = 1.f / th2 - qw / (2.f * s * th);
+  }
   // V^-1 t = t - 1/2 w x t + c w x (w x t)
   const float3 wt = cross(w, T.t);
   v = axpy(c, cross(w, wt), axpy(-0.5f, wt, T.t));
@@ -222,14 +242,33 @@ __device__ __forceinline__ Pose se3_exp_step(float3 v, float3 w) {
   return T;
 }
 
-// se3_exp (_torch_native_backend.py:258-286): T = (V(w) v, exp(w))
+// se3_exp (_torch_native_backend.py:258-286): T = (V(w) v, exp(w)).  Below th = 1 the series
+// of exp_coeffs and of sin(th/2)/th, cos(th/2); beyond, one sincos of th/2 gives them all
+// (sin th = 2 sin(th/2) cos(th/2), 1 - cos th = 2 sin^2(th/2)).
 __device__ __forceinline__ Pose se3_exp(float3 v, float3 w) {
-  float b, c;
-  exp_coeffs(dot(w, w), b, c);
+  const float th2 = dot(w, w);
+  float b, c, k, cw;
+  if (th2 < 1.f) {
+    exp_coeffs(th2, b, c);
+    const float x2 = 0.25f * th2;  // (th / 2)^2
+    // sin(x)/x = 1 - x^2/6 + x^4/120 - x^6/5040 + x^8/362880; k = sin(th/2)/th = (sin(x)/x) / 2
+    k = 0.5f * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 1.f / 362880.f, -1.f / 5040.f), 1.f / 120.f), -1.f / 6.f), 1.f);
+    // cos(x) = 1 - x^2/2 + x^4/24 - x^6/720 + x^8/40320 - x^10/3628800
+    cw = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -1.f / 3628800.f, 1.f / 40320.f), -1.f / 720.f), 1.f / 24.f),
+                   -0.5f), 1.f);
+  } else {
+    const float th = sqrtf(th2);
+    float sh;
+    sincospif(th * (0.5f / 3.14159265358979f), &sh, &cw);
+    const float it = 1.f / th;
+    b = 2.f * sh * sh * (it * it);
+    c = (th - 2.f * sh * cw) * (it * it * it);
+    k = sh * it;
+  }
   const float3 wv = cross(w, v);
   Pose T;
   T.t = axpy(c, cross(w, wv), axpy(b, wv, v));
-  T.q = so3_exp(w);
+  T.q = make_float4(k * w.x, k * w.y, k * w.z, cw);
   return T;
 }
 
