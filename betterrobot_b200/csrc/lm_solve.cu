@@ -844,13 +844,23 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     const int ndl = misc[1];
 #pragma unroll 1
     for (int dl = 0; dl < ndl; ++dl) {
+      // this depth's factor entries and ancestors do not depend on the synchronisation below:
+      // loaded before it, so that only the ancestor's delta is read after it
+      R lf[NR];
+      int an[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const bool deeper = dr[r] > dl;
+        lf[r] = deeper ? Lm[ror[r] + dl] : (R)0;
+        an[r] = deeper ? ancd[(tl + T * r) * L.anc_stride + dl] : 0;
+      }
 #pragma unroll
       for (int r = 0; r < NR; ++r)
         if (dr[r] == dl) delta[tl + T * r] = zr[r] * dvr[r];
       tm.sync();
 #pragma unroll
       for (int r = 0; r < NR; ++r)
-        if (dr[r] > dl) zr[r] = rfma(-Lm[ror[r] + dl], delta[ancd[(tl + T * r) * L.anc_stride + dl]], zr[r]);
+        if (dr[r] > dl) zr[r] = rfma(-lf[r], delta[an[r]], zr[r]);
     }
     tm.sync();
     return true;
