@@ -794,10 +794,17 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
     const int toff = (5 + nlev + 3) & ~3;
     const uint4* tasks = reinterpret_cast<const uint4*>(sched + toff);
     const uint2* extra = reinterpret_cast<const uint2*>(sched + toff + 4 * (int)sched[1]);
+    // this lane's first task of level l + 1 is loaded during level l (its index clamped to the
+    // last task, used only when it lies in level l + 1)
+    const int last = (int)sched[1] - 1;
+    int t0 = 0;
+    uint4 first = last >= 0 ? __ldg(tasks + (tl < last ? tl : last)) : make_uint4(0u, 0u, 0u, 0u);
     for (int l = 0; l < nlev; ++l) {
       const int t1 = (int)__ldg(sched + 5 + l);
-      int p = (int)__ldg(sched + 4 + l) + tl;
-      uint4 nx = p < t1 ? __ldg(tasks + p) : make_uint4(0u, 0u, 0u, 0u);
+      int p = t0 + tl;
+      uint4 nx = p < t1 ? first : make_uint4(0u, 0u, 0u, 0u);
+      if (last >= 0) first = __ldg(tasks + (t1 + tl < last ? t1 + tl : last));
+      t0 = t1;
       for (; p < t1; p += T) {
         const uint4 tk = nx;                                   // the next pass's task is in flight
         if (p + T < t1) nx = __ldg(tasks + p + T);
