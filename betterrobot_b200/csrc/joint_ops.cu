@@ -39,9 +39,13 @@ struct JointOpParams {
 
 constexpr int kJointOpsWarps = 4;
 
-// Floats of shared memory one warp stages per tile.
+// Floats of shared memory one warp stages.  integrate: two input tiles (the next one is
+// copied while this one is computed).  difference: one input tile and the free-flyer
+// outputs of that tile (its float64 logs make it compute heavy: measured at 1 M humanoid
+// configurations, a second tile halves the warps per SM and cost 104 -> 162 us).
+__host__ __device__ inline int joint_ops_in_floats(int nq, int nv, bool diff) { return 32 * (diff ? 2 * nq : nq + nv); }
 __host__ __device__ inline int joint_ops_warp_floats(int nq, int nv, bool diff) {
-  return 32 * (diff ? 2 * nq + nv : nq + nv);
+  return diff ? joint_ops_in_floats(nq, nv, diff) + 32 * nv : 2 * joint_ops_in_floats(nq, nv, diff);
 }
 
 __device__ __forceinline__ DPose dpose7(const float* p) {
@@ -97,18 +101,35 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
   const int warps = blockDim.x >> 5;
   const int lb = diff ? nq : nv;  // floats per configuration of b
   const int lo = diff ? nv : nq;  // floats per configuration of out
-  float* A = slabs + (size_t)(threadIdx.x >> 5) * joint_ops_warp_floats(nq, nv, diff);
-  float* Bs = A + 32 * nq;
-  float* O = Bs + 32 * lb;        // difference: free-flyer outputs, v-shaped
+  const int IN = joint_ops_in_floats(nq, nv, diff);
+  float* base = slabs + (size_t)(threadIdx.x >> 5) * joint_ops_warp_floats(nq, nv, diff);
+  float* O = base + IN;           // difference: free-flyer outputs, v-shaped
+  const bool dbl = kVec && !diff; // integrate with 16-byte copies: next tile in flight
   const int64_t tiles = (p.batch + 31) >> 5;
+  const int64_t step = (int64_t)gridDim.x * warps;
   const int n_ff = nff;
-  for (int64_t tile = (int64_t)blockIdx.x * warps + (threadIdx.x >> 5); tile < tiles;
-       tile += (int64_t)gridDim.x * warps) {
+  auto fetch = [&](int64_t t, float* buf) {  // the tile's rows of both inputs into buf
+    const int64_t b = t << 5;
+    const int c = p.batch - b < 32 ? (int)(p.batch - b) : 32;
+    slab_in<kVec>(buf, p.a + b * nq, c * nq, lane);
+    slab_in<kVec>(buf + 32 * nq, p.b + b * lb, c * lb, lane);
+  };
+  int64_t tile = (int64_t)blockIdx.x * warps + (threadIdx.x >> 5);
+  if (dbl && tile < tiles) fetch(tile, base);
+  if (dbl) cp_async_commit();
+  for (int k = 0; tile < tiles; tile += step, ++k) {
     const int64_t b0 = tile << 5;
     const int cnt = p.batch - b0 < 32 ? (int)(p.batch - b0) : 32;
-    slab_in<kVec>(A, p.a + b0 * nq, cnt * nq, lane);
-    slab_in<kVec>(Bs, p.b + b0 * lb, cnt * lb, lane);
-    if (kVec) cp_async_wait_all();
+    float* A = dbl ? base + (k & 1) * IN : base;
+    float* Bs = A + 32 * nq;
+    if (dbl) {  // the next tile's copies are issued before this one is computed
+      if (tile + step < tiles) fetch(tile + step, base + ((k + 1) & 1) * IN);
+      cp_async_commit();
+      cp_async_wait_groups<1>();
+    } else {
+      fetch(tile, A);
+      if (kVec) cp_async_wait_all();
+    }
     __syncwarp();
     if (lane < cnt) {
       for (int f = 0; f < n_ff; ++f) {
@@ -192,8 +213,9 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
       const int c = e / lo;
       go[e] = val(c, e - c * lo);
     }
-    __syncwarp();  // the next tile overwrites the slabs
+    __syncwarp();  // this tile's buffer and O are free for the tiles after the next
   }
+  if (kVec) cp_async_wait_all();
 }
 
 }  // namespace br
