@@ -463,6 +463,9 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
   };
 
   // float64 residual of the stack at q with world poses `pose`: fills tw, xi, dr; returns 0.5 |r|^2.
+  // the parent joint of this lane's first target, read once: the residual's first pose load
+  // then follows FK's last barrier directly
+  const int fpar_own = tl < nt ? fparent[tl] : 0;
   auto residual = [&](const double* q, const double* pose) -> double {
     double acc = 0.0;
     // one pass over the targets (jobs 0..nt-1) and, for the rest term, the joints (jobs
@@ -475,7 +478,7 @@ __device__ void solve_problem(const LmParams& P, const br_tree_t& tree, int prob
       double wv = 0.0, ww = 0.0;
       if (jb < nt) {
         const int t = jb;
-        const DPose Tee = dcompose(lds(pose, nj, fparent[t]), to_d(ld8(fplace + 8 * t)));
+        const DPose Tee = dcompose(lds(pose, nj, jb < T ? fpar_own : fparent[t]), to_d(ld8(fplace + 8 * t)));
         std8(tw + 8 * t, Tee);
         double* e = xi + 8 * t;
         const DPose Tt = ldd(tgt + 8 * t);
