@@ -561,7 +561,7 @@ extern "C" int br_frame_jacobians(const br_tree_t* tree, const float* q, int64_t
                                   float* jacobians, void* stream) {
   int st = validate_tree(tree);
   if (st) return st;
-  if (batch < 0 || (batch > 0 && tree->nq > 0 && !q) || !jacobians) return BR_EINVAL;
+  if (batch < 0 || (batch > 0 && ((tree->nq > 0 && !q) || !jacobians))) return BR_EINVAL;  // B = 0: empty buffers
   if (!aligned4(q) || !aligned4(jacobians) || (target_pose_world && !aligned4(target_pose_world))) return BR_EALIGN;
   FkParams p = {};
   p.q = q;
@@ -581,7 +581,7 @@ extern "C" int br_frame_jacobians_from_poses(const br_tree_t* tree, const float*
                                              float* jacobians, void* stream) {
   int st = validate_tree(tree);
   if (st) return st;
-  if (batch < 0 || (batch > 0 && !joint_pose_world) || !jacobians) return BR_EINVAL;
+  if (batch < 0 || (batch > 0 && (!joint_pose_world || !jacobians))) return BR_EINVAL;  // B = 0: empty buffers
   if (!aligned4(joint_pose_world) || !aligned4(jacobians)) return BR_EALIGN;
   FkParams p = {};
   p.oMi_in = joint_pose_world;

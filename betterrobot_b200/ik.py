@@ -185,7 +185,8 @@ class PackedIK:
         # per-problem layout: classes contiguous, in class order
         self.class_start = np.cumsum([0] + self.counts)[:-1]
         nq = np.concatenate([np.full(n, m.nq, np.int64) for n, m in zip(self.counts, models)])
-        self.q_offset_np = np.concatenate([[0], np.cumsum(nq)[:-1]]).astype(np.int64)
+        # P + 1 offsets (the last one is the total), so a class with no problems indexes in range
+        self.q_offset_np = np.concatenate([[0], np.cumsum(nq)]).astype(np.int64)
         self.q_total = int(nq.sum())
         nt_all = np.concatenate([np.asarray(n, np.int32) for n in n_targets])
         if (nt_all < 1).any() or (nt_all > self.K).any():
@@ -193,7 +194,7 @@ class PackedIK:
         fr = np.zeros((self.P, self.K), np.int32)
         for c in range(self.C):
             f = np.asarray(frame_ids[c], np.int32)
-            if f.min() < 0 or f.max() >= models[c].nframes:
+            if f.size and (f.min() < 0 or f.max() >= models[c].nframes):
                 raise ShapeError(f"class {c}: frame id out of range")
             s0 = self.class_start[c]
             fr[s0:s0 + self.counts[c], :f.shape[1]] = f
@@ -215,7 +216,7 @@ class PackedIK:
             s0 = self.class_start[c]
             dims.append(rows[s0:s0 + self.counts[c]].sum(-1) + 2 * m.nq + m.nv)
         rdim = np.concatenate(dims)
-        self.r_offset_np = np.concatenate([[0], np.cumsum(rdim)[:-1]]).astype(np.int64)
+        self.r_offset_np = np.concatenate([[0], np.cumsum(rdim)]).astype(np.int64)
         self.r_dim = rdim
         # work items: heaviest classes first, and inside a class the problems with the fewest
         # targets first (they run the most iterations: a less constrained problem's rest term
@@ -364,8 +365,11 @@ def solve_ik_batched(model, frame_ids, targets: torch.Tensor, initial_q: torch.T
             if cost_cfg.rest_weight > 0.0:
                 parts.append(r[..., nt_rows + 2 * model.nq:])
             return torch.cat(parts, -1) if len(parts) > 1 else parts[0]
-        res = (stack_rows(pk.residual.view(P, -1)) if (pk.r_dim == pk.r_dim[0]).all()
-               else [stack_rows(r) for r in torch.split(pk.residual, [int(d) for d in pk.r_dim])])
+        if P == 0:
+            res = pk.residual.view(0, 0)
+        else:
+            res = (stack_rows(pk.residual.view(P, -1)) if (pk.r_dim == pk.r_dim[0]).all()
+                   else [stack_rows(r) for r in torch.split(pk.residual, [int(d) for d in pk.r_dim])])
     return BatchIKResult(q=pk.q_of(0), iters=pk.iters, converged=(pk.status & 0xFF) == 0, status=pk.status,
                          cost=pk.cost, residual=res)
 

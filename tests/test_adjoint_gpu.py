@@ -129,3 +129,17 @@ def test_grad_output_scaling():
     q2 = q.detach().clone().requires_grad_(True)
     (g1,) = torch.autograd.grad(pose_loss(m, q2, fids, T, w).sum(), q2)
     torch.testing.assert_close(g, g1 * go[:, None], rtol=1e-6, atol=1e-6)
+
+
+def test_empty_batch_loss_and_gradient():
+    """B = 0: an empty loss and an empty gradient, no launch."""
+    from betterrobot_b200.adjoint import pose_loss
+    m = syn.model_from_spec(syn.humanoid_spec())
+    fids = syn.op_frame_ids(m)
+    q = torch.zeros(0, m.nq, device="cuda", requires_grad=True)
+    T = torch.zeros(0, len(fids), 7, device="cuda")
+    w = torch.ones(len(fids), device="cuda")
+    loss = pose_loss(m, q, fids, T, w)
+    assert loss.shape == (0,)
+    loss.sum().backward()
+    assert q.grad.shape == (0, m.nq)

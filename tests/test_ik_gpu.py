@@ -426,3 +426,15 @@ def test_position_orientation_targets_vs_oracle(robot, frames, kinds):
     ok, conv, dres = _agreement(out, ref.converged, ref.residual)
     assert (dres <= RES_TOL).mean() >= 0.9, np.sort(dres)[-8:]
     assert (conv == ref.converged).mean() >= 0.85, (conv.mean(), ref.converged.mean())
+
+
+def test_empty_problem_batch():
+    """P = 0 problems: empty results, no launch."""
+    m, _ = _models("chain7")
+    out = bik.solve_ik_batched(m, [m.frame_id("ee")], torch.zeros(0, 1, 7, device="cuda"),
+                               torch.zeros(0, m.nq, device="cuda"))
+    assert out.q.shape == (0, m.nq)
+    assert out.iters.shape == (0,) and out.converged.shape == (0,)
+    out = bik.solve_ik_batched(m, [m.frame_id("ee")], torch.zeros(0, 1, 7, device="cuda"),
+                               torch.zeros(0, m.nq, device="cuda"), with_residual=True)
+    assert out.q.shape == (0, m.nq) and out.residual.numel() == 0

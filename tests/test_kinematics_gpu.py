@@ -259,3 +259,20 @@ def test_integrate_difference_unaligned_pointers_match():
     integrate_into(m, shifted(q), shifted(v), out_q)
     difference_into(m, shifted(q), shifted(q1), out_v)
     assert torch.equal(out_q, ref_q) and torch.equal(out_v, ref_v)
+
+
+def test_empty_batches():
+    """B = 0 everywhere: outputs of shape (0, ...) and no launch."""
+    m = syn.model_from_spec(SPECS["humanoid"])
+    q = torch.zeros(0, m.nq, device="cuda")
+    data = br.forward_kinematics(m, q, compute_frames=True)
+    assert data.joint_pose_world.shape == (0, m.njoints, 7)
+    assert data.frame_pose_world.shape[0] == 0
+    fids = syn.op_frame_ids(m)
+    T, J = br.frame_jacobians(m, q, fids)
+    assert T.shape == (0, len(fids), 7) and J.shape == (0, len(fids), 6, m.nv)
+    br.compute_joint_jacobians(m, data)
+    assert data.joint_jacobians.shape == (0, m.njoints, 6, m.nv)
+    from betterrobot_b200.configuration import difference, integrate
+    assert integrate(m, q, torch.zeros(0, m.nv, device="cuda")).shape == (0, m.nq)
+    assert difference(m, q, q).shape == (0, m.nv)
