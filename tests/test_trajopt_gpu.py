@@ -244,3 +244,12 @@ def test_solve_trajopt_facade_matches_reference_golden():
         st.add("other", _ref_like("CollisionResidual"), 1.0)
         btr.solve_trajopt(m, horizon=T, dt=float(dt), initial_q_traj=X0.cuda(), cost_stack=st,
                           optimizer=_ref_like("GaussNewton", tol=1e-6, eps=1e-8))
+
+
+def test_empty_trajectory_batch():
+    """N = 0 trajectories: empty results, no launch."""
+    m = syn.model_from_spec(syn.chain_spec())
+    out = btr.solve_trajopt_batched(m, m.frame_id("ee"), torch.zeros(0, 7, device="cuda"),
+                                    torch.zeros(0, 16, m.nq, device="cuda"))
+    assert out.q.shape == (0, 16, m.nq)
+    assert out.converged.shape == (0,) and out.iters.shape == (0,)
