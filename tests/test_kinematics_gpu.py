@@ -103,7 +103,7 @@ def test_frame_jacobians_match_oracle(robot, reference, B):
 @pytest.mark.parametrize("reference", ["world", "local_world_aligned", "local"])
 def test_large_jacobian_blocks_match_oracle(reference):
     """Every frame of the humanoid (44: a 38 KB Jacobian block per configuration, staged and
-    stored in pieces of four targets), and all 32 joints from stored placements
+    stored in pieces of eight targets), and all 32 joints from stored placements
     (compute_joint_jacobians, 27.6 KB blocks), against the oracle; B = 129 leaves partial CTAs."""
     m = syn.model_from_spec(SPECS["humanoid"])
     m64 = syn.model_from_spec(SPECS["humanoid"], dtype=torch.float64)
@@ -121,8 +121,8 @@ def test_large_jacobian_blocks_match_oracle(reference):
 @pytest.mark.parametrize("reference", ["world", "local_world_aligned", "local"])
 def test_large_unaligned_jacobian_blocks_in_pieces(reference):
     """A 33-DOF chain with 21 body frames: a 16.6 KB J block per configuration, staged in pieces
-    of four targets, whose 3,168 B pieces and 16,632 B block are stored lane by lane (21 x 33 is
-    odd: the block is not a multiple of 16 bytes); B = 70 leaves partial CTAs."""
+    of ten targets (10, 10, 1), whose 7,920 B pieces and 16,632 B block are stored lane by lane
+    (21 x 33 is odd: the block is not a multiple of 16 bytes); B = 70 leaves partial CTAs."""
     spec = syn.chain_spec(seed=12, n=33, name="chain33")
     m = syn.model_from_spec(spec)
     m64 = syn.model_from_spec(spec, dtype=torch.float64)
