@@ -144,6 +144,8 @@ BR_API int br_forward_kinematics(const br_tree_t* tree, const float* q, int64_t 
  * reference frame `reference` (BR_REF_*), and if non-NULL target_pose_world
  * [batch, n_targets, 7].  Replaces forward_kinematics(..., compute_frames=True)
  * followed by get_frame_jacobian per frame (src/better_robot/kinematics/jacobian.py:129-227).
+ * batch == 0 launches nothing and accepts NULL buffers.  A J block above 16 KB per
+ * configuration is staged and stored in pieces of an even number of targets.
  */
 BR_API int br_frame_jacobians(const br_tree_t* tree, const float* q, int64_t batch,
                        const int32_t* targets, int32_t n_targets, int32_t reference,
@@ -155,6 +157,7 @@ BR_API int br_frame_jacobians(const br_tree_t* tree, const float* q, int64_t bat
  * encoding and output layout as br_frame_jacobians.  Replaces get_frame_jacobian
  * on a populated Data (jacobian.py:129-227) and, with targets = all joints and
  * BR_REF_WORLD, compute_joint_jacobians (jacobian.py:30-97, protocol.py:64-68).
+ * batch == 0 launches nothing and accepts NULL buffers.
  */
 BR_API int br_frame_jacobians_from_poses(const br_tree_t* tree, const float* joint_pose_world, int64_t batch,
                                   const int32_t* targets, int32_t n_targets, int32_t reference,
