@@ -168,6 +168,29 @@ def lm_iteration_flops(model, frame_ids) -> int:
     return f
 
 
+SE3_INVERSE_FLOPS = 33        # rotate (30) + negate (3)
+JR_INV_T_XI_FLOPS = 150       # closed-form Jr^-T(xi) xi: ~10 cross products, 3 coefficients, 4 axpys
+WRENCH_FLOPS = 72             # F = [R g_lin; p x R g_lin + R g_ang]
+COLUMN_TWIST_FLOPS = 40       # world column S_c = [o x a; a] from its joint pose
+PAIR_FLOPS = 11               # <S_c, F_f> per (frame, supporting column)
+
+
+def adjoint_flops_per_config(model, frame_ids, recompute: bool) -> int:
+    """Algorithmic flops of the pose loss and its gradient for one configuration: FK (one
+    local transform and one compose per joint), per frame its placement, the target's inverse,
+    the error pose, its log and weighted square; backward: the same FK and frame poses again
+    when ``recompute``, per frame Jr^-T(xi) xi and the world wrench, one world twist per
+    column and one dot product per (frame, supporting column), the raw-q map of a free flyer."""
+    nj, nv = model.njoints, model.nv
+    fk = nj * 2 * SE3_COMPOSE_FLOPS
+    frames = len(frame_ids) * (2 * SE3_COMPOSE_FLOPS + SE3_INVERSE_FLOPS + SE3_LOG_FLOPS + 13)
+    pairs = sum(sum(int(model.nvs[j]) for j in model.supports[model.frames[f].parent_joint]) for f in frame_ids)
+    bwd = len(frame_ids) * (JR_INV_T_XI_FLOPS + WRENCH_FLOPS) + nv * COLUMN_TWIST_FLOPS + pairs * PAIR_FLOPS + 60
+    if recompute:
+        bwd += fk + frames
+    return fk + frames + bwd
+
+
 def lm_launch_flops(wl, iters) -> float:
     """Flops of one solve of the packed mix: per problem, its iterations x its class's iteration
     flops for its own targets."""
@@ -598,7 +621,11 @@ def bench_adjoint(steps: int, warmup: int):
             e1.record(stream)
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / steps
-            out[f"B{B}_{mode}"] = {"ms_fwd_bwd": ms, "configs_per_s": B / (ms * 1e-3)}
+            fl = adjoint_flops_per_config(m, fids, recompute=(mode == "recompute" or
+                                                              (mode == "auto" and B * m.njoints * 28 > 126 << 20)))
+            tf = B * fl / (ms * 1e-3) / 1e12
+            out[f"B{B}_{mode}"] = {"ms_fwd_bwd": ms, "configs_per_s": B / (ms * 1e-3), "flops_per_config": fl,
+                                   "tflops": tf, "frac_fp32_peak": tf / FP32_PEAK_TFLOPS}
     return out
 
 
