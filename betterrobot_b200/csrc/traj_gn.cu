@@ -508,12 +508,23 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
   // one forward pass gives S = H_bb - H_bI P^-1 H_Ib and rb = -g_b - H_bI P^-1 (-g_I) without
   // storing P^-1 h0 and P^-1 hT; after the boundary solve, the interior step is one more
   // banded solve with right-hand side -g_I - h0 delta_0 - hT delta_{T-1}.
+  // Twisted factorization (m = T - 2 >= kTwistMin interior knots): the band of DOF i is
+  // factored from both ends at once, thread 2i taking rows 0..k-1 top-down (L D L^T) and
+  // thread 2i + 1 rows m-1..k+2 bottom-up (U E U^T), k = m / 2, which halves the dependent
+  // chain; both then reduce the 2 x 2 block of rows k, k+1 from the two sides' updates.  The
+  // multipliers of the rows into the middle block are kept in the free slots of rows k, k+1
+  // (bl1), every second-neighbour multiplier is c2 times a stored reciprocal pivot.  With
+  // z = M^-1 v the twisted forward substitution, h^T P^-1 v is the sum over the top and bottom
+  // rows of z_h z_v / pivot plus the middle block's r_h^T B^-1 r_v.
+  constexpr int kTwistMin = 8;
   auto newton_solve = [&](double damp) -> bool {
     const int m = T - 2;
+    const bool tw = m >= kTwistMin;
+    const int km = m / 2;
     bool good = true;
     double suu = 0.0, suw = 0.0, sww = 0.0, suy = 0.0, swy = 0.0;
     const double h1 = -4.0 * c2;                    // H[(p+1), (p)] inside the interior
-    if (tid < nv) {
+    if (!tw && tid < nv) {
       const int i = tid;
       double d1 = 0.0, di1 = 0.0, di2 = 0.0, l1p = 0.0;
       double y1 = 0, y2 = 0, u1 = 0, u2 = 0, w1 = 0, w2 = 0;
@@ -534,6 +545,86 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
         y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
       }
     }
+    const unsigned tmask = __ballot_sync(0xffffffffu, tid < 2 * nv);
+    if (tw && tid < 2 * nv) {
+      const int i = tid >> 1, side = tid & 1;
+      // side 0: p = 0, 1, .., km-1; side 1: p = m-1, m-2, .., km+2 (the same recurrence on
+      // the reversed band: diagonal, off-diagonals h1 and c2 are symmetric)
+      const int p0 = side ? m - 1 : 0, dir = side ? -1 : 1, steps = side ? m - km - 2 : km;
+      double d1 = 0.0, di1 = 0.0, di2 = 0.0, l1p = 0.0;
+      double y1 = 0, y2 = 0, u1 = 0, u2 = 0, w1 = 0, w2 = 0;
+      for (int q = 0; q < steps; ++q) {
+        const int p = p0 + dir * q, t = p + 1;
+        const double l2 = (q >= 2) ? c2 * di2 : 0.0;
+        const double l1 = (q >= 1) ? (h1 - c2 * l1p) * di1 : 0.0;
+        const double dp = hdiag(t, i, damp) - l1 * l1 * d1 - l2 * c2;
+        if (!(dp > 0.0)) { good = false; break; }
+        const double dip = fast_rcp(dp);
+        bl1[p * nv + i] = l1; bdi[p * nv + i] = dip;
+        const double y = -g[t * nv + i] - l1 * y1 - l2 * y2;
+        const double u = h0_at(t) - l1 * u1 - l2 * u2;
+        const double w = hT_at(t) - l1 * w1 - l2 * w2;
+        suu += u * u * dip; suw += u * w * dip; sww += w * w * dip;
+        suy += u * y * dip; swy += w * y * dip;
+        di2 = di1; di1 = dip; d1 = dp; l1p = l1;
+        y2 = y1; y1 = y; u2 = u1; u1 = u; w2 = w1; w1 = w;
+      }
+      // this side's multipliers into the middle block: the adjacent middle row (km for the top,
+      // km + 1 for the bottom) from this side's last two rows, the far middle row from its last
+      const double n1 = (h1 - c2 * l1p) * di1, n2 = c2 * di2, f1 = c2 * di1;
+      const int near = side ? km + 1 : km;
+      bl1[near * nv + i] = n1;
+      // updates of the middle block: near diagonal, off-diagonal, far diagonal; right-hand sides
+      const double a_near = n1 * n1 * d1 + n2 * c2, a_off = c2 * n1, a_far = f1 * c2;
+      const double ry_near = n1 * y1 + n2 * y2, ry_far = f1 * y1;
+      const double ru_near = n1 * u1 + n2 * u2, ru_far = f1 * u1;
+      const double rw_near = n1 * w1 + n2 * w2, rw_far = f1 * w1;
+      // the other side's updates (lanes 2i, 2i + 1 of one warp)
+      const double o_near = __shfl_xor_sync(tmask, a_near, 1), o_off = __shfl_xor_sync(tmask, a_off, 1),
+                   o_far = __shfl_xor_sync(tmask, a_far, 1);
+      const double oy_near = __shfl_xor_sync(tmask, ry_near, 1), oy_far = __shfl_xor_sync(tmask, ry_far, 1);
+      const double ou_near = __shfl_xor_sync(tmask, ru_near, 1), ou_far = __shfl_xor_sync(tmask, ru_far, 1);
+      const double ow_near = __shfl_xor_sync(tmask, rw_near, 1), ow_far = __shfl_xor_sync(tmask, rw_far, 1);
+      const double osuu = __shfl_xor_sync(tmask, suu, 1), osuw = __shfl_xor_sync(tmask, suw, 1),
+                   osww = __shfl_xor_sync(tmask, sww, 1), osuy = __shfl_xor_sync(tmask, suy, 1),
+                   oswy = __shfl_xor_sync(tmask, swy, 1);
+      good = good && __shfl_xor_sync(tmask, (int)good, 1);
+      // middle block in (top, bottom) order, the same on both lanes
+      const double tA = side ? o_near : a_near, tF = side ? o_far : a_far, tO = side ? o_off : a_off;
+      const double bA = side ? a_near : o_near, bF = side ? a_far : o_far, bO = side ? a_off : o_off;
+      const int t0 = km + 1, t1 = km + 2;
+      const double B00 = hdiag(t0, i, damp) - tA - bF;
+      const double B10 = h1 - tO - bO;
+      const double B11 = hdiag(t1, i, damp) - tF - bA;
+      auto mid = [&](double v0, double v1, double top_near, double top_far, double bot_near, double bot_far,
+                     double& r0, double& r1) {
+        r0 = v0 - top_near - bot_far;
+        r1 = v1 - top_far - bot_near;
+      };
+      double ry0, ry1, ru0, ru1, rw0, rw1;
+      mid(-g[t0 * nv + i], -g[t1 * nv + i], side ? oy_near : ry_near, side ? oy_far : ry_far,
+          side ? ry_near : oy_near, side ? ry_far : oy_far, ry0, ry1);
+      mid(h0_at(t0), h0_at(t1), side ? ou_near : ru_near, side ? ou_far : ru_far,
+          side ? ru_near : ou_near, side ? ru_far : ou_far, ru0, ru1);
+      mid(hT_at(t0), hT_at(t1), side ? ow_near : rw_near, side ? ow_far : rw_far,
+          side ? rw_near : ow_near, side ? rw_far : ow_far, rw0, rw1);
+      good = good && B00 > 0.0;
+      const double dk = good ? fast_rcp(B00) : 0.0;
+      const double lm = B10 * dk;
+      const double D1 = B11 - lm * B10;
+      good = good && D1 > 0.0;
+      const double dk1 = good ? fast_rcp(D1) : 0.0;
+      if (side == 0) { bdi[km * nv + i] = dk; bdi[(km + 1) * nv + i] = dk1; }
+      // a^T B^-1 b = a0 b0 / B00 + (a1 - l a0)(b1 - l b0) / D1
+      auto bq = [&](double a0, double a1, double b0, double b1) {
+        return a0 * b0 * dk + (a1 - lm * a0) * (b1 - lm * b0) * dk1;
+      };
+      suu += osuu + bq(ru0, ru1, ru0, ru1);
+      suw += osuw + bq(ru0, ru1, rw0, rw1);
+      sww += osww + bq(rw0, rw1, rw0, rw1);
+      suy += osuy + bq(ru0, ru1, ry0, ry1);
+      swy += oswy + bq(rw0, rw1, ry0, ry1);
+    }
     if (__syncthreads_or(!good)) return false;
     // boundary block H_bb, packed lower: b = i for (knot 0, DOF i), nv + i for (knot T-1, DOF i)
     const int nbp = nb * (nb + 1) / 2;
@@ -553,8 +644,8 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
       Sb[e] = h;
     }
     __syncthreads();
-    if (tid < nv) {
-      const int i = tid;
+    if (tw ? (tid < 2 * nv && (tid & 1) == 0) : tid < nv) {
+      const int i = tw ? tid >> 1 : tid;
       Sb[tri_at(i, i)] -= suu;
       Sb[tri_at(nv + i, i)] -= suw;
       Sb[tri_at(nv + i, nv + i)] -= sww;
@@ -612,8 +703,53 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
     }
     __syncthreads();
     // interior step of DOF i: P_i d = -g_I - h0 z(knot 0) - hT z(knot T-1); forward into delta,
-    // then backward in place
-    if (tid < nv) {
+    // then backward in place (twisted: from both ends to the middle block and back out)
+    if (tw && tid < 2 * nv) {
+      const int i = tid >> 1, side = tid & 1;
+      const double z0 = zb[i], zT = zb[nv + i];
+      if (side == 0) {
+        delta[i] = z0;
+        delta[(T - 1) * nv + i] = zT;
+      }
+      auto rhs = [&](int t) { return -g[t * nv + i] - h0_at(t) * z0 - hT_at(t) * zT; };
+      const int p0 = side ? m - 1 : 0, dir = side ? -1 : 1, steps = side ? m - km - 2 : km;
+      double y1 = 0, y2 = 0;
+      for (int q = 0; q < steps; ++q) {
+        const int p = p0 + dir * q, t = p + 1;
+        const double l1 = bl1[p * nv + i], l2 = (q >= 2) ? c2 * bdi[(p - 2 * dir) * nv + i] : 0.0;
+        const double y = rhs(t) - l1 * y1 - l2 * y2;
+        delta[t * nv + i] = y;
+        y2 = y1; y1 = y;
+      }
+      // middle block: this side's last two rows, multipliers as in the factorization
+      const int pl = p0 + dir * (steps - 1);                      // this side's last row
+      const double n1 = bl1[(side ? km + 1 : km) * nv + i];
+      const double n2 = c2 * bdi[(pl - dir) * nv + i], f1 = c2 * bdi[pl * nv + i];
+      const double r_near = n1 * y1 + n2 * y2, r_far = f1 * y1;
+      const double o_near = __shfl_xor_sync(tmask, r_near, 1), o_far = __shfl_xor_sync(tmask, r_far, 1);
+      const double on1 = __shfl_xor_sync(tmask, n1, 1);
+      const double tn = side ? o_near : r_near, tf = side ? o_far : r_far;
+      const double bn = side ? r_near : o_near, bfar = side ? r_far : o_far;
+      const double r0 = rhs(km + 1) - tn - bfar, r1 = rhs(km + 2) - tf - bn;
+      const double dk = bdi[km * nv + i], dk1 = bdi[(km + 1) * nv + i];
+      const double lm = (h1 - c2 * n1 - c2 * on1) * dk;           // B10 / B00 (symmetric in the sides)
+      const double x1 = (r1 - lm * r0) * dk1, x0 = r0 * dk - lm * x1;
+      if (side == 0) {
+        delta[(km + 1) * nv + i] = x0;
+        delta[(km + 2) * nv + i] = x1;
+      }
+      // back substitution outwards: x_p = z_p / pivot_p - (near multiplier) x_(p+dir') - c2 / pivot_p x_(p+2dir')
+      double xa = side ? x1 : x0, xb = side ? x0 : x1;            // the next two rows towards the middle
+      for (int q = steps - 1; q >= 0; --q) {
+        const int p = p0 + dir * q;
+        const double di = bdi[p * nv + i];
+        const double ln = bl1[(p + dir) * nv + i];                 // the row towards the middle, relative to p
+        const double y = delta[(p + 1) * nv + i] * di - ln * xa - c2 * di * xb;
+        delta[(p + 1) * nv + i] = y;
+        xb = xa; xa = y;
+      }
+    }
+    if (!tw && tid < nv) {
       const int i = tid;
       const double z0 = zb[i], zT = zb[nv + i];
       delta[i] = z0;
