@@ -283,8 +283,10 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
   };
   // both pose terms at xs, warp 0 the goal (knot T-1), warp 1 the start (knot 0): xi (into
   // rg / rs); with want_J also J = Jr^-1 blockdiag(R^T,R^T) J_lwa (6 x nv, into Jg / Js).
-  // A term that is not in the problem (weight 0 or no start pose) is skipped.
-  auto pose_terms = [&](const double* xs, bool want_J) __attribute__((always_inline)) {
+  // A term that is not in the problem (weight 0 or no start pose) is skipped.  With `reuse`
+  // the knot's FK and xi are those the last call left (the build follows the cost evaluation
+  // of the same point, and nothing in between writes the pose buffers).
+  auto pose_terms = [&](const double* xs, bool want_J, bool reuse) __attribute__((always_inline)) {
     if (warp < 2) {
       const int h = warp;
       const bool active = h == 0 ? has_goal : has_start;
@@ -293,12 +295,17 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
         const DPose target{d3(tp[0], tp[1], tp[2]), make_double4(tp[3], tp[4], tp[5], tp[6])};
         double* r = h == 0 ? rg : rs;
         double* J = h == 0 ? Jg : Js;
-        double* pose = fk(xs, h == 0 ? T - 1 : 0, h);
+        double* pose = reuse ? ((tree.rounds & 1) ? pB : pA) + 8 * nj * h : fk(xs, h == 0 ? T - 1 : 0, h);
         const DPose Tee = dcompose(ldd8(pose + 8 * fpar), DPose{d3(fpl.t.x, fpl.t.y, fpl.t.z),
                                                                 make_double4(fpl.q.x, fpl.q.y, fpl.q.z, fpl.q.w)});
         double3 v, w;
-        dse3_log(dcompose(dinverse(target), Tee), v, w);
-        if (lane == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
+        if (reuse) {
+          v = d3(r[0], r[1], r[2]);
+          w = d3(r[3], r[4], r[5]);
+        } else {
+          dse3_log(dcompose(dinverse(target), Tee), v, w);
+          if (lane == 0) { r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = w.x; r[4] = w.y; r[5] = w.z; }
+        }
         if (want_J) {
           const DJrInv Jr = djr_inv_se3<9>(v, w);
           const double4 qc = dqconj(Tee.q);
@@ -403,7 +410,7 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
   // total cost 0.5 |r|^2 at xs (pose terms evaluated into rg / rs)
   auto cost_of = [&](const double* xs) -> double {
     double acc = 0.0;
-    pose_terms(xs, false);
+    pose_terms(xs, false, false);
     if (kManifold) knot_differences(xs);
     for (int e = tid; e < (T - 2) * nv; e += NT) {              // smoothness.py:118-125
       const double a = kManifold ? c * (dd[e + nv] - dd[e]) : c * (xs[e + 2 * nv] - 2.0 * xs[e + nv] + xs[e]);
@@ -434,7 +441,7 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
   };
   // J^T J of the pose terms (packed lower) and g = J^T r at x; returns |g|
   auto build = [&]() -> double {
-    pose_terms(x, true);
+    pose_terms(x, true, true);                        // FK and xi of x from the cost evaluation of x
     const int npk = nv * (nv + 1) / 2;
     for (int e = tid; e < npk; e += NT) {
       const int2 ab = tri_decode(e);
@@ -820,7 +827,7 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
   float* xo = P.x + traj * (int64_t)nqT;
   for (int e = tid; e < nqT; e += NT) xo[e] = (float)x[e];
   if (P.goal_grad && has_goal) {
-    pose_terms(x, false);
+    pose_terms(x, false, false);
     if (tid == 0) {
       const double3 v = d3(rg[0], rg[1], rg[2]);
       const double3 w = d3(rg[3], rg[4], rg[5]);
