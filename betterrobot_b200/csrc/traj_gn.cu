@@ -330,7 +330,8 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
         }
       }
     }
-    __syncthreads();
+    // the build reads J next; a cost evaluation reads xi only after its block sum's barriers
+    if (want_J) __syncthreads();
   };
   // dd[t] = difference(xs_t, xs_{t+1}) (t < T-1) and dr[t] = difference(xref_t, xs_t)
   // (model.py:176-190): free-flyer log(q_a^-1 q_b) (free_flyer.py:53-57), spherical
@@ -828,6 +829,7 @@ __global__ void __launch_bounds__(kTrajThreads) traj_gn_kernel(const TrajParams 
   for (int e = tid; e < nqT; e += NT) xo[e] = (float)x[e];
   if (P.goal_grad && has_goal) {
     pose_terms(x, false, false);
+    __syncthreads();
     if (tid == 0) {
       const double3 v = d3(rg[0], rg[1], rg[2]);
       const double3 w = d3(rg[3], rg[4], rg[5]);
