@@ -99,6 +99,8 @@ _lock = threading.Lock()
 def load(path: str = LIB_PATH):
     """Load the shared library (no device is touched)."""
     global _lib
+    if _lib is not None:  # loaded: no lock on the per-call path
+        return _lib
     with _lock:
         if _lib is None:
             if not os.path.exists(path):
@@ -121,10 +123,16 @@ def call(name: str, *args) -> None:
         raise KernelError(f"{name} returned {st} ({msg})", st)
 
 
+_cuda_seen = False
+
+
 def require_cuda(t) -> None:
-    import torch
-    if not torch.cuda.is_available():
-        raise BackendNotAvailableError("the sm_100a path needs a CUDA device; none is available")
+    global _cuda_seen
+    if not _cuda_seen:  # a device, once found, stays for the process
+        import torch
+        if not torch.cuda.is_available():
+            raise BackendNotAvailableError("the sm_100a path needs a CUDA device; none is available")
+        _cuda_seen = True
     if not t.is_cuda:
         from .exceptions import DeviceMismatchError
         raise DeviceMismatchError(f"expected a CUDA tensor, got device={t.device}")

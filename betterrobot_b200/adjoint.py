@@ -29,20 +29,41 @@ def choose_mode(model, batch: int, device) -> str:
     return "store" if batch * model.njoints * 28 <= l2 else "recompute"
 
 
+_IDS: dict = {}
+
+
+def _ids(frame_ids: tuple):
+    """The frame ids as a ctypes array, built once per id tuple."""
+    arr = _IDS.get(frame_ids)
+    if arr is None:
+        if len(_IDS) >= 256:
+            _IDS.clear()
+        arr = _IDS[frame_ids] = (_lib.c_int32 * len(frame_ids))(*frame_ids)
+    return arr
+
+
+def _on_device(device, fn) -> None:
+    """Run ``fn(stream)`` with ``device`` current (no context switch when it already is)."""
+    if device.index == torch.cuda.current_device():
+        fn(torch.cuda.current_stream().cuda_stream)
+    else:
+        with torch.cuda.device(device):
+            fn(torch.cuda.current_stream().cuda_stream)
+
+
 class _PoseLoss(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q, targets, weights, model, frame_ids, mode):
         B = q.shape[0]
         dt = device_tree(model, q.device)
-        ids = (_lib.c_int32 * len(frame_ids))(*frame_ids)
+        ids = _ids(frame_ids)
         loss = torch.empty(B, device=q.device, dtype=torch.float32)
         oMi = torch.empty(B, model.njoints, 7, device=q.device) if mode == "store" else None
         per_cfg = int(weights.dim() == 2)
-        with torch.cuda.device(q.device):
-            _lib.call("br_pose_loss", dt.ptr, q.data_ptr(), B, ids, len(frame_ids), targets.data_ptr(),
-                      weights.data_ptr(), per_cfg, loss.data_ptr(), oMi.data_ptr() if oMi is not None else None,
-                      _lib.stream_ptr())
-        ctx.model, ctx.frame_ids, ctx.per_cfg = model, list(frame_ids), per_cfg
+        _on_device(q.device, lambda s: _lib.call(
+            "br_pose_loss", dt.ptr, q.data_ptr(), B, ids, len(frame_ids), targets.data_ptr(), weights.data_ptr(),
+            per_cfg, loss.data_ptr(), oMi.data_ptr() if oMi is not None else None, s))
+        ctx.model, ctx.frame_ids, ctx.per_cfg = model, frame_ids, per_cfg
         if oMi is not None:
             ctx.save_for_backward(q, targets, weights, oMi)
         else:
@@ -57,11 +78,11 @@ class _PoseLoss(torch.autograd.Function):
         g = grad_loss.contiguous().float()
         grad_q = torch.empty_like(q)
         dt = device_tree(ctx.model, q.device)
-        ids = (_lib.c_int32 * len(ctx.frame_ids))(*ctx.frame_ids)
-        with torch.cuda.device(q.device):
-            _lib.call("br_pose_loss_backward", dt.ptr, q.data_ptr(), oMi.data_ptr() if oMi is not None else None,
-                      q.shape[0], ids, len(ctx.frame_ids), targets.data_ptr(), weights.data_ptr(), ctx.per_cfg,
-                      g.data_ptr(), grad_q.data_ptr(), _lib.stream_ptr())
+        ids = _ids(ctx.frame_ids)
+        _on_device(q.device, lambda s: _lib.call(
+            "br_pose_loss_backward", dt.ptr, q.data_ptr(), oMi.data_ptr() if oMi is not None else None,
+            q.shape[0], ids, len(ctx.frame_ids), targets.data_ptr(), weights.data_ptr(), ctx.per_cfg,
+            g.data_ptr(), grad_q.data_ptr(), s))
         return grad_q, None, None, None, None, None
 
 
@@ -76,7 +97,7 @@ def pose_loss(model, q: torch.Tensor, frame_ids: Sequence[int], targets: torch.T
     _validate_q(model, q, check_quaternion)
     if q.dim() != 2:
         raise ShapeError("pose_loss takes q of shape (B, nq)")
-    frame_ids = [int(f) for f in frame_ids]
+    frame_ids = tuple(int(f) for f in frame_ids)
     B, F = q.shape[0], len(frame_ids)
     if targets.shape != (B, F, 7):
         raise ShapeError(f"targets must be ({B}, {F}, 7), got {tuple(targets.shape)}")
