@@ -183,6 +183,14 @@ def test_size_limits_vs_oracle(spec, N, T):
     _vs_oracle(spec, N, T, 53)
 
 
+@pytest.mark.parametrize("T", [3, 9, 10, 11])
+def test_band_factorization_paths_vs_oracle(T):
+    """Around the switch to the twisted band factorization (>= 8 interior knots: T >= 10): the
+    one-ended path at T = 3 and 9, the smallest twisted cases at T = 10 (2 bottom rows) and
+    T = 11 (an odd band), against the float64 oracle."""
+    _vs_oracle(syn.chain_spec(), 12, T, 59)
+
+
 def test_trajopt_rejects_oversized_trees_and_bad_shapes():
     m = syn.model_from_spec(syn.humanoid_spec())     # 128 knots of 36 DOFs: above shared memory
     X0 = torch.zeros(2, 128, m.nq, device="cuda")
