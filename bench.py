@@ -57,6 +57,9 @@ FKJ_BYTES_PER_CONFIG = 4 * (37 + 12 * 7 + 12 * 6 * 36)  # q read + oMf + J writt
 # of ``bench.py --only fkj`` (dram__bytes_read.sum 9.77 MB + dram__bytes_write.sum 642.18 MB); the
 # rest of the 711 MB of output is still in L2 when the launch ends.
 FKJ_TRAFFIC_BYTES = 9.766e6 + 642.179e6
+# DRAM bytes of one lm_solve_kernel launch on the 8,192-problem mix (ncu dram__bytes_read.sum 3.06 MB,
+# dram__bytes_write.sum 0: the results stay in L2 until the next reader): neither HBM nor L2 bound
+LM_TRAFFIC_BYTES = 3.063e6
 JOINT_OPS_BATCH = 1 << 20
 REACH_TOL = 1e-4
 CANDIDATES = {
@@ -925,7 +928,7 @@ def main():
                         "achieved": ik["flops"] / (ik["ms"] * 1e-3) / 1e12, "peak": FP32_PEAK_TFLOPS,
                         "unit": "TFLOP/s", "frac": ik["flops"] / (ik["ms"] * 1e-3) / 1e12 / FP32_PEAK_TFLOPS,
                         "peak_kind": "nominal FP32 CUDA-core peak (148 SMs x 128 x 2 x 1.965 GHz)",
-                        "flops_per_launch": ik["flops"],
+                        "flops_per_launch": ik["flops"], "traffic": LM_TRAFFIC_BYTES,
                         "flops_basis": "reference's dense LM iteration per problem x its iterations"},
         "ik": {"problems": ik["problems"] * world, "reached_1e-4": reached, "converged": ik["converged"],
                "iters_mean": ik["iters_mean"], "kernel": "lm_solve_kernel", "launches_per_step": 1,
