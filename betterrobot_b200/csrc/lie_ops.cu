@@ -4,11 +4,12 @@
 // tangents [v, w], linear first) and the SE3 right Jacobians of
 // src/better_robot/lie/tangents.py:184-207.
 //
-// One thread per element, grid-stride, one kernel instantiation per op.  The same
-// device functions run inside the fused FK / Jacobian / LM / adjoint kernels, so this
-// entry point also exposes them to parity tests one operation at a time.  Every op is
-// memory bound (<= 2 kFLOP per element for the 6x6 outputs); records are 3..36 floats,
-// read and written with scalar loads by consecutive threads.
+// One lane per element, one warp per tile of 32 consecutive elements (grid-stride over
+// tiles), one kernel instantiation per op.  The same device functions run inside the
+// fused FK / Jacobian / LM / adjoint kernels, so this entry point also exposes them to
+// parity tests one operation at a time.  Records are 3..36 floats; a tile's records are
+// contiguous slabs, staged through shared memory by cp.async on the way in and written
+// back with coalesced 16-byte stores (lie_ops_kernel below).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
