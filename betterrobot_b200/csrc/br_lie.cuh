@@ -93,11 +93,12 @@ __device__ __forceinline__ float3 so3_log(float4 q) {
 // (se3_log, _torch_native_backend.py:298-303) and of the SO3 Jr^-1
 // (tangents.right_jacobian_inv_so3:122-145).  Series 1/12 + t2/720 + t2^2/30240
 // + t2^3/1209600 + t2^4/47900160 below theta = 1 (float32 cancels there).
+__device__ __forceinline__ float vinv_series(float th2) {
+  return fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 47900160.f, 1.f / 1209600.f), 1.f / 30240.f), 1.f / 720.f),
+              1.f / 12.f);
+}
 __device__ __forceinline__ float vinv_coeff(float th2) {
-  if (th2 < 1.f) {
-    return fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 47900160.f, 1.f / 1209600.f), 1.f / 30240.f),
-                          1.f / 720.f), 1.f / 12.f);
-  }
+  if (th2 < 1.f) return vinv_series(th2);
   const float th = sqrtf(th2);
   float sh, ch;
   sincospif(th * (0.5f / 3.14159265358979f), &sh, &ch);  // sin, cos of th / 2 (th <= pi for a log)
@@ -148,50 +149,31 @@ __device__ __forceinline__ void jr_inv_T_xi(float3 v, float3 w, float3& gl, floa
 
 // SE3 log -> (v, w)   (se3_log, _torch_native_backend.py:289-310).  The rotation part as
 // so3_log; the V^-1 coefficient c = 1/th^2 - cot(th/2) / (2 th) takes cot(th/2) = |q_w| / s
-// from the quaternion itself (th / 2 = atan2(s, |q_w|)), so no trigonometric call is needed
-// beyond the atan2 (the series of vinv_coeff below th = 1, where the closed form cancels).
+// from the quaternion itself (th / 2 = a = atan2(s, |q_w|)), so no trigonometric call is
+// needed beyond the atan2 (the series of vinv_coeff below th = 1, where the closed form
+// cancels).  One reciprocal r = 1/(s a) gives both th / s = 2 a^2 r and
+// c = 1/(4 a^2) - |q_w| / (4 s a) = r (s^2 r - |q_w|) / 4.
 __device__ __forceinline__ void se3_log(const Pose& T, float3& v, float3& w) {
   float4 q = T.q;
   if (q.w < 0.f) q = make_float4(-q.x, -q.y, -q.z, -q.w);
   const float s2 = q.x * q.x + q.y * q.y + q.z * q.z;
-  const float s = sqrtf(s2);
   const float qw = fminf(fmaxf(q.w, -1.f), 1.f);
-  float factor;
+  float factor, c;
   if (s2 < 0.25e-8f) {
     factor = 2.f + s2 * (2.f / 3.f);
+    c = vinv_series(factor * factor * s2);
   } else {
-    factor = 2.f * atan2f(s, qw) / s;
+    const float s = sqrtf(s2);
+    const float a = atan2f(s, qw);
+    const float r = 1.f / (s * a);
+    factor = 2.f * (a * a) * r;
+    const float th2 = 4.f * (a * a);
+    c = th2 < 1.f ? vinv_series(th2) : 0.25f * r * fmaf(s2, r, -qw);
   }
   w = f3(factor * q.x, factor * q.y, factor * q.z);
-  const float th2 = dot(w, w);
-  float c;
-  if (th2 < 1.f) {
-    c = vinv_coeff(th2);
-  } else {
-    const float th = sqrtf(th2);
-    c = 1.f / th2 - qw / (2.f * s * th);
-  }
   // V^-1 t = t - 1/2 w x t + c w x (w x t)
   const float3 wt = cross(w, T.t);
   v = axpy(c, cross(w, wt), axpy(-0.5f, wt, T.t));
-}
-
-// b = (1 - cos th)/th^2 and c = (th - sin th)/th^3 of se3_exp (_torch_native_backend.py:272-278)
-__device__ __forceinline__ void exp_coeffs(float th2, float& b, float& c) {
-  if (th2 < 1.f) {
-    // b = 1/2 - t2/24 + t2^2/720 - t2^3/40320 + t2^4/3628800
-    b = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 3628800.f, -1.f / 40320.f), 1.f / 720.f), -1.f / 24.f), 0.5f);
-    // c = 1/6 - t2/120 + t2^2/5040 - t2^3/362880 + t2^4/39916800
-    c = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 39916800.f, -1.f / 362880.f), 1.f / 5040.f), -1.f / 120.f),
-             1.f / 6.f);
-  } else {
-    const float th = sqrtf(th2);
-    float s, co, sh, ch;
-    sincosf(th, &s, &co);
-    sincosf(0.5f * th, &sh, &ch);
-    b = 2.f * sh * sh / th2;  // 1 - cos th = 2 sin^2(th/2)
-    c = (th - s) / (th * th2);
-  }
 }
 
 // so3_exp (_torch_native_backend.py:144-159)
@@ -242,29 +224,24 @@ __device__ __forceinline__ Pose se3_exp_step(float3 v, float3 w) {
   return T;
 }
 
-// se3_exp (_torch_native_backend.py:258-286): T = (V(w) v, exp(w)).  Below th = 1 the series
-// of exp_coeffs and of sin(th/2)/th, cos(th/2); beyond, one sincos of th/2 gives them all
-// (sin th = 2 sin(th/2) cos(th/2), 1 - cos th = 2 sin^2(th/2)).
+// se3_exp (_torch_native_backend.py:258-286): T = (V(w) v, exp(w)).  One sincos of th/2 gives
+// every coefficient (sin th = 2 sin(th/2) cos(th/2), 1 - cos th = 2 sin^2(th/2)); only
+// c = (th - sin th)/th^3 cancels in float32 at small angles, so below th = 1 it comes from its
+// series instead.  Selects, not branches: a warp of mixed angles runs one path.  At th = 0
+// (below 1e-8 rad) the limits b = 1/2, sin(th/2)/th = 1/2, cos(th/2) = 1 are taken.
 __device__ __forceinline__ Pose se3_exp(float3 v, float3 w) {
   const float th2 = dot(w, w);
-  float b, c, k, cw;
-  if (th2 < 1.f) {
-    exp_coeffs(th2, b, c);
-    const float x2 = 0.25f * th2;  // (th / 2)^2
-    // sin(x)/x = 1 - x^2/6 + x^4/120 - x^6/5040 + x^8/362880; k = sin(th/2)/th = (sin(x)/x) / 2
-    k = 0.5f * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 1.f / 362880.f, -1.f / 5040.f), 1.f / 120.f), -1.f / 6.f), 1.f);
-    // cos(x) = 1 - x^2/2 + x^4/24 - x^6/720 + x^8/40320 - x^10/3628800
-    cw = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -1.f / 3628800.f, 1.f / 40320.f), -1.f / 720.f), 1.f / 24.f),
-                   -0.5f), 1.f);
-  } else {
-    const float th = sqrtf(th2);
-    float sh;
-    sincospif(th * (0.5f / 3.14159265358979f), &sh, &cw);
-    const float it = 1.f / th;
-    b = 2.f * sh * sh * (it * it);
-    c = (th - 2.f * sh * cw) * (it * it * it);
-    k = sh * it;
-  }
+  const bool tiny = th2 < 1e-16f;
+  const float th = sqrtf(tiny ? 1.f : th2);
+  float sh, ch;
+  sincospif(th * (0.5f / 3.14159265358979f), &sh, &ch);
+  const float it = 1.f / th;
+  const float b = tiny ? 0.5f : 2.f * sh * sh * (it * it);
+  const float k = tiny ? 0.5f : sh * it;
+  const float cw = tiny ? 1.f : ch;
+  const float c = th2 < 1.f ? fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 39916800.f, -1.f / 362880.f),
+                                                        1.f / 5040.f), -1.f / 120.f), 1.f / 6.f)
+                            : (th - 2.f * sh * ch) * (it * it * it);
   const float3 wv = cross(w, v);
   Pose T;
   T.t = axpy(c, cross(w, wv), axpy(b, wv, v));
