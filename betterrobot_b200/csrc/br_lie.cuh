@@ -114,10 +114,13 @@ __device__ __forceinline__ float vinv_coeff(float th2) {
 //             + c4 (w^v^w^w^ + w^w^v^w^) u,
 // c2 = (th - sin th)/th^3, c3 = (th^2 + 2 cos th - 2)/(2 th^4), c4 = (2 th - 3 sin th + th cos th)/(2 th^5)
 // (Taylor series of each for th^2 < 2, where the closed forms cancel).  Equal to applying the
-// exact (infinite-series) Jr^-1 of jr_inv_se3 below, at a fraction of its arithmetic.
+// exact (infinite-series) Jr^-1 of jr_inv_se3 below, at a fraction of its arithmetic.  Beyond
+// th = 1 one sincos of th/2 and one reciprocal r = 1/(th sin(th/2)) give every coefficient:
+// sin th = 2 sin(th/2) cos(th/2), cos th = 1 - 2 sin^2(th/2), 1/th = sin(th/2) r,
+// cot(th/2) = th cos(th/2) r.
 __device__ __forceinline__ void jr_inv_T_xi(float3 v, float3 w, float3& gl, float3& ga) {
   const float th2 = dot(w, w);
-  float c2, c3, c4;
+  float c, c2, c3, c4;
   if (th2 < 2.f) {
     c2 = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 39916800.f, -1.f / 362880.f), 1.f / 5040.f), -1.f / 120.f),
               1.f / 6.f);
@@ -125,15 +128,24 @@ __device__ __forceinline__ void jr_inv_T_xi(float3 v, float3 w, float3& gl, floa
                    -1.f / 720.f), 1.f / 24.f);
     c4 = fmaf(th2, fmaf(th2, fmaf(th2, fmaf(th2, 1.f / 1245404160.f, -1.f / 9979200.f), 1.f / 120960.f),
                    -1.f / 2520.f), 1.f / 120.f);
+  }
+  if (th2 < 1.f) {
+    c = vinv_series(th2);
   } else {
     const float th = sqrtf(th2);
-    float s, co;
-    sincospif(th * (1.f / 3.14159265358979f), &s, &co);
-    c2 = (th - s) / (th * th2);
-    c3 = (th2 + 2.f * co - 2.f) / (2.f * th2 * th2);
-    c4 = (2.f * th - 3.f * s + th * co) / (2.f * th2 * th2 * th);
+    float sh, ch;
+    sincospif(th * (0.5f / 3.14159265358979f), &sh, &ch);
+    const float r = 1.f / (th * sh);
+    const float it = sh * r;                       // 1 / th
+    c = it * fmaf(-0.5f * ch, th * r, it);         // 1/th^2 - cot(th/2) / (2 th)
+    if (th2 >= 2.f) {
+      const float s = 2.f * sh * ch, co = fmaf(-2.f * sh, sh, 1.f);
+      const float it2 = it * it;
+      c2 = (th - s) * (it2 * it);
+      c3 = 0.5f * (th2 + 2.f * co - 2.f) * (it2 * it2);
+      c4 = 0.5f * (2.f * th - 3.f * s + th * co) * (it2 * it2 * it);
+    }
   }
-  const float c = vinv_coeff(th2);
   auto vinv = [&](float3 x) { return axpy(c, cross(w, cross(w, x)), axpy(-0.5f, cross(w, x), x)); };
   gl = vinv(v);
   const float3 a1 = cross(w, gl), a2 = cross(w, a1);
