@@ -9,9 +9,10 @@
 //     SE3 Jr^-1 (closed form jr_inv_T_xi; autograd differentiates se3_log exactly);
 //   * F_f = Ad(oMf^-1)^T g_f = [R g_lin; p x (R g_lin) + R g_ang] is the same
 //     sensitivity as a wrench at the world origin;
-//   * dL/dv_c = sum_{f : c supports f} <S_c, F_f> with S_c the world twist of tangent
-//     column c ([o x a; a] rotation, [a; 0] translation) — a reverse accumulation over
-//     the tree without any per-joint tape;
+//   * dL/dv_c = sum_{f : c supports f} <S_c, F_f> = <S_c, W_j> with S_c the world twist
+//     of tangent column c ([o x a; a] rotation, [a; 0] translation) and W_j the summed
+//     wrench of the frames that c's joint j moves — a reverse accumulation over the tree
+//     without any per-joint tape;
 //   * revolute / prismatic / translation: dL/dq = dL/dv; free-flyer and spherical: the
 //     body twist of the joint maps to raw q = [t, quat] through R (translation) and the
 //     normalisation of the quaternion ((I - u u^T)/|quat| and du -> 2 vec(u* (x) du));
@@ -44,16 +45,16 @@ struct LossParams {
 };
 
 struct LossLayout {
-  int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, fparent, fplace, fmask;
+  int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, fparent, fplace, fsup;
   int cta_floats;
-  int in0, in1, poseT, poseQ, anc, F, gv, stage;
+  int in0, in1, poseT, poseQ, anc, F, W, gv, stage;
   int warp_floats;
   __host__ __device__ LossLayout(int nj, int nq, int nv, int nf) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += round4(n); return r; };
     parent = take(nj); jtype = take(nj); idxq = take(nj); axis = take(4 * nj); place = take(8 * nj);
     cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
-    fparent = take(nf); fplace = take(8 * nf); fmask = take(2 * nf);
+    fparent = take(nf); fplace = take(8 * nf); fsup = take(2 * nf);
     cta_floats = o;
     o = 0;
     // the inputs of one configuration (q, stored oMi, targets), double buffered: the next
@@ -61,6 +62,7 @@ struct LossLayout {
     in0 = take(nq + 7 * nj + 7 * nf); in1 = take(nq + 7 * nj + 7 * nf);
     poseT = take(4 * nj); poseQ = take(4 * nj); anc = take(nj);
     F = take(8 * nf);     // world wrench per frame (f.xyz, pad, tau.xyz, pad)
+    W = take(8 * nj);     // summed wrench of the frames each joint moves (same layout)
     gv = take(nv);        // dL/dv
     stage = take(nj * 7); // oMi staging (store mode)
     warp_floats = o;
@@ -82,7 +84,7 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
   float* s_caxis = smem + L.caxis;
   int* s_fparent = reinterpret_cast<int*>(smem + L.fparent);
   float* s_fplace = smem + L.fplace;
-  unsigned long long* s_fmask = reinterpret_cast<unsigned long long*>(smem + L.fmask);
+  unsigned long long* s_fsup = reinterpret_cast<unsigned long long*>(smem + L.fsup);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpc = blockDim.x >> 5;
   for (int i = threadIdx.x; i < nj; i += blockDim.x) {
     s_parent[i] = tree.parent[i];
@@ -102,17 +104,8 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
     for (int k = 0; k < 8; ++k) s_fplace[8 * f + k] = tree.frame_placement[8 * id + k];
   }
   __syncthreads();
-  // column mask of each frame: bit c set iff tangent column c moves the frame
-  for (int f = warp; f < nf; f += wpc) {
-    const unsigned long long sup = tree.support[s_fparent[f]];
-    unsigned long long m = 0ull;
-    for (int c0 = 0; c0 < nv; c0 += kWarp) {
-      const int c = c0 + lane;
-      const bool in = c < nv && ((sup >> s_cjoint[c]) & 1ull);
-      m |= (unsigned long long)__ballot_sync(0xffffffffu, in) << c0;
-    }
-    if (lane == 0) s_fmask[f] = m;
-  }
+  // joints that move each frame: bit j set iff joint j supports the frame's parent joint
+  for (int f = threadIdx.x; f < nf; f += blockDim.x) s_fsup[f] = tree.support[s_fparent[f]];
   __syncthreads();
 
   float* w = smem + L.cta_floats + warp * L.warp_floats;
@@ -120,6 +113,7 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
   float* wpQ = w + L.poseQ;
   int* wanc = reinterpret_cast<int*>(w + L.anc);
   float* wF = w + L.F;
+  float* wW = w + L.W;
   float* wg = w + L.gv;
   float* wst = w + L.stage;
   const int64_t stride = (int64_t)gridDim.x * wpc;
@@ -225,21 +219,32 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
       continue;
     }
     __syncwarp();
+    // dL/dv_c = sum over the frames f that column c moves of <S_c, F_f> = <S_c, W_j>, where
+    // W_j sums F_f over the frames that c's joint j moves: one sum per joint, one dot per column
+    for (int j = lane; j < nj; j += kWarp) {
+      float4 sf = make_float4(0.f, 0.f, 0.f, 0.f), st = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int f = 0; f < nf; ++f) {
+        if ((s_fsup[f] >> j) & 1ull) {
+          const float4 fw = *reinterpret_cast<const float4*>(wF + 8 * f);
+          const float4 tq = *reinterpret_cast<const float4*>(wF + 8 * f + 4);
+          sf.x += fw.x; sf.y += fw.y; sf.z += fw.z;
+          st.x += tq.x; st.y += tq.y; st.z += tq.z;
+        }
+      }
+      *reinterpret_cast<float4*>(wW + 8 * j) = sf;
+      *reinterpret_cast<float4*>(wW + 8 * j + 4) = st;
+    }
+    __syncwarp();
     const float go = __ldg(p.grad_loss + b);
     for (int c = lane; c < nv; c += kWarp) {
-      const Pose Tj = load_split(wpT, wpQ, s_cjoint[c]);
+      const int j = s_cjoint[c];
+      const Pose Tj = load_split(wpT, wpQ, j);
       const float3 a = qrot(Tj.q, f3(s_caxis[4 * c], s_caxis[4 * c + 1], s_caxis[4 * c + 2]));
       const float3 m = s_ckind[c] == 0 ? cross(Tj.t, a) : a;  // linear part of the world twist
       const float3 an = s_ckind[c] == 0 ? a : f3(0.f, 0.f, 0.f);
-      float gsum = 0.f;
-      for (int f = 0; f < nf; ++f) {
-        if ((s_fmask[f] >> c) & 1ull) {
-          const float4 fw = *reinterpret_cast<const float4*>(wF + 8 * f);
-          const float4 tq = *reinterpret_cast<const float4*>(wF + 8 * f + 4);
-          gsum += dot(m, f3(fw.x, fw.y, fw.z)) + dot(an, f3(tq.x, tq.y, tq.z));
-        }
-      }
-      wg[c] = gsum * go;
+      const float4 fw = *reinterpret_cast<const float4*>(wW + 8 * j);
+      const float4 tq = *reinterpret_cast<const float4*>(wW + 8 * j + 4);
+      wg[c] = (dot(m, f3(fw.x, fw.y, fw.z)) + dot(an, f3(tq.x, tq.y, tq.z))) * go;
     }
     __syncwarp();
     float* gq = p.grad_q + b * nq;
