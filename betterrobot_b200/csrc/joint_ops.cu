@@ -40,12 +40,13 @@ struct JointOpParams {
 constexpr int kJointOpsWarps = 4;
 
 // Floats of shared memory one warp stages.  integrate: two input tiles (the next one is
-// copied while this one is computed).  difference: one input tile and the free-flyer
-// outputs of that tile (its float64 logs make it compute heavy: measured at 1 M humanoid
-// configurations, a second tile halves the warps per SM and cost 104 -> 162 us).
+// copied while this one is computed).  difference: one input tile, whose q0 rows also take
+// the outputs of the joints computed per lane (a joint's nv outputs overwrite the first nv
+// of its own nq >= nv slots); a second tile would halve its warps per SM (its float64 logs
+// make it compute heavy: measured at 1 M humanoid configurations, 104 -> 162 us).
 __host__ __device__ inline int joint_ops_in_floats(int nq, int nv, bool diff) { return 32 * (diff ? 2 * nq : nq + nv); }
 __host__ __device__ inline int joint_ops_warp_floats(int nq, int nv, bool diff) {
-  return diff ? joint_ops_in_floats(nq, nv, diff) + 32 * nv : 2 * joint_ops_in_floats(nq, nv, diff);
+  return diff ? joint_ops_in_floats(nq, nv, diff) : 2 * joint_ops_in_floats(nq, nv, diff);
 }
 
 __device__ __forceinline__ DPose dpose7(const float* p) {
@@ -69,7 +70,8 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
                                                                         const JointOpParams p) {
   extern __shared__ __align__(16) float slabs[];
   __shared__ int16_t vmap[BR_MAX_NQ];     // q slot -> v slot of a 1:1 joint, -1 for other slots
-  __shared__ int16_t qmap[BR_MAX_NV];     // v slot -> q slot of a 1:1 joint, -1 for other slots
+  __shared__ int16_t qmap[BR_MAX_NV];     // v slot -> q slot k of a 1:1 joint (k), or of the q0 slot that
+                                          // holds a per-lane joint's output (-k - 1)
   __shared__ int16_t ffq[BR_MAX_JOINTS];  // q / v offsets and kind of the joints handled per lane
   __shared__ int16_t ffv[BR_MAX_JOINTS];   // (free-flyer, spherical, planar, unbounded revolute)
   __shared__ int8_t ffk[BR_MAX_JOINTS];
@@ -89,6 +91,7 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
         qmap[iv + k] = (int16_t)(iq + k);
       }
     } else {
+      for (int k = 0; k < joint_nv(jt); ++k) qmap[iv + k] = (int16_t)(-(iq + k) - 1);
       const int s = atomicAdd(&nff, 1);
       ffq[s] = (int16_t)iq;
       ffv[s] = (int16_t)iv;
@@ -103,7 +106,6 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
   const int lo = diff ? nv : nq;  // floats per configuration of out
   const int IN = joint_ops_in_floats(nq, nv, diff);
   float* base = slabs + (size_t)(threadIdx.x >> 5) * joint_ops_warp_floats(nq, nv, diff);
-  float* O = base + IN;           // difference: free-flyer outputs, v-shaped
   const bool dbl = kVec && !diff; // integrate with 16-byte copies: next tile in flight
   const int64_t tiles = (p.batch + 31) >> 5;
   const int64_t step = (int64_t)gridDim.x * warps;
@@ -158,8 +160,9 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
             qa[k + 1] = (float)s;
           }
         } else {
+          // outputs in place of the joint's own q0 slots (each read before it is written)
           const float* qb = Bs + lane * nq + iq;
-          float* o = O + lane * nv + iv;
+          float* o = qa;
           if (jt == BR_JOINT_FREE_FLYER) {
             double3 v, w;
             dse3_log(dcompose(dinverse(dpose7(qa)), dpose7(qb)), v, w);
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
       }
     }
     __syncwarp();
-    // out[e] for the tile's slab: 1:1 slots from the staged inputs, free-flyer slots from above
+    // out[e] for the tile's slab: 1:1 slots from the staged inputs, the other slots from above
     float* go = p.out + b0 * lo;
     const int n = cnt * lo;
     auto val = [&](int c, int k) -> float {
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
         return kv >= 0 ? x + Bs[c * nv + kv] : x;
       }
       const int kq = qmap[k];
-      return kq >= 0 ? Bs[c * nq + kq] - A[c * nq + kq] : O[c * nv + k];
+      return kq >= 0 ? Bs[c * nq + kq] - A[c * nq + kq] : A[c * nq - kq - 1];
     };
     int done = 0;
     if (kVec) {
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(32 * kJointOpsWarps) joint_ops_kernel(const br
       const int c = e / lo;
       go[e] = val(c, e - c * lo);
     }
-    __syncwarp();  // this tile's buffer and O are free for the tiles after the next
+    __syncwarp();  // this tile's buffer is free for the tiles after the next
   }
   if (kVec) cp_async_wait_all();
 }
