@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(kLieWarps * kWarp) lie_ops_kernel(const float*
   __shared__ __align__(16) float smem[kLieWarps * TILE];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float* sbuf = smem + w * TILE;
-  float* so = sbuf + 2 * IN;
+  float* so = sbuf + NB * IN;                  // the output tile follows the NB input buffers
+  static_assert(NB * IN + kWarp * O == TILE, "a warp's input buffers and output tile fill its slice");
   const bool va = ((reinterpret_cast<uintptr_t>(a) & 15u) == 0), vb = ((reinterpret_cast<uintptr_t>(b) & 15u) == 0),
              vo = ((reinterpret_cast<uintptr_t>(out) & 15u) == 0);
   const int64_t ntiles = (n + kWarp - 1) / kWarp;

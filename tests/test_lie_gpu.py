@@ -131,6 +131,24 @@ def test_large_batch_grid_stride():
     assert float(I[:, :3].abs().max()) < 1e-4 and float((I[:, 6].abs() - 1).abs().max()) < 1e-6
 
 
+def test_wide_outputs_large_batch():
+    """2^18 elements through the ops with 36-float outputs (SE3 adjoint / adjoint-inverse stage
+    one input buffer per warp, Jr / Jr^-1 two): every warp of every CTA busy, grid-stride, a
+    ragged last tile; every row against the float64 oracle."""
+    n = (1 << 18) + 7
+    rng = np.random.default_rng(21)
+    T = rng.normal(size=(n, 7))
+    T[:, 3:] /= np.linalg.norm(T[:, 3:], axis=1, keepdims=True)
+    Tc = cu(T)
+    assert_close(dlie.se3_adjoint(Tc).reshape(n, 36), lie.se3_adjoint(np64(Tc)).reshape(n, 36), name="se3_adjoint")
+    assert_close(dlie.se3_adjoint_inv(Tc).reshape(n, 36), lie.se3_adjoint_inv(np64(Tc)).reshape(n, 36),
+                 name="se3_adjoint_inv")
+    xi = cu(rng.normal(scale=0.5, size=(n, 6)))
+    Jr = dlie.right_jacobian_se3(xi).reshape(n, 36)
+    ref = lie.right_jacobian_se3(np64(xi)).reshape(n, 36)
+    assert_close(Jr, ref, tol=1e-5, name="right_jacobian_se3")
+
+
 def test_boundary_errors():
     with pytest.raises(DeviceMismatchError):
         dlie.se3_log(torch.zeros(2, 7))
