@@ -4,7 +4,8 @@
 // (the reference obtains dL/dq by torch autograd through every SE3 op of
 // src/better_robot/kinematics/forward.py:73-135 and lie/_torch_native_backend.py).
 //
-// Adjoint, one warp per configuration:
+// Adjoint, one warp per configuration (two configurations per pass of the warp where their
+// frames fit one lane each: the per-frame stage then runs on both at once):
 //   * g_f = 2 w_f Jr^-1(xi_f)^T xi_f is dL/d(body twist of frame f), with the exact
 //     SE3 Jr^-1 (closed form jr_inv_T_xi; autograd differentiates se3_log exactly);
 //   * F_f = Ad(oMf^-1)^T g_f = [R g_lin; p x (R g_lin) + R g_ang] is the same
@@ -48,6 +49,8 @@ struct LossLayout {
   int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, fparent, fplace, fsup;
   int cta_floats;
   int in0, in1, poseT, poseQ, anc, F, W, gv, stage;
+  int pair;   // configurations per pass: 2 when both configurations' frames fit one lane each
+  int inlen;  // floats of one configuration's inputs (16-byte multiple)
   int warp_floats;
   __host__ __device__ LossLayout(int nj, int nq, int nv, int nf) {
     int o = 0;
@@ -57,11 +60,13 @@ struct LossLayout {
     fparent = take(nf); fplace = take(8 * nf); fsup = take(2 * nf);
     cta_floats = o;
     o = 0;
-    // the inputs of one configuration (q, stored oMi, targets), double buffered: the next
-    // configuration's are copied in (cp.async) while this one is computed
-    in0 = take(nq + 7 * nj + 7 * nf); in1 = take(nq + 7 * nj + 7 * nf);
-    poseT = take(4 * nj); poseQ = take(4 * nj); anc = take(nj);
-    F = take(8 * nf);     // world wrench per frame (f.xyz, pad, tau.xyz, pad)
+    pair = 2 * nf <= 32 ? 2 : 1;
+    inlen = round4(nq + 7 * nj + 7 * nf);
+    // the inputs of a pass's configurations (q, stored oMi, targets), double buffered: the next
+    // pass's are copied in (cp.async) while this one is computed
+    in0 = take(pair * inlen); in1 = take(pair * inlen);
+    poseT = take(pair * 4 * nj); poseQ = take(pair * 4 * nj); anc = take(nj);
+    F = take(pair * 8 * nf);  // world wrench per frame (f.xyz, pad, tau.xyz, pad), per configuration
     W = take(8 * nj);     // summed wrench of the frames each joint moves (same layout)
     gv = take(nv);        // dL/dv
     stage = take(nj * 7); // oMi staging (store mode)
@@ -70,7 +75,7 @@ struct LossLayout {
 };
 
 template <bool kBackward>
-__global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
+__global__ void __launch_bounds__(256, 2) pose_loss_kernel(const br_tree_t tree, const LossParams p) {
   extern __shared__ __align__(16) float smem[];
   const int nj = tree.njoints, nq = tree.nq, nv = tree.nv, nf = p.nf;
   const LossLayout L(nj, nq, nv, nf);
@@ -109,18 +114,21 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
   __syncthreads();
 
   float* w = smem + L.cta_floats + warp * L.warp_floats;
-  float* wpT = w + L.poseT;
-  float* wpQ = w + L.poseQ;
   int* wanc = reinterpret_cast<int*>(w + L.anc);
-  float* wF = w + L.F;
   float* wW = w + L.W;
   float* wg = w + L.gv;
   float* wst = w + L.stage;
   const int64_t stride = (int64_t)gridDim.x * wpc;
   const bool stored = kBackward && p.oMi_in;
   const int o_pose = nq, o_tgt = nq + (stored ? 7 * nj : 0);   // offsets in an input buffer
-  // queue the copies of configuration bb's inputs into `dst` (one commit group per call,
-  // empty past the end of the batch): 4-byte cp.async, the rows are 4-byte aligned only
+  // Configurations b and b + stride are taken as a pair when both fit the frame stage's lanes
+  // (2 nf <= 32): their FK, per-joint and per-column stages run one after the other over the
+  // whole warp, the per-frame stage (one lane per frame) over both at once.  Pose set, wrench
+  // set and input buffer hp belong to configuration b + hp * stride.
+  const int pair = L.pair;
+  const int64_t step = stride * pair;
+  // queue the copies of configuration bb's inputs into `dst` (nothing past the end of the
+  // batch): 4-byte cp.async, the rows are 4-byte aligned only
   auto prefetch = [&](int64_t bb, float* dst) {
     if (bb < p.batch) {
       const float* qb = p.q + bb * nq;
@@ -132,179 +140,213 @@ __global__ void pose_loss_kernel(const br_tree_t tree, const LossParams p) {
       const float* tb = p.targets + bb * (int64_t)nf * 7;
       for (int i = lane; i < nf * 7; i += kWarp) cp_async4(dst + o_tgt + i, tb + i);
     }
-    cp_async_commit();
   };
-  float* cur = w + L.in0;                  // this configuration's inputs; the other buffer: the next's
+  float* cur = w + L.in0;                  // this pass's inputs; the other buffers: the next pass's
   float* nxt = w + L.in1;
   int64_t b = (int64_t)blockIdx.x * wpc + warp;
-  prefetch(b, cur);
-  for (; b < p.batch; b += stride) {
-    __syncwarp();                          // every lane is done with the buffer refilled next
-    prefetch(b + stride, nxt);
-    cp_async_wait_groups<1>();             // this configuration's copies (all but the newest group)
+  for (int hp = 0; hp < pair; ++hp) prefetch(b + hp * stride, cur + hp * L.inlen);
+  cp_async_commit();                       // one commit group per pass
+  for (; b < p.batch; b += step) {
+    __syncwarp();                          // every lane is done with the buffers refilled next
+    for (int hp = 0; hp < pair; ++hp) prefetch(b + step + hp * stride, nxt + hp * L.inlen);
+    cp_async_commit();
+    cp_async_wait_groups<1>();             // this pass's copies (all but the newest group)
     __syncwarp();
-    const float* wq = cur;
-    const float* wtg = cur + o_tgt;
-    float* t = cur; cur = nxt; nxt = t;
-    if (stored) {
-      const float* ob = wq + o_pose;
-      for (int i = lane; i < nj * 7; i += kWarp) {
-        const int j = i / 7, c = i - 7 * j;
-        if (c < 3) wpT[4 * j + c] = ob[i];
-        else wpQ[4 * j + c - 3] = ob[i];
-      }
-      __syncwarp();
-    } else {
-      // forward kinematics by pointer jumping (see fk_jac.cu)
-      for (int j = lane; j < nj; j += kWarp) {
-        store_split(wpT, wpQ, j, local_transform(s_jtype[j], load_pose8(s_place + 8 * j), s_axis + 4 * j,
-                                                 wq + s_idxq[j]));
-        wanc[j] = s_parent[j];
-      }
-      __syncwarp();
-      for (int r = 0; r < tree.rounds; ++r) {
-        Pose A[2], Tj[2];
-        int aa[2], an[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int j = lane + kWarp * k;
-          an[k] = (j < nj) ? wanc[j] : -1;
-          if (an[k] >= 0) {
-            A[k] = load_split(wpT, wpQ, an[k]);
-            Tj[k] = load_split(wpT, wpQ, j);
-            aa[k] = wanc[an[k]];
-          }
+    const float* wq0 = cur;
+    { float* t = cur; cur = nxt; nxt = t; }
+    const int np = (pair == 2 && b + stride < p.batch) ? 2 : 1;
+    for (int hp = 0; hp < np; ++hp) {
+      const int64_t bh = b + hp * stride;
+      const float* wqh = wq0 + hp * L.inlen;
+      float* wpT = w + L.poseT + hp * 4 * nj;
+      float* wpQ = w + L.poseQ + hp * 4 * nj;
+      if (stored) {
+        const float* ob = wqh + o_pose;
+        for (int i = lane; i < nj * 7; i += kWarp) {
+          const int j = i / 7, c = i - 7 * j;
+          if (c < 3) wpT[4 * j + c] = ob[i];
+          else wpQ[4 * j + c - 3] = ob[i];
         }
         __syncwarp();
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int j = lane + kWarp * k;
-          if (an[k] >= 0) {
-            store_split(wpT, wpQ, j, compose(A[k], Tj[k]));
-            wanc[j] = aa[k];
-          }
+      } else {
+        // forward kinematics by pointer jumping (see fk_jac.cu)
+        for (int j = lane; j < nj; j += kWarp) {
+          store_split(wpT, wpQ, j, local_transform(s_jtype[j], load_pose8(s_place + 8 * j), s_axis + 4 * j,
+                                                   wqh + s_idxq[j]));
+          wanc[j] = s_parent[j];
         }
         __syncwarp();
-      }
-      if (!kBackward && p.oMi_out) {
-        for (int j = lane; j < nj; j += kWarp) store_pose7(wst + 7 * j, load_split(wpT, wpQ, j));
-        __syncwarp();
-        warp_copy(p.oMi_out + b * (int64_t)nj * 7, wst, nj * 7, lane);
+        for (int r = 0; r < tree.rounds; ++r) {
+          Pose A[2], Tj[2];
+          int aa[2], an[2];
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const int j = lane + kWarp * k;
+            an[k] = (j < nj) ? wanc[j] : -1;
+            if (an[k] >= 0) {
+              A[k] = load_split(wpT, wpQ, an[k]);
+              Tj[k] = load_split(wpT, wpQ, j);
+              aa[k] = wanc[an[k]];
+            }
+          }
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const int j = lane + kWarp * k;
+            if (an[k] >= 0) {
+              store_split(wpT, wpQ, j, compose(A[k], Tj[k]));
+              wanc[j] = aa[k];
+            }
+          }
+          __syncwarp();
+        }
+        if (!kBackward && p.oMi_out) {
+          for (int j = lane; j < nj; j += kWarp) store_pose7(wst + 7 * j, load_split(wpT, wpQ, j));
+          __syncwarp();
+          warp_copy(p.oMi_out + bh * (int64_t)nj * 7, wst, nj * 7, lane);
+          __syncwarp();
+        }
       }
     }
-    // per-frame residual, loss and (backward) world wrench
-    float acc = 0.f;
-    for (int f = lane; f < nf; f += kWarp) {
-      const Pose Tf = compose(load_split(wpT, wpQ, s_fparent[f]), load_pose8(s_fplace + 8 * f));
-      const float* tp = wtg + 7 * f;
+    // per-frame residual, loss and (backward) world wrench; frame f of the pair's second
+    // configuration on lane nf + f
+    float acc0 = 0.f, acc1 = 0.f;
+    for (int i = lane; i < np * nf; i += kWarp) {
+      const int hp = i >= nf ? 1 : 0;
+      const int f = i - hp * nf;
+      const int64_t bh = b + hp * stride;
+      const Pose Tf = compose(load_split(w + L.poseT + hp * 4 * nj, w + L.poseQ + hp * 4 * nj, s_fparent[f]),
+                              load_pose8(s_fplace + 8 * f));
+      const float* tp = wq0 + hp * L.inlen + o_tgt + 7 * f;
       const Pose Tt{f3(tp[0], tp[1], tp[2]), make_float4(tp[3], tp[4], tp[5], tp[6])};
       float3 v, om;
       se3_log(compose(inverse(Tt), Tf), v, om);
-      const float wf = __ldg(p.weights + (p.weights_per_config ? b * nf + f : f));
-      acc += wf * (dot(v, v) + dot(om, om));
+      const float wf = __ldg(p.weights + (p.weights_per_config ? bh * nf + f : f));
+      const float lf = wf * (dot(v, v) + dot(om, om));
+      if (hp) acc1 += lf; else acc0 += lf;
       if (kBackward) {
         float3 gl, ga;
         jr_inv_T_xi(v, om, gl, ga);
         const float s2 = 2.f * wf;
         const float3 fw = qrot(Tf.q, scale(gl, s2));
         const float3 tau = add(cross(Tf.t, fw), qrot(Tf.q, scale(ga, s2)));
+        float* wF = w + L.F + hp * 8 * nf;
         *reinterpret_cast<float4*>(wF + 8 * f) = make_float4(fw.x, fw.y, fw.z, 0.f);
         *reinterpret_cast<float4*>(wF + 8 * f + 4) = make_float4(tau.x, tau.y, tau.z, 0.f);
       }
     }
     if (!kBackward) {
+      // the second configuration's terms moved to lanes 0..nf-1 first, so that both sums
+      // take the same order (that of a configuration processed alone)
+      if (pair == 2) {
+        const float m1 = __shfl_sync(0xffffffffu, acc1, (lane + nf) & (kWarp - 1));
+        acc1 = lane + nf < kWarp ? m1 : 0.f;
+      }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) p.loss[b] = acc;
+      for (int o = 16; o > 0; o >>= 1) {
+        acc0 += __shfl_xor_sync(0xffffffffu, acc0, o);
+        acc1 += __shfl_xor_sync(0xffffffffu, acc1, o);
+      }
+      if (lane == 0) {
+        p.loss[b] = acc0;
+        if (np == 2) p.loss[b + stride] = acc1;
+      }
       continue;
     }
     __syncwarp();
-    // dL/dv_c = sum over the frames f that column c moves of <S_c, F_f> = <S_c, W_j>, where
-    // W_j sums F_f over the frames that c's joint j moves: one sum per joint, one dot per column
-    for (int j = lane; j < nj; j += kWarp) {
-      float4 sf = make_float4(0.f, 0.f, 0.f, 0.f), st = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (int f = 0; f < nf; ++f) {
-        if ((s_fsup[f] >> j) & 1ull) {
-          const float4 fw = *reinterpret_cast<const float4*>(wF + 8 * f);
-          const float4 tq = *reinterpret_cast<const float4*>(wF + 8 * f + 4);
-          sf.x += fw.x; sf.y += fw.y; sf.z += fw.z;
-          st.x += tq.x; st.y += tq.y; st.z += tq.z;
+    for (int hp = 0; hp < np; ++hp) {
+      const int64_t bh = b + hp * stride;
+      const float* wqh = wq0 + hp * L.inlen;
+      const float* wF = w + L.F + hp * 8 * nf;
+      const float* wpT = w + L.poseT + hp * 4 * nj;
+      const float* wpQ = w + L.poseQ + hp * 4 * nj;
+      // dL/dv_c = sum over the frames f that column c moves of <S_c, F_f> = <S_c, W_j>, where
+      // W_j sums F_f over the frames that c's joint j moves: one sum per joint, one dot per column
+      for (int j = lane; j < nj; j += kWarp) {
+        float4 sf = make_float4(0.f, 0.f, 0.f, 0.f), st = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int f = 0; f < nf; ++f) {
+          if ((s_fsup[f] >> j) & 1ull) {
+            const float4 fw = *reinterpret_cast<const float4*>(wF + 8 * f);
+            const float4 tq = *reinterpret_cast<const float4*>(wF + 8 * f + 4);
+            sf.x += fw.x; sf.y += fw.y; sf.z += fw.z;
+            st.x += tq.x; st.y += tq.y; st.z += tq.z;
+          }
+        }
+        *reinterpret_cast<float4*>(wW + 8 * j) = sf;
+        *reinterpret_cast<float4*>(wW + 8 * j + 4) = st;
+      }
+      __syncwarp();
+      const float go = __ldg(p.grad_loss + bh);
+      for (int c = lane; c < nv; c += kWarp) {
+        const int j = s_cjoint[c];
+        const Pose Tj = load_split(wpT, wpQ, j);
+        const float3 a = qrot(Tj.q, f3(s_caxis[4 * c], s_caxis[4 * c + 1], s_caxis[4 * c + 2]));
+        const float3 m = s_ckind[c] == 0 ? cross(Tj.t, a) : a;  // linear part of the world twist
+        const float3 an = s_ckind[c] == 0 ? a : f3(0.f, 0.f, 0.f);
+        const float4 fw = *reinterpret_cast<const float4*>(wW + 8 * j);
+        const float4 tq = *reinterpret_cast<const float4*>(wW + 8 * j + 4);
+        wg[c] = (dot(m, f3(fw.x, fw.y, fw.z)) + dot(an, f3(tq.x, tq.y, tq.z))) * go;
+      }
+      __syncwarp();
+      float* gq = p.grad_q + bh * nq;
+      for (int j = lane; j < nj; j += kWarp) {
+        const int jt = s_jtype[j];
+        const int iq = s_idxq[j];
+        if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
+          gq[iq] = wg[tree.idx_v[j]];
+        } else if (jt == BR_JOINT_TRANSLATION) {                     // q is the body translation
+          const int iv = tree.idx_v[j];
+          gq[iq] = wg[iv]; gq[iq + 1] = wg[iv + 1]; gq[iq + 2] = wg[iv + 2];
+        } else if (jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
+          // th = atan2(s, c) (revolute.py:206-211): dth/dc = -s / r^2, dth/ds = c / r^2
+          const float g = wg[tree.idx_v[j]];
+          const float c = wqh[iq], sn = wqh[iq + 1];
+          const float r2 = fmaxf(c * c + sn * sn, 1e-30f);
+          gq[iq] = -g * sn / r2;
+          gq[iq + 1] = g * c / r2;
+        } else if (jt == BR_JOINT_PLANAR) {
+          // T = ([x, y, 0], Rz(th)) with cos(th/2) = sqrt((1+c)/2), sin(th/2) = sqrt((1-c)/2) sign(s)
+          // (planar.py:20-41): body twist = (R^T [dx, dy, 0], e_z dth), dth/dc = -1 / sin(th),
+          // and th does not depend on s away from s = 0
+          const int iv = tree.idx_v[j];
+          const float c = wqh[iq + 2], sn = wqh[iq + 3];
+          const float4 hq = planar_quat(c, sn);
+          const float ct = hq.w * hq.w - hq.z * hq.z, st = 2.f * hq.z * hq.w;
+          const float g0 = wg[iv], g1 = wg[iv + 1], g2 = wg[iv + 2];
+          gq[iq] = ct * g0 - st * g1;
+          gq[iq + 1] = st * g0 + ct * g1;
+          gq[iq + 2] = -g2 / st;
+          gq[iq + 3] = 0.f;
+        } else if (jt == BR_JOINT_FREE_FLYER || jt == BR_JOINT_SPHERICAL) {
+          // free-flyer [t, quat] / spherical [quat]: the quaternion's body rotation
+          const bool ff = jt == BR_JOINT_FREE_FLYER;
+          const int iv = tree.idx_v[j];
+          const int qo = ff ? iq + 3 : iq;                          // first quaternion slot
+          const int vo = ff ? iv + 3 : iv;                          // first rotation column
+          const float4 qr = make_float4(wqh[qo], wqh[qo + 1], wqh[qo + 2], wqh[qo + 3]);
+          const float4 u = qnormalize(qr);
+          const float n = fmaxf(sqrtf(qr.x * qr.x + qr.y * qr.y + qr.z * qr.z + qr.w * qr.w), 1e-8f);
+          const float3 ga = f3(wg[vo], wg[vo + 1], wg[vo + 2]);
+          // quaternion: delta_ang = 2 vec(u* (x) du), du = (I - u u^T) dquat / n
+          float4 h;
+          h.x = u.w * ga.x - u.z * ga.y + u.y * ga.z;
+          h.y = u.z * ga.x + u.w * ga.y - u.x * ga.z;
+          h.z = -u.y * ga.x + u.x * ga.y + u.w * ga.z;
+          h.w = -u.x * ga.x - u.y * ga.y - u.z * ga.z;
+          const float uh = u.x * h.x + u.y * h.y + u.z * h.z + u.w * h.w;
+          const float s = 2.f / n;
+          if (ff) {
+            const float3 gt = qrot(u, f3(wg[iv], wg[iv + 1], wg[iv + 2]));  // translation: delta_lin = R^T dt
+            gq[iq] = gt.x; gq[iq + 1] = gt.y; gq[iq + 2] = gt.z;
+          }
+          gq[qo] = s * (h.x - u.x * uh);
+          gq[qo + 1] = s * (h.y - u.y * uh);
+          gq[qo + 2] = s * (h.z - u.z * uh);
+          gq[qo + 3] = s * (h.w - u.w * uh);
         }
       }
-      *reinterpret_cast<float4*>(wW + 8 * j) = sf;
-      *reinterpret_cast<float4*>(wW + 8 * j + 4) = st;
+      __syncwarp();
     }
-    __syncwarp();
-    const float go = __ldg(p.grad_loss + b);
-    for (int c = lane; c < nv; c += kWarp) {
-      const int j = s_cjoint[c];
-      const Pose Tj = load_split(wpT, wpQ, j);
-      const float3 a = qrot(Tj.q, f3(s_caxis[4 * c], s_caxis[4 * c + 1], s_caxis[4 * c + 2]));
-      const float3 m = s_ckind[c] == 0 ? cross(Tj.t, a) : a;  // linear part of the world twist
-      const float3 an = s_ckind[c] == 0 ? a : f3(0.f, 0.f, 0.f);
-      const float4 fw = *reinterpret_cast<const float4*>(wW + 8 * j);
-      const float4 tq = *reinterpret_cast<const float4*>(wW + 8 * j + 4);
-      wg[c] = (dot(m, f3(fw.x, fw.y, fw.z)) + dot(an, f3(tq.x, tq.y, tq.z))) * go;
-    }
-    __syncwarp();
-    float* gq = p.grad_q + b * nq;
-    for (int j = lane; j < nj; j += kWarp) {
-      const int jt = s_jtype[j];
-      const int iq = s_idxq[j];
-      if (jt == BR_JOINT_REVOLUTE || jt == BR_JOINT_PRISMATIC) {
-        gq[iq] = wg[tree.idx_v[j]];
-      } else if (jt == BR_JOINT_TRANSLATION) {                     // q is the body translation
-        const int iv = tree.idx_v[j];
-        gq[iq] = wg[iv]; gq[iq + 1] = wg[iv + 1]; gq[iq + 2] = wg[iv + 2];
-      } else if (jt == BR_JOINT_REVOLUTE_UNBOUNDED) {
-        // th = atan2(s, c) (revolute.py:206-211): dth/dc = -s / r^2, dth/ds = c / r^2
-        const float g = wg[tree.idx_v[j]];
-        const float c = wq[iq], sn = wq[iq + 1];
-        const float r2 = fmaxf(c * c + sn * sn, 1e-30f);
-        gq[iq] = -g * sn / r2;
-        gq[iq + 1] = g * c / r2;
-      } else if (jt == BR_JOINT_PLANAR) {
-        // T = ([x, y, 0], Rz(th)) with cos(th/2) = sqrt((1+c)/2), sin(th/2) = sqrt((1-c)/2) sign(s)
-        // (planar.py:20-41): body twist = (R^T [dx, dy, 0], e_z dth), dth/dc = -1 / sin(th),
-        // and th does not depend on s away from s = 0
-        const int iv = tree.idx_v[j];
-        const float c = wq[iq + 2], sn = wq[iq + 3];
-        const float4 hq = planar_quat(c, sn);
-        const float ct = hq.w * hq.w - hq.z * hq.z, st = 2.f * hq.z * hq.w;
-        const float g0 = wg[iv], g1 = wg[iv + 1], g2 = wg[iv + 2];
-        gq[iq] = ct * g0 - st * g1;
-        gq[iq + 1] = st * g0 + ct * g1;
-        gq[iq + 2] = -g2 / st;
-        gq[iq + 3] = 0.f;
-      } else if (jt == BR_JOINT_FREE_FLYER || jt == BR_JOINT_SPHERICAL) {
-        // free-flyer [t, quat] / spherical [quat]: the quaternion's body rotation
-        const bool ff = jt == BR_JOINT_FREE_FLYER;
-        const int iv = tree.idx_v[j];
-        const int qo = ff ? iq + 3 : iq;                          // first quaternion slot
-        const int vo = ff ? iv + 3 : iv;                          // first rotation column
-        const float4 qr = make_float4(wq[qo], wq[qo + 1], wq[qo + 2], wq[qo + 3]);
-        const float4 u = qnormalize(qr);
-        const float n = fmaxf(sqrtf(qr.x * qr.x + qr.y * qr.y + qr.z * qr.z + qr.w * qr.w), 1e-8f);
-        const float3 ga = f3(wg[vo], wg[vo + 1], wg[vo + 2]);
-        // quaternion: delta_ang = 2 vec(u* (x) du), du = (I - u u^T) dquat / n
-        float4 h;
-        h.x = u.w * ga.x - u.z * ga.y + u.y * ga.z;
-        h.y = u.z * ga.x + u.w * ga.y - u.x * ga.z;
-        h.z = -u.y * ga.x + u.x * ga.y + u.w * ga.z;
-        h.w = -u.x * ga.x - u.y * ga.y - u.z * ga.z;
-        const float uh = u.x * h.x + u.y * h.y + u.z * h.z + u.w * h.w;
-        const float s = 2.f / n;
-        if (ff) {
-          const float3 gt = qrot(u, f3(wg[iv], wg[iv + 1], wg[iv + 2]));  // translation: delta_lin = R^T dt
-          gq[iq] = gt.x; gq[iq + 1] = gt.y; gq[iq + 2] = gt.z;
-        }
-        gq[qo] = s * (h.x - u.x * uh);
-        gq[qo + 1] = s * (h.y - u.y * uh);
-        gq[qo + 2] = s * (h.z - u.z * uh);
-        gq[qo + 3] = s * (h.w - u.w * uh);
-      }
-    }
-    __syncwarp();
   }
   cp_async_wait_groups<0>();               // the (empty) last group
 }
