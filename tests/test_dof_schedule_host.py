@@ -173,6 +173,57 @@ def test_schedule_levels_are_race_free(name):
     assert seen == sum(d * (d + 1) // 2 + d for d in dep)
 
 
+def _trunk(dof_parent, kmax=6):
+    """The float64 LM variants' register trunk (``lm_solve.cu``): the largest n <= 6 with DOFs
+    0..n-1 a chain from the root and every other DOF below DOF n - 1; 0 when n < 2."""
+    dp = [int(p) for p in dof_parent]
+    nv = len(dp)
+    _, anc, _ = _tree(dp)
+    for n in range(min(nv, kmax), 1, -1):
+        if dp[0] < 0 and all(dp[c] == c - 1 for c in range(1, n)) and all(n - 1 in anc[c] for c in range(n, nv)):
+            return n
+    return 0
+
+
+@pytest.mark.parametrize("name", ["chain7", "humanoid", "dual_arm", "mixed", "forest", "star"])
+def test_schedule_ends_with_the_trunk(name):
+    """The kernel skips the schedule's last n levels for a trunk of n DOFs and eliminates
+    n - 1, ..., 0 itself in registers, entry (i, j) <- fma(-(L_ki / d_k), L_kj, .): those
+    levels must hold exactly that, one DOF per level, one contribution per entry."""
+    parents = _dof_parents()
+    if name not in parents:
+        pytest.skip("no such robot in this build")
+    dp = parents[name]
+    n = _trunk(dp)
+    expect = {"chain7": 6, "humanoid": 6, "dual_arm": 0, "forest": 0, "star": 0}
+    if name in expect:
+        assert n == expect[name]
+    if n == 0:
+        return
+    nlev, _, starts, tasks, extra = _decode(_schedule(dp))
+    _, _, rowoff = _tree(dp)
+    zoff = rowoff[len(dp)]
+    tri = lambda i: i * (i + 1) // 2  # noqa: E731
+    for step, lev in enumerate(range(nlev - n, nlev)):
+        k = n - 1 - step
+        seen = set()
+        for tk in tasks[starts[lev]:starts[lev + 1]]:
+            cs = _contribs(tk, extra)
+            assert len(cs) == 1
+            a, b, d = cs[0]
+            dst = int(tk[0] & 0xffff)
+            assert d == k and dst not in seen
+            seen.add(dst)
+            if dst < zoff:                       # entry (i, j) of a trunk row, i < k
+                i = max(r for r in range(k) if tri(r) <= dst)
+                j = dst - tri(i)
+                assert (a, b) == (tri(k) + i, tri(k) + j)
+            else:                                # right-hand side of trunk DOF i < k
+                i = dst - zoff
+                assert i < k and (a, b) == (tri(k) + i, zoff + k)
+        assert len(seen) == tri(k) + k           # every entry of rows 0..k-1 and their z
+
+
 def test_schedule_rejects_bad_parents():
     lib = _lib()
     bad = np.array([-1, 1], np.int32)   # a DOF whose parent is not earlier
