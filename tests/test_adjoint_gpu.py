@@ -4,7 +4,7 @@
 * against float64 central finite differences (eps 1e-6) of the oracle loss;
 * store and recompute modes give identical gradients.
 
-Tolerance (north star): relative error ``|g - g_ref|_2 / |g_ref|_2 <= 1e-5`` per
+Tolerance: relative error ``|g - g_ref|_2 / |g_ref|_2 <= 1e-5`` per
 configuration (float32 kernel vs float64 references); the loss itself within
 1e-5 relative.
 """

@@ -192,7 +192,7 @@ def test_schedule_ends_with_the_trunk(name):
     levels must hold exactly that, one DOF per level, one contribution per entry."""
     parents = _dof_parents()
     if name not in parents:
-        pytest.skip("no such robot in this build")
+        pytest.skip("no such robot in the synthetic module")
     dp = parents[name]
     n = _trunk(dp)
     expect = {"chain7": 6, "humanoid": 6, "dual_arm": 0, "forest": 0, "star": 0}
