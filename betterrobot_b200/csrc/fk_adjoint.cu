@@ -49,9 +49,12 @@ struct LossLayout {
   int parent, jtype, idxq, axis, place, cjoint, ckind, caxis, fparent, fplace, fsup;
   int cta_floats;
   int in0, in1, poseT, poseQ, anc, F, W, gv, stage;
-  int pair;   // configurations per pass: 2 when both configurations' frames fit one lane each
+  int pair;   // configurations per pass (2 or 1)
   int inlen;  // floats of one configuration's inputs (16-byte multiple)
   int warp_floats;
+  // A warp's slice with two configurations per pass above this many floats would leave one
+  // 8-warp CTA per SM instead of two (the humanoid at 12 frames takes 2,644).
+  static constexpr int kPairMaxWarpFloats = 3456;
   __host__ __device__ LossLayout(int nj, int nq, int nv, int nf) {
     int o = 0;
     auto take = [&](int n) { int r = o; o += round4(n); return r; };
@@ -59,18 +62,22 @@ struct LossLayout {
     cjoint = take(nv); ckind = take(nv); caxis = take(4 * nv);
     fparent = take(nf); fplace = take(8 * nf); fsup = take(2 * nf);
     cta_floats = o;
-    o = 0;
-    pair = 2 * nf <= 32 ? 2 : 1;
     inlen = round4(nq + 7 * nj + 7 * nf);
-    // the inputs of a pass's configurations (q, stored oMi, targets), double buffered: the next
-    // pass's are copied in (cp.async) while this one is computed
-    in0 = take(pair * inlen); in1 = take(pair * inlen);
-    poseT = take(pair * 4 * nj); poseQ = take(pair * 4 * nj); anc = take(nj);
-    F = take(pair * 8 * nf);  // world wrench per frame (f.xyz, pad, tau.xyz, pad), per configuration
-    W = take(8 * nj);     // summed wrench of the frames each joint moves (same layout)
-    gv = take(nv);        // dL/dv
-    stage = take(nj * 7); // oMi staging (store mode)
-    warp_floats = o;
+    // two configurations per pass when both configurations' frames fit one lane each and the
+    // slice stays small enough, else one
+    for (pair = 2 * nf <= 32 ? 2 : 1;; pair = 1) {
+      o = 0;
+      // the inputs of a pass's configurations (q, stored oMi, targets), double buffered: the
+      // next pass's are copied in (cp.async) while this one is computed
+      in0 = take(pair * inlen); in1 = take(pair * inlen);
+      poseT = take(pair * 4 * nj); poseQ = take(pair * 4 * nj); anc = take(nj);
+      F = take(pair * 8 * nf);  // world wrench per frame (f.xyz, pad, tau.xyz, pad), per configuration
+      W = take(8 * nj);         // summed wrench of the frames each joint moves (same layout)
+      gv = take(nv);            // dL/dv
+      stage = take(nj * 7);     // oMi staging (store mode)
+      warp_floats = o;
+      if (pair == 1 || warp_floats <= kPairMaxWarpFloats) break;
+    }
   }
 };
 

@@ -99,6 +99,27 @@ def test_matches_float64_central_differences(robot):
     assert rel.max() <= GRAD_TOL, rel
 
 
+@pytest.mark.parametrize("nf", [16, 20])
+@pytest.mark.parametrize("mode", ["store", "recompute"])
+def test_frame_counts_around_configuration_pairing(nf, mode):
+    """With 2 nf <= 32 frames a warp takes two configurations per pass (B odd: the last pass
+    of a warp may hold one), with more it takes one: both against float64 central differences."""
+    m, m64 = syn.model_from_spec(syn.humanoid_spec()), syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
+    base = syn.op_frame_ids(m) + list(range(m.nframes))
+    fids = [int(base[i % len(base)]) for i in range(nf)]
+    B = 37
+    q = syn.random_q(m64, B, 98, rev_range=2.5, base_translation=1.0).numpy()
+    targets = syn.random_targets(B, nf, 99).numpy()
+    w = np.random.default_rng(100).uniform(0.5, 2.0, size=nf)
+    loss, grad = _grad(m, q, fids, targets, w, mode)
+    q32 = q.astype(np.float32).astype(np.float64)
+    t32 = targets.astype(np.float32).astype(np.float64)
+    w32 = w.astype(np.float32).astype(np.float64)
+    np.testing.assert_allclose(loss, _loss64(m64, q32, fids, t32, w32), rtol=1e-5)
+    rel = _rel(grad, _fd(m64, q32, fids, t32, w32))
+    assert rel.max() <= GRAD_TOL, rel
+
+
 def test_store_equals_recompute_and_weights_per_config():
     m = syn.model_from_spec(syn.humanoid_spec())
     m64 = syn.model_from_spec(syn.humanoid_spec(), dtype=torch.float64)
