@@ -30,6 +30,37 @@ def test_header_declares_entry_points():
     assert sorted(_lib.SIGNATURES) == names
 
 
+def _prototypes():
+    """name -> list of parameter declarations, from every BR_API prototype of the headers."""
+    out = {}
+    for fn in os.listdir(os.path.join(REPO, "include")):
+        if fn.endswith(".h"):
+            src = open(os.path.join(REPO, "include", fn)).read()
+            for m in re.finditer(r"BR_API\s+[^;{]*?\b(br_\w+)\s*\(([^)]*)\)\s*;", src, flags=re.S):
+                params = [" ".join(x.split()) for x in m.group(2).split(",")]
+                out[m.group(1)] = [] if params == ["void"] or params == [""] else params
+    return out
+
+
+def test_ctypes_signatures_match_the_prototypes():
+    """Every entry point's ctypes argtypes have the prototype's arity, and each parameter's
+    kind: a pointer (to a struct: POINTER of the mirror struct) / int32_t / int64_t."""
+    protos = _prototypes()
+    assert sorted(protos) == sorted(_lib.SIGNATURES)
+    for name, params in protos.items():
+        args = _lib.SIGNATURES[name][1]
+        assert len(args) == len(params), name
+        for decl, ct in zip(params, args):
+            if "*" in decl:
+                assert ct is ctypes.c_void_p or issubclass(ct, ctypes._Pointer), (name, decl, ct)
+            elif decl.startswith("int64_t"):
+                assert ct is ctypes.c_int64, (name, decl, ct)
+            elif decl.startswith("int32_t"):
+                assert ct is ctypes.c_int32, (name, decl, ct)
+            else:
+                raise AssertionError(f"{name}: unexpected parameter type {decl!r}")
+
+
 def test_library_loads_and_exports_every_declared_symbol():
     lib = _lib.load()
     for name in _declared_symbols():
