@@ -68,6 +68,44 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert b"sm_100a" in lib.br_version()
 
 
+def _header_structs():
+    """typedef name -> [(C type, field name)] in declaration order, from the headers."""
+    out = {}
+    for fn in os.listdir(os.path.join(REPO, "include")):
+        if fn.endswith(".h"):
+            src = open(os.path.join(REPO, "include", fn)).read()
+            src = re.sub(r"/\*.*?\*/", " ", src, flags=re.S)
+            for m in re.finditer(r"typedef\s+struct\s+\w+\s*\{(.*?)\}\s*(\w+)\s*;", src, flags=re.S):
+                fields = []
+                for decl in m.group(1).split(";"):
+                    decl = " ".join(decl.split())
+                    if not decl:
+                        continue
+                    first = re.match(r"((?:const\s+)?\w+\s*\**)\s*(.*)", decl)
+                    ctype, names = first.group(1).replace(" ", ""), first.group(2)
+                    for nm in names.split(","):
+                        nm = nm.strip()
+                        stars = len(nm) - len(nm.lstrip("*"))
+                        fields.append((ctype + "*" * stars, nm.lstrip("*").strip()))
+                out[m.group(2)] = fields
+    return out
+
+
+@pytest.mark.parametrize("c_name,mirror", [("br_tree_t", "BrTree"), ("br_ik_settings_t", "IKSettings"),
+                                           ("br_ik_batch_t", "IKBatch"), ("br_ik_result_t", "IKResultBuf"),
+                                           ("br_traj_settings_t", "TrajSettings")])
+def test_struct_mirrors_match_header(c_name, mirror):
+    """Field names, order and kinds of each ctypes mirror equal the header's struct."""
+    fields = _header_structs()[c_name]
+    py = getattr(_lib, mirror)._fields_
+    assert [n for _, n in fields] == [n for n, _ in py], c_name
+    for (ctype, name), (_, ct) in zip(fields, py):
+        if ctype.endswith("*"):
+            assert ct is ctypes.c_void_p or issubclass(ct, ctypes._Pointer), (name, ctype, ct)
+        else:
+            assert ct is {"float": ctypes.c_float, "int32_t": ctypes.c_int32, "int64_t": ctypes.c_int64}[ctype], name
+
+
 def test_tree_struct_layout_matches_header():
     # 8 int32 (sizes, rounds, kinds, dof_entries, dof_depth), then 14 table pointers and dof_sched
     assert ctypes.sizeof(_lib.BrTree) == 32 + 15 * 8
